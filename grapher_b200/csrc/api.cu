@@ -1,0 +1,1072 @@
+// api.cu -- the C ABI of libgvizcuda (include/gvizcuda.h).
+//
+// One handle = one set of device buffers + one stream. A step is
+//   structForce -> oldStructForce            (gvizForceEmbedder.c:449-450)
+//   quadtree rebuild (tree.cu)               (:451-453)
+//   attraction + repulsion + gravity         (:455-457, computeForceRange)
+//   swing/traction, global speed, apply      (:459-465)
+//   step tail and the five stats             (:467-492)
+// captured once into a CUDA graph and replayed; nothing in it waits on the
+// host, so Run() can enqueue many steps and check convergence in batches.
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "epilogue.cuh"
+#include "internal.cuh"
+
+void tree_set_smem_limits();
+void enqueue_cell_dump(gvizCudaForce *h, int32_t *depth, uint64_t *hi,
+                       uint64_t *lo, double *mass, double *cx, double *cy,
+                       uint64_t *cnt);
+
+namespace {
+
+constexpr int kRunBatch = 8;
+
+int set_err(gvizCudaForce *h, int code) {
+  if (h && code != GVIZ_CUDA_OK) h->lastError = code;
+  return code;
+}
+
+template <typename T>
+int dalloc(gvizCudaForce *h, T **p, size_t count) {
+  size_t bytes = count * sizeof(T);
+  if (bytes == 0) bytes = 16;
+  if (cudaMalloc((void **)p, bytes) != cudaSuccess) {
+    *p = nullptr;
+    return set_err(h, GVIZ_CUDA_ERR_ALLOC);
+  }
+  return GVIZ_CUDA_OK;
+}
+
+template <typename T>
+void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+bool g_dirUploaded[64] = {false};
+
+int upload_dir_table(gvizCudaForce *h) {
+  if (h->device < 64 && g_dirUploaded[h->device]) return GVIZ_CUDA_OK;
+  double t[2 * GVIZ_DIR_TABLE];
+  for (int k = 0; k < GVIZ_DIR_TABLE; k++) {
+    double a = 2.0 * M_PI * (double)k / (double)GVIZ_DIR_TABLE;
+    t[2 * k] = cos(a);
+    t[2 * k + 1] = sin(a);
+  }
+  if (dir_table_upload_forces(t) || dir_table_upload_precise(t))
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  if (h->device < 64) g_dirUploaded[h->device] = true;
+  return GVIZ_CUDA_OK;
+}
+
+void free_all(gvizCudaForce *h) {
+  dfree(h->d_rowOff);
+  dfree(h->d_cols);
+  dfree(h->d_degree);
+  dfree(h->d_mass);
+  dfree(h->d_massF);
+  dfree(h->d_radius);
+  dfree(h->d_radiusF);
+  dfree(h->d_gid);
+  dfree(h->d_graphOff);
+  dfree(h->d_meanDegPlusOne);
+  dfree(h->d_chunkBegin);
+  dfree(h->d_chunkEnd);
+  dfree(h->d_chunkGraph);
+  dfree(h->d_gChunkBegin);
+  dfree(h->d_gChunkEnd);
+  dfree(h->d_pos);
+  dfree(h->d_sf);
+  dfree(h->d_sfOld);
+  dfree(h->d_disp);
+  dfree(h->d_applied);
+  dfree(h->d_att);
+  dfree(h->d_rep);
+  dfree(h->d_swing);
+  dfree(h->d_trac);
+  dfree(h->d_attF);
+  dfree(h->d_attD);
+  dfree(h->d_speed);
+  dfree(h->d_eff);
+  dfree(h->d_active);
+  dfree(h->d_anyActive);
+  dfree(h->d_iter);
+  dfree(h->d_runLeft);
+  dfree(h->d_runEps);
+  dfree(h->d_stats);
+  dfree(h->d_lastStats);
+  dfree(h->d_chunkStat);
+  dfree(h->d_status);
+  dfree(h->d_chunkBox);
+  dfree(h->d_roots);
+  dfree(h->d_keyHi);
+  dfree(h->d_keyLo);
+  dfree(h->d_ck);
+  dfree(h->d_ckAlt);
+  dfree(h->d_idx);
+  dfree(h->d_idxAlt);
+  dfree(h->d_sHi);
+  dfree(h->d_sLo);
+  dfree(h->d_flag);
+  dfree(h->d_scan);
+  dfree(h->d_runStart);
+  dfree(h->d_deepRuns);
+  dfree(h->d_counts);
+  dfree(h->d_radixHist);
+  dfree(h->d_scanTile);
+  dfree(h->d_bHi);
+  dfree(h->d_bLo);
+  dfree(h->d_bGid);
+  dfree(h->d_bStart);
+  dfree(h->d_nLeft);
+  dfree(h->d_nRight);
+  dfree(h->d_nFirst);
+  dfree(h->d_nLast);
+  dfree(h->d_nDelta);
+  dfree(h->d_nCounter);
+  dfree(h->d_upInt);
+  dfree(h->d_upLeaf);
+  dfree(h->d_nM);
+  dfree(h->d_nSX);
+  dfree(h->d_nSY);
+  dfree(h->d_nCnt);
+  dfree(h->d_nT);
+  dfree(h->d_nFlag);
+  dfree(h->d_bM);
+  dfree(h->d_bSX);
+  dfree(h->d_bSY);
+  dfree(h->d_bCnt);
+  dfree(h->d_bT);
+  dfree(h->d_rootNode);
+  dfree(h->d_rootT);
+  dfree(h->d_graphBase);
+  dfree(h->d_nodes);
+  dfree(h->d_leafDepth);
+  dfree(h->d_counters);
+}
+
+int upload_radius(gvizCudaForce *h) {
+  const size_t V = h->V;
+  std::vector<double> r(V ? V : 1, 0.0);
+  std::vector<float> rf(V ? V : 1, 0.0f);
+  std::vector<uint32_t> deg(V ? V : 1);
+  if (V && cudaMemcpy(deg.data(), h->d_degree, V * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  if (h->params.preventOverlap) {
+    // gvizForceEmbedderVertexRadius, src/embedders/gvizForceEmbedder.c:389-393
+    for (size_t i = 0; i < V; i++) {
+      r[i] = h->params.radiusBase *
+             (1.0 + h->params.radiusPerDegree * sqrt((double)deg[i]));
+      rf[i] = (float)r[i];
+    }
+  }
+  if (V && (cudaMemcpy(h->d_radius, r.data(), V * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(h->d_radiusF, rf.data(), V * 4, cudaMemcpyHostToDevice) != cudaSuccess))
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  return GVIZ_CUDA_OK;
+}
+
+// ---- the step ------------------------------------------------------------
+
+void enqueue_step(gvizCudaForce *h) {
+  cudaStream_t st = h->stream;
+  cudaMemsetAsync(h->d_status, 0, sizeof(uint32_t), st);
+  cudaMemcpyAsync(h->d_sfOld, h->d_sf, h->V * sizeof(double2),
+                  cudaMemcpyDeviceToDevice, st);
+  const bool f64 = h->params.precision == GVIZ_CUDA_FP64;
+  const bool bh = h->params.barnesHutEnabled != 0;
+  if (bh) enqueue_tree_build(h);
+  if (f64)
+    enqueue_attraction_f64(h);
+  else
+    enqueue_attraction_f32(h);
+  if (bh) {
+    if (f64)
+      enqueue_walk_f64(h);
+    else
+      enqueue_walk_f32(h, nullptr);
+  } else {
+    if (f64)
+      enqueue_exact_f64(h);
+    else
+      enqueue_exact_f32(h);
+  }
+  if (!h->forceOnly) enqueue_fa2(h);
+}
+
+int ensure_graph(gvizCudaForce *h) {
+  if (!h->graphDirty && h->stepExec) return GVIZ_CUDA_OK;
+  if (h->stepExec) {
+    cudaGraphExecDestroy(h->stepExec);
+    h->stepExec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  enqueue_step(h);
+  if (cudaStreamEndCapture(h->stream, &g) != cudaSuccess || !g)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  size_t nNodes = 0;
+  cudaGraphGetNodes(g, nullptr, &nNodes);
+  std::vector<cudaGraphNode_t> nodes(nNodes);
+  if (nNodes) cudaGraphGetNodes(g, nodes.data(), &nNodes);
+  h->kernelsPerStep = 0;
+  for (size_t i = 0; i < nNodes; i++) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+      h->kernelsPerStep++;
+  }
+  cudaError_t e = cudaGraphInstantiate(&h->stepExec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  h->graphDirty = false;
+  return GVIZ_CUDA_OK;
+}
+
+int launch_steps(gvizCudaForce *h, uint32_t n) {
+  if (h->V == 0) return GVIZ_CUDA_OK;
+  int rc = ensure_graph(h);
+  if (rc) return rc;
+  for (uint32_t i = 0; i < n; i++)
+    if (cudaGraphLaunch(h->stepExec, h->stream) != cudaSuccess)
+      return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  return GVIZ_CUDA_OK;
+}
+
+int status_to_code(uint32_t st) {
+  if (st & GVIZ_ST_NONFINITE) return GVIZ_CUDA_ERR_NONFINITE;
+  if (st & GVIZ_ST_DEEP_RUN) return GVIZ_CUDA_ERR_DEEP_RUN;
+  if (st & GVIZ_ST_TREE) return GVIZ_CUDA_ERR_CUDA;
+  return GVIZ_CUDA_OK;
+}
+
+int sync_and_check(gvizCudaForce *h) {
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  uint32_t st = 0;
+  if (cudaMemcpy(&st, h->d_status, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  return set_err(h, status_to_code(st));
+}
+
+void set_all_active(gvizCudaForce *h, uint64_t runLeft, double eps) {
+  std::vector<uint32_t> one(h->G, 1u);
+  std::vector<uint64_t> left(h->G, runLeft);
+  std::vector<double> e(h->G, eps);
+  uint32_t any = (uint32_t)h->G;
+  cudaMemcpy(h->d_active, one.data(), h->G * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->d_runLeft, left.data(), h->G * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->d_runEps, e.data(), h->G * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(h->d_anyActive, &any, 4, cudaMemcpyHostToDevice);
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+double fill_stats(gvizCudaForce *h, gvizCudaStepStats *stats) {
+  std::vector<double> row(h->G * 5);
+  cudaMemcpy(row.data(), h->d_lastStats, h->G * 5 * sizeof(double),
+             cudaMemcpyDeviceToHost);
+  if (stats)
+    for (size_t g = 0; g < h->G; g++) {
+      stats[g].maxDisp = row[5 * g + 0];
+      stats[g].speed = row[5 * g + 1];
+      stats[g].meanAttractive = row[5 * g + 2];
+      stats[g].meanRepulsive = row[5 * g + 3];
+      stats[g].meanGravity = row[5 * g + 4];
+    }
+  return row[0];
+}
+
+}  // namespace
+
+// ---- shared helpers declared in internal.cuh -----------------------------
+
+int gviz_check(gvizCudaForce *h, cudaError_t e) {
+  return e == cudaSuccess ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_CUDA);
+}
+
+void prof_mark(gvizCudaForce *h, const char *name) {
+  if (!h->profiling || h->nProf >= 63) return;
+  h->profName[h->nProf] = name;
+  cudaEventRecord(h->profEv[h->nProf + 1], h->stream);
+  h->nProf++;
+}
+
+// ---- C ABI ---------------------------------------------------------------
+
+extern "C" {
+
+void gvizCudaForceDefaultParams(gvizCudaForceParams *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->edgeLength = 10.0;        // GVIZ_FORCE_EMBEDDER_EDGE_LENGTH_DEFAULT
+  p->theta = 1.0;              // GVIZ_FORCE_EMBEDDER_THETA_DEFAULT
+  p->nodesPerCell = 1;         // GVIZ_QUADTREE_NODES_PER_CELL_DEFAULT
+  p->barnesHutEnabled = 1;
+  p->gravityK = 0.0;
+  p->radiusBase = 0.0;
+  p->radiusPerDegree = 0.0;
+  p->overlapConstant = 100.0;  // GVIZ_FORCE_EMBEDDER_OVERLAP_CONSTANT_DEFAULT
+  p->preventOverlap = 0;
+  p->precision = GVIZ_CUDA_FP32;
+  p->jitterTolerance = 1.0;    // GVIZ_FORCE_EMBEDDER_JITTER_TOLERANCE_DEFAULT
+  p->strictReductions = 0;
+  p->farField = 0;
+}
+
+int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
+  if (!out || !g) return GVIZ_CUDA_ERR_ARG;
+  *out = nullptr;
+  const size_t V = g->vertexCount;
+  const size_t G = g->graphCount ? g->graphCount : 1;
+  if (V > 0 && (!g->rowOffsets || (g->rowOffsets[V] > 0 && !g->neighbors)))
+    return GVIZ_CUDA_ERR_ARG;
+  if (G > 1 && !g->graphOffsets) return GVIZ_CUDA_ERR_ARG;
+  if (g->model != GVIZ_CUDA_MODEL_FR && g->model != GVIZ_CUDA_MODEL_LINLOG)
+    return GVIZ_CUDA_ERR_ARG;
+  if (V >= 0x7fffffffull / 3 || (V && g->rowOffsets[V] >= 0xffffffffull))
+    return GVIZ_CUDA_ERR_LIMIT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0)
+    return GVIZ_CUDA_ERR_NO_DEVICE;
+  if (g->device < 0 || g->device >= ndev) return GVIZ_CUDA_ERR_ARG;
+
+  gvizCudaForce *h = new (std::nothrow) gvizCudaForce();
+  if (!h) return GVIZ_CUDA_ERR_ALLOC;
+  h->device = g->device;
+  DeviceGuard guard(h->device);
+  h->model = g->model;
+  h->V = V;
+  h->G = G;
+  h->E2 = V ? g->rowOffsets[V] : 0;
+  gvizCudaForceDefaultParams(&h->params);
+  int gb = 0;
+  while (G > 1 && (1ull << gb) < G) gb++;
+  if (gb & 1) gb++;
+  h->gbits = G > 1 ? gb : 0;
+  if (h->gbits > 40) {
+    delete h;
+    return GVIZ_CUDA_ERR_LIMIT;
+  }
+
+  // graph offsets, validation, degree, mass, chunks (host)
+  std::vector<uint64_t> goff(G + 1);
+  if (G == 1) {
+    goff[0] = 0;
+    goff[1] = V;
+  } else {
+    for (size_t i = 0; i <= G; i++) goff[i] = g->graphOffsets[i];
+  }
+  if (goff[0] != 0 || goff[G] != V) {
+    delete h;
+    return GVIZ_CUDA_ERR_ARG;
+  }
+  std::vector<uint32_t> gid(G > 1 ? V : 0);
+  for (size_t gg = 0; gg < G; gg++) {
+    if (goff[gg + 1] < goff[gg]) {
+      delete h;
+      return GVIZ_CUDA_ERR_ARG;
+    }
+    if (G > 1)
+      for (uint64_t v = goff[gg]; v < goff[gg + 1]; v++) gid[v] = (uint32_t)gg;
+  }
+  std::vector<uint32_t> row(V + 1), deg(V ? V : 1);
+  std::vector<double> mass(V ? V : 1);
+  std::vector<float> massF(V ? V : 1);
+  for (size_t v = 0; v <= V; v++) row[v] = (uint32_t)(V ? g->rowOffsets[v] : 0);
+  for (size_t v = 0; v < V; v++) {
+    if (g->rowOffsets[v + 1] < g->rowOffsets[v]) {
+      delete h;
+      return GVIZ_CUDA_ERR_ARG;
+    }
+    uint64_t d = g->degree ? g->degree[v] : g->rowOffsets[v + 1] - g->rowOffsets[v];
+    deg[v] = (uint32_t)d;
+    // gvizForceModel vertexMass, src/embedders/gvizForceModel.c:5-8, 31
+    mass[v] = g->model == GVIZ_CUDA_MODEL_FR ? 1.0 : 1.0 + (double)d;
+    massF[v] = (float)mass[v];
+  }
+  for (uint64_t e = 0; e < h->E2; e++) {
+    uint32_t u = g->neighbors[e];
+    if (u >= V) {
+      delete h;
+      return GVIZ_CUDA_ERR_ARG;
+    }
+  }
+  if (G > 1) {  // edges must stay inside their graph
+    for (size_t v = 0; v < V; v++)
+      for (uint64_t e = g->rowOffsets[v]; e < g->rowOffsets[v + 1]; e++)
+        if (gid[g->neighbors[e]] != gid[v]) {
+          delete h;
+          return GVIZ_CUDA_ERR_ARG;
+        }
+  }
+  std::vector<double> mdp(G);
+  for (size_t gg = 0; gg < G; gg++) {
+    // meanDegreePlusOne, src/embedders/gvizForceEmbedder.c:251-259
+    double s = 0.0;
+    for (uint64_t v = goff[gg]; v < goff[gg + 1]; v++) s += (double)(deg[v] + 1);
+    uint64_t n = goff[gg + 1] - goff[gg];
+    mdp[gg] = n ? s / (double)n : 0.0;
+  }
+  std::vector<uint32_t> cb, ce, cg, gcb(G), gce(G);
+  for (size_t gg = 0; gg < G; gg++) {
+    gcb[gg] = (uint32_t)cb.size();
+    for (uint64_t s = goff[gg]; s < goff[gg + 1]; s += GVIZ_CHUNK) {
+      cb.push_back((uint32_t)s);
+      ce.push_back((uint32_t)std::min<uint64_t>(s + GVIZ_CHUNK, goff[gg + 1]));
+      cg.push_back((uint32_t)gg);
+    }
+    gce[gg] = (uint32_t)cb.size();
+  }
+  h->nChunks = (uint32_t)cb.size();
+  h->h_graphOff = (uint64_t *)malloc(sizeof(uint64_t) * (G + 1));
+  h->h_meanDegPlusOne = (double *)malloc(sizeof(double) * G);
+  memcpy(h->h_graphOff, goff.data(), sizeof(uint64_t) * (G + 1));
+  memcpy(h->h_meanDegPlusOne, mdp.data(), sizeof(double) * G);
+
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return GVIZ_CUDA_ERR_CUDA;
+  }
+  h->ownStream = true;
+  const size_t Vs = V ? V : 1;
+  const size_t C = h->nChunks ? h->nChunks : 1;
+  h->maxNodes = 3 * Vs + 64;
+  int rc = 0;
+  rc |= dalloc(h, &h->d_rowOff, V + 1);
+  rc |= dalloc(h, &h->d_cols, h->E2);
+  rc |= dalloc(h, &h->d_degree, Vs);
+  rc |= dalloc(h, &h->d_mass, Vs);
+  rc |= dalloc(h, &h->d_massF, Vs);
+  rc |= dalloc(h, &h->d_radius, Vs);
+  rc |= dalloc(h, &h->d_radiusF, Vs);
+  if (G > 1) rc |= dalloc(h, &h->d_gid, Vs);
+  rc |= dalloc(h, &h->d_graphOff, G + 1);
+  rc |= dalloc(h, &h->d_meanDegPlusOne, G);
+  rc |= dalloc(h, &h->d_chunkBegin, C);
+  rc |= dalloc(h, &h->d_chunkEnd, C);
+  rc |= dalloc(h, &h->d_chunkGraph, C);
+  rc |= dalloc(h, &h->d_gChunkBegin, G);
+  rc |= dalloc(h, &h->d_gChunkEnd, G);
+  rc |= dalloc(h, &h->d_pos, Vs);
+  rc |= dalloc(h, &h->d_sf, Vs);
+  rc |= dalloc(h, &h->d_sfOld, Vs);
+  rc |= dalloc(h, &h->d_disp, Vs);
+  rc |= dalloc(h, &h->d_applied, Vs);
+  rc |= dalloc(h, &h->d_att, Vs);
+  rc |= dalloc(h, &h->d_rep, Vs);
+  rc |= dalloc(h, &h->d_swing, Vs);
+  rc |= dalloc(h, &h->d_trac, Vs);
+  rc |= dalloc(h, &h->d_attF, Vs);
+  rc |= dalloc(h, &h->d_attD, Vs);
+  rc |= dalloc(h, &h->d_speed, G);
+  rc |= dalloc(h, &h->d_eff, G);
+  rc |= dalloc(h, &h->d_active, G);
+  rc |= dalloc(h, &h->d_anyActive, 1);
+  rc |= dalloc(h, &h->d_iter, G);
+  rc |= dalloc(h, &h->d_runLeft, G);
+  rc |= dalloc(h, &h->d_runEps, G);
+  rc |= dalloc(h, &h->d_stats, (size_t)GVIZ_STATS_CAP * G * 5);
+  rc |= dalloc(h, &h->d_lastStats, G * 5);
+  rc |= dalloc(h, &h->d_chunkStat, C);
+  rc |= dalloc(h, &h->d_status, 1);
+  rc |= dalloc(h, &h->d_chunkBox, C);
+  rc |= dalloc(h, &h->d_roots, G);
+  rc |= dalloc(h, &h->d_keyHi, Vs);
+  rc |= dalloc(h, &h->d_keyLo, Vs);
+  rc |= dalloc(h, &h->d_ck, Vs);
+  rc |= dalloc(h, &h->d_ckAlt, Vs);
+  rc |= dalloc(h, &h->d_idx, Vs);
+  rc |= dalloc(h, &h->d_idxAlt, Vs);
+  rc |= dalloc(h, &h->d_sHi, Vs);
+  rc |= dalloc(h, &h->d_sLo, Vs);
+  rc |= dalloc(h, &h->d_flag, Vs);
+  rc |= dalloc(h, &h->d_scan, Vs);
+  rc |= dalloc(h, &h->d_runStart, Vs);
+  rc |= dalloc(h, &h->d_deepRuns, 2 * Vs);
+  rc |= dalloc(h, &h->d_counts, 8);
+  rc |= dalloc(h, &h->d_radixHist, radix_hist_entries(Vs));
+  rc |= dalloc(h, &h->d_scanTile,
+               std::max(scan_scratch_entries(radix_hist_entries(Vs)),
+                        scan_scratch_entries(2 * Vs + G)));
+  rc |= dalloc(h, &h->d_bHi, Vs);
+  rc |= dalloc(h, &h->d_bLo, Vs);
+  rc |= dalloc(h, &h->d_bGid, Vs);
+  rc |= dalloc(h, &h->d_bStart, Vs);
+  rc |= dalloc(h, &h->d_nLeft, Vs);
+  rc |= dalloc(h, &h->d_nRight, Vs);
+  rc |= dalloc(h, &h->d_nFirst, Vs);
+  rc |= dalloc(h, &h->d_nLast, Vs);
+  rc |= dalloc(h, &h->d_nDelta, Vs);
+  rc |= dalloc(h, &h->d_nCounter, Vs);
+  rc |= dalloc(h, &h->d_upInt, Vs);
+  rc |= dalloc(h, &h->d_upLeaf, Vs);
+  rc |= dalloc(h, &h->d_nM, Vs);
+  rc |= dalloc(h, &h->d_nSX, Vs);
+  rc |= dalloc(h, &h->d_nSY, Vs);
+  rc |= dalloc(h, &h->d_nCnt, Vs);
+  rc |= dalloc(h, &h->d_nT, Vs);
+  rc |= dalloc(h, &h->d_nFlag, Vs);
+  rc |= dalloc(h, &h->d_bM, Vs);
+  rc |= dalloc(h, &h->d_bSX, Vs);
+  rc |= dalloc(h, &h->d_bSY, Vs);
+  rc |= dalloc(h, &h->d_bCnt, Vs);
+  rc |= dalloc(h, &h->d_bT, Vs);
+  rc |= dalloc(h, &h->d_rootNode, G);
+  rc |= dalloc(h, &h->d_rootT, G);
+  rc |= dalloc(h, &h->d_graphBase, G);
+  rc |= dalloc(h, &h->d_nodes, h->maxNodes * sizeof(NodeD));
+  rc |= dalloc(h, &h->d_leafDepth, Vs);
+  rc |= dalloc(h, &h->d_counters, 4);
+  if (rc) {
+    gvizCudaForceDestroy(h);
+    return GVIZ_CUDA_ERR_ALLOC;
+  }
+  bool ok = true;
+  auto up = [&](void *dst, const void *src, size_t bytes) {
+    if (bytes && cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) ok = false;
+  };
+  up(h->d_rowOff, row.data(), (V + 1) * 4);
+  if (h->E2) up(h->d_cols, g->neighbors, h->E2 * 4);
+  up(h->d_degree, deg.data(), V * 4);
+  up(h->d_mass, mass.data(), V * 8);
+  up(h->d_massF, massF.data(), V * 4);
+  if (G > 1) up(h->d_gid, gid.data(), V * 4);
+  up(h->d_graphOff, goff.data(), (G + 1) * 8);
+  up(h->d_meanDegPlusOne, mdp.data(), G * 8);
+  up(h->d_chunkBegin, cb.data(), cb.size() * 4);
+  up(h->d_chunkEnd, ce.data(), ce.size() * 4);
+  up(h->d_chunkGraph, cg.data(), cg.size() * 4);
+  up(h->d_gChunkBegin, gcb.data(), G * 4);
+  up(h->d_gChunkEnd, gce.data(), G * 4);
+  ok = ok && cudaMemset(h->d_nCounter, 0, Vs * 4) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_pos, 0, Vs * 16) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_counters, 0, 32) == cudaSuccess;
+  if (!ok || upload_dir_table(h) || upload_radius(h)) {
+    gvizCudaForceDestroy(h);
+    return GVIZ_CUDA_ERR_CUDA;
+  }
+  tree_set_smem_limits();
+  for (int i = 0; i < 65; i++) cudaEventCreate(&h->profEv[i]);
+  // Init leaves the FA2 state zeroed (src/embedders/gvizForceEmbedder.c:221);
+  // Begin sets it up.
+  ok = cudaMemset(h->d_speed, 0, G * 8) == cudaSuccess &&
+       cudaMemset(h->d_eff, 0, G * 8) == cudaSuccess &&
+       cudaMemset(h->d_sf, 0, Vs * 16) == cudaSuccess &&
+       cudaMemset(h->d_iter, 0, G * 8) == cudaSuccess &&
+       cudaMemset(h->d_lastStats, 0, G * 40) == cudaSuccess;
+  if (!ok) {
+    gvizCudaForceDestroy(h);
+    return GVIZ_CUDA_ERR_CUDA;
+  }
+  set_all_active(h, ~0ull, -INFINITY);
+  *out = h;
+  return GVIZ_CUDA_OK;
+}
+
+void gvizCudaForceDestroy(gvizCudaForce *h) {
+  if (!h) return;
+  DeviceGuard guard(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->stepExec) cudaGraphExecDestroy(h->stepExec);
+  for (int i = 0; i < 65; i++)
+    if (h->profEv[i]) cudaEventDestroy(h->profEv[i]);
+  free_all(h);
+  mlp_free(h);
+  if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
+  free(h->h_graphOff);
+  free(h->h_meanDegPlusOne);
+  delete h;
+}
+
+int gvizCudaForceSetParams(gvizCudaForce *h, const gvizCudaForceParams *p) {
+  if (!h || !p) return GVIZ_CUDA_ERR_ARG;
+  if (p->nodesPerCell < 1 || p->nodesPerCell > GVIZ_MAX_NODES_PER_CELL)
+    return set_err(h, GVIZ_CUDA_ERR_LIMIT);
+  if (!(p->theta > 0.0) || !(p->edgeLength > 0.0) ||
+      (p->precision != GVIZ_CUDA_FP32 && p->precision != GVIZ_CUDA_FP64))
+    return set_err(h, GVIZ_CUDA_ERR_ARG);
+  if (p->farField && !h->d_mlp) return set_err(h, GVIZ_CUDA_ERR_ARG);
+  DeviceGuard guard(h->device);
+  const bool radiusChanged = p->preventOverlap != h->params.preventOverlap ||
+                             p->radiusBase != h->params.radiusBase ||
+                             p->radiusPerDegree != h->params.radiusPerDegree;
+  h->params = *p;
+  h->graphDirty = true;
+  if (radiusChanged) return upload_radius(h);
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceGetParams(const gvizCudaForce *h, gvizCudaForceParams *p) {
+  if (!h || !p) return GVIZ_CUDA_ERR_ARG;
+  *p = h->params;
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceSetPositions(gvizCudaForce *h, const double *xy) {
+  if (!h || (!xy && h->V)) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (!h->V) return GVIZ_CUDA_OK;
+  if (cudaMemcpyAsync(h->d_pos, xy, h->V * 16, cudaMemcpyHostToDevice, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceGetPositions(gvizCudaForce *h, double *xy) {
+  if (!h || (!xy && h->V)) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (!h->V) return GVIZ_CUDA_OK;
+  if (cudaMemcpyAsync(xy, h->d_pos, h->V * 16, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess ||
+      cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceBegin(gvizCudaForce *h) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  std::vector<double> one(h->G, 1.0);
+  bool ok = cudaMemcpy(h->d_speed, one.data(), h->G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemcpy(h->d_eff, one.data(), h->G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_sf, 0, (h->V ? h->V : 1) * 16) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_disp, 0, (h->V ? h->V : 1) * 16) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_iter, 0, h->G * 8) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_lastStats, 0, h->G * 40) == cudaSuccess;
+  if (!ok) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  set_all_active(h, ~0ull, -INFINITY);
+  h->begun = true;
+  h->hostIteration = 0;
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceSetFa2State(gvizCudaForce *h, const double *sf,
+                             const double *speed, const double *eff) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  bool ok = true;
+  if (sf && h->V) ok = cudaMemcpy(h->d_sf, sf, h->V * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+  if (speed) ok = ok && cudaMemcpy(h->d_speed, speed, h->G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  if (eff) ok = ok && cudaMemcpy(h->d_eff, eff, h->G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  return ok ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_CUDA);
+}
+
+int gvizCudaForceGetFa2State(gvizCudaForce *h, double *sf, double *speed,
+                             double *eff) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  bool ok = true;
+  if (sf && h->V) ok = cudaMemcpy(sf, h->d_sf, h->V * 16, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (speed) ok = ok && cudaMemcpy(speed, h->d_speed, h->G * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (eff) ok = ok && cudaMemcpy(eff, h->d_eff, h->G * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  return ok ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_CUDA);
+}
+
+double gvizCudaForceStep(gvizCudaForce *h, gvizCudaStepStats *stats) {
+  if (!h) return (double)GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return (double)set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  if (h->V == 0) {
+    // the reference still appends stats for an empty graph
+    if (stats)
+      for (size_t g = 0; g < h->G; g++) {
+        memset(&stats[g], 0, sizeof(stats[g]));
+        stats[g].speed = 1.0;
+      }
+    return 0.0;
+  }
+  int rc = launch_steps(h, 1);
+  if (rc) return (double)rc;
+  rc = sync_and_check(h);
+  h->hostIteration++;
+  double md = fill_stats(h, stats);
+  return rc ? (double)rc : md;
+}
+
+double gvizCudaForceStepHost(gvizCudaForce *h, double *xy,
+                             gvizCudaStepStats *stats) {
+  if (!h || (!xy && h->V)) return (double)GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return (double)set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  if (h->V == 0) return gvizCudaForceStep(h, stats);
+  if (cudaMemcpyAsync(h->d_pos, xy, h->V * 16, cudaMemcpyHostToDevice, h->stream) != cudaSuccess)
+    return (double)set_err(h, GVIZ_CUDA_ERR_CUDA);
+  int rc = launch_steps(h, 1);
+  if (rc) return (double)rc;
+  if (cudaMemcpyAsync(xy, h->d_pos, h->V * 16, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+    return (double)set_err(h, GVIZ_CUDA_ERR_CUDA);
+  rc = sync_and_check(h);
+  h->hostIteration++;
+  double md = fill_stats(h, stats);
+  return rc ? (double)rc : md;
+}
+
+int gvizCudaForceEnqueueSteps(gvizCudaForce *h, uint32_t n) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  int rc = launch_steps(h, n);
+  if (!rc) h->hostIteration += n;
+  return rc;
+}
+
+int gvizCudaForceSynchronize(gvizCudaForce *h) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  return sync_and_check(h);
+}
+
+int gvizCudaForceRun(gvizCudaForce *h, size_t maxIters, double epsilon,
+                     uint64_t *rounds) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  std::vector<uint64_t> it0(h->G), it1(h->G);
+  cudaMemcpy(it0.data(), h->d_iter, h->G * 8, cudaMemcpyDeviceToHost);
+  if (maxIters > 0 && h->V > 0) {
+    set_all_active(h, maxIters, epsilon);
+    size_t launched = 0;
+    while (launched < maxIters) {
+      uint32_t n = (uint32_t)std::min<size_t>(kRunBatch, maxIters - launched);
+      int rc = launch_steps(h, n);
+      if (rc) return rc;
+      launched += n;
+      uint32_t any = 0;
+      if (cudaMemcpyAsync(&any, h->d_anyActive, 4, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+        return set_err(h, GVIZ_CUDA_ERR_CUDA);
+      int sc = sync_and_check(h);
+      if (sc) return sc;
+      if (any == 0) break;
+    }
+    set_all_active(h, ~0ull, -INFINITY);
+  }
+  cudaMemcpy(it1.data(), h->d_iter, h->G * 8, cudaMemcpyDeviceToHost);
+  if (rounds)
+    for (size_t g = 0; g < h->G; g++) rounds[g] = it1[g] - it0[g];
+  h->hostIteration += it1[0] - it0[0];
+  return GVIZ_CUDA_OK;
+}
+
+int64_t gvizCudaForceStatHistory(gvizCudaForce *h, uint32_t graph, double *out,
+                                 size_t cap) {
+  if (!h || graph >= h->G) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  cudaStreamSynchronize(h->stream);
+  uint64_t it = 0;
+  cudaMemcpy(&it, h->d_iter + graph, 8, cudaMemcpyDeviceToHost);
+  const uint64_t kept = std::min<uint64_t>(it, GVIZ_STATS_CAP);
+  const uint64_t first = it - kept;
+  uint64_t w = 0;
+  for (uint64_t s = first; s < it && w < cap; s++, w++) {
+    const size_t rowIdx = (size_t)(s % GVIZ_STATS_CAP);
+    if (out)
+      cudaMemcpy(out + 5 * w, h->d_stats + (rowIdx * h->G + graph) * 5,
+                 5 * sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  return (int64_t)kept;
+}
+
+int gvizCudaForceGetForces(gvizCudaForce *h, double *disp, double *sf,
+                           double *att, double *rep, double *swing,
+                           double *trac, double *applied) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  const size_t V = h->V;
+  if (!V) return GVIZ_CUDA_OK;
+  bool ok = true;
+  auto dn = [&](void *dst, const void *src, size_t bytes) {
+    if (dst && cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
+  };
+  dn(disp, h->d_disp, V * 16);
+  dn(sf, h->d_sf, V * 16);
+  dn(att, h->d_att, V * 8);
+  dn(rep, h->d_rep, V * 8);
+  dn(swing, h->d_swing, V * 8);
+  dn(trac, h->d_trac, V * 8);
+  dn(applied, h->d_applied, V * 16);
+  return ok ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_CUDA);
+}
+
+static uint64_t mask_hi(int d) {
+  if (d <= 0) return 0;
+  if (d >= 32) return ~0ull;
+  return ~0ull << (64 - 2 * d);
+}
+static uint64_t mask_lo(int d) {
+  if (d <= 32) return 0;
+  if (d >= 64) return ~0ull;
+  return ~0ull << (128 - 2 * d);
+}
+
+int gvizCudaForceTreeLeaves(gvizCudaForce *h, int32_t *leafDepth,
+                            uint64_t *pathHi, uint64_t *pathLo,
+                            uint64_t *nodeCount) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  const size_t V = h->V;
+  if (V == 0) {
+    if (nodeCount) *nodeCount = 0;
+    return GVIZ_CUDA_OK;
+  }
+  cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+  enqueue_tree_build(h);
+  enqueue_tree_export(h, (int32_t *)h->d_leafDepth);
+  int rc = sync_and_check(h);
+  if (rc) return rc;
+  std::vector<int32_t> depth(V);
+  std::vector<uint64_t> hi(V), lo(V);
+  std::vector<uint32_t> idx(V);
+  uint32_t counts[8];
+  bool ok = cudaMemcpy(depth.data(), h->d_leafDepth, V * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(hi.data(), h->d_sHi, V * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(lo.data(), h->d_sLo, V * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(idx.data(), h->d_idx, V * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(counts, h->d_counts, 32, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (!ok) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  for (size_t s = 0; s < V; s++) {
+    const uint32_t v = idx[s];
+    const int d = depth[v];
+    if (leafDepth) leafDepth[v] = d;
+    if (pathHi) pathHi[v] = hi[s] & mask_hi(d);
+    if (pathLo) pathLo[v] = lo[s] & mask_lo(d);
+  }
+  if (nodeCount) *nodeCount = counts[3];
+  return GVIZ_CUDA_OK;
+}
+
+int64_t gvizCudaForceTreeNodes(gvizCudaForce *h, size_t cap, int32_t *depth,
+                               uint64_t *pathHi, uint64_t *pathLo,
+                               double *mass, double *comX, double *comY,
+                               uint64_t *count) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (h->V == 0) return 0;
+  const size_t M = h->maxNodes;
+  int32_t *dd = nullptr;
+  uint64_t *dh = nullptr, *dl = nullptr, *dc = nullptr;
+  double *dm = nullptr, *dx = nullptr, *dy = nullptr;
+  int rc = 0;
+  rc |= dalloc(h, &dd, M);
+  rc |= dalloc(h, &dh, M);
+  rc |= dalloc(h, &dl, M);
+  rc |= dalloc(h, &dc, M);
+  rc |= dalloc(h, &dm, M);
+  rc |= dalloc(h, &dx, M);
+  rc |= dalloc(h, &dy, M);
+  int64_t w = 0;
+  if (!rc) {
+    cudaMemsetAsync(dd, 0xff, M * 4, h->stream);
+    cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+    enqueue_tree_build(h);
+    enqueue_cell_dump(h, dd, dh, dl, dm, dx, dy, dc);
+    rc = sync_and_check(h);
+    if (!rc) {
+      std::vector<int32_t> D(M);
+      std::vector<uint64_t> H(M), L(M), Cn(M);
+      std::vector<double> Ms(M), X(M), Y(M);
+      cudaMemcpy(D.data(), dd, M * 4, cudaMemcpyDeviceToHost);
+      cudaMemcpy(H.data(), dh, M * 8, cudaMemcpyDeviceToHost);
+      cudaMemcpy(L.data(), dl, M * 8, cudaMemcpyDeviceToHost);
+      cudaMemcpy(Cn.data(), dc, M * 8, cudaMemcpyDeviceToHost);
+      cudaMemcpy(Ms.data(), dm, M * 8, cudaMemcpyDeviceToHost);
+      cudaMemcpy(X.data(), dx, M * 8, cudaMemcpyDeviceToHost);
+      cudaMemcpy(Y.data(), dy, M * 8, cudaMemcpyDeviceToHost);
+      for (size_t i = 0; i < M; i++) {
+        if (D[i] < 0) continue;
+        if ((size_t)w < cap) {
+          if (depth) depth[w] = D[i];
+          if (pathHi) pathHi[w] = H[i];
+          if (pathLo) pathLo[w] = L[i];
+          if (mass) mass[w] = Ms[i];
+          if (comX) comX[w] = X[i];
+          if (comY) comY[w] = Y[i];
+          if (count) count[w] = Cn[i];
+        }
+        w++;
+      }
+    }
+  }
+  dfree(dd);
+  dfree(dh);
+  dfree(dl);
+  dfree(dc);
+  dfree(dm);
+  dfree(dx);
+  dfree(dy);
+  return rc ? (int64_t)rc : w;
+}
+
+int gvizCudaForceExactRepulsion(gvizCudaForce *h, const uint32_t *targets,
+                                size_t n, double *out) {
+  if (!h || (n && (!targets || !out))) return GVIZ_CUDA_ERR_ARG;
+  if (n == 0) return GVIZ_CUDA_OK;
+  for (size_t i = 0; i < n; i++)
+    if (targets[i] >= h->V) return set_err(h, GVIZ_CUDA_ERR_ARG);
+  DeviceGuard guard(h->device);
+  uint32_t *dt = nullptr;
+  double2 *dout = nullptr;
+  int rc = dalloc(h, &dt, n) | dalloc(h, &dout, n);
+  if (!rc) {
+    cudaMemcpy(dt, targets, n * 4, cudaMemcpyHostToDevice);
+    enqueue_exact_judge(h, dt, n, dout);
+    rc = sync_and_check(h);
+    if (!rc && cudaMemcpy(out, dout, n * 16, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = set_err(h, GVIZ_CUDA_ERR_CUDA);
+  }
+  dfree(dt);
+  dfree(dout);
+  return rc;
+}
+
+int gvizCudaForceRepulsion(gvizCudaForce *h, double *out) {
+  if (!h || (!out && h->V)) return GVIZ_CUDA_ERR_ARG;
+  if (h->V == 0) return GVIZ_CUDA_OK;
+  DeviceGuard guard(h->device);
+  double2 *dv = nullptr;
+  int rc = dalloc(h, &dv, h->V);
+  if (!rc) {
+    h->forceOnly = true;
+    h->repVecOut = dv;
+    cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+    enqueue_step(h);
+    h->forceOnly = false;
+    h->repVecOut = nullptr;
+    rc = sync_and_check(h);
+    if (!rc && cudaMemcpy(out, dv, h->V * 16, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = set_err(h, GVIZ_CUDA_ERR_CUDA);
+  }
+  dfree(dv);
+  return rc;
+}
+
+int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
+                                   uint64_t *warpNodeVisits) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (h->V == 0 || !h->params.barnesHutEnabled) {
+    const uint64_t n = h->V;
+    if (interactions) *interactions = h->params.barnesHutEnabled ? 0 : n * (n ? n - 1 : 0);
+    if (warpNodeVisits) *warpNodeVisits = 0;
+    return GVIZ_CUDA_OK;
+  }
+  const gvizCudaForceParams saved = h->params;
+  h->params.precision = GVIZ_CUDA_FP32;
+  h->forceOnly = true;
+  cudaMemsetAsync(h->d_counters, 0, 32, h->stream);
+  cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+  enqueue_tree_build(h);
+  enqueue_attraction_f32(h);
+  enqueue_walk_f32(h, h->d_counters);
+  h->forceOnly = false;
+  h->params = saved;
+  int rc = sync_and_check(h);
+  uint64_t c[2] = {0, 0};
+  cudaMemcpy(c, h->d_counters, 16, cudaMemcpyDeviceToHost);
+  if (interactions) *interactions = c[0];
+  if (warpNodeVisits) *warpNodeVisits = c[1];
+  return rc;
+}
+
+int gvizCudaForceProfileStep(gvizCudaForce *h, size_t cap, const char **names,
+                             double *ms) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  if (h->V == 0) return 0;
+  h->profiling = true;
+  h->nProf = 0;
+  cudaEventRecord(h->profEv[0], h->stream);
+  enqueue_step(h);
+  h->profiling = false;
+  int rc = sync_and_check(h);
+  h->hostIteration++;
+  if (rc) return rc;
+  int n = h->nProf;
+  for (int i = 0; i < n && (size_t)i < cap; i++) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, h->profEv[i], h->profEv[i + 1]);
+    if (names) names[i] = h->profName[i];
+    if (ms) ms[i] = t;
+  }
+  return n;
+}
+
+int gvizCudaForceTimeSteps(gvizCudaForce *h, uint32_t n, float *ms) {
+  if (!h || !ms) return GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  *ms = 0.f;
+  if (h->V == 0 || n == 0) return GVIZ_CUDA_OK;
+  int rc = ensure_graph(h);
+  if (rc) return rc;
+  cudaEventRecord(h->profEv[0], h->stream);
+  rc = launch_steps(h, n);
+  if (rc) return rc;
+  cudaEventRecord(h->profEv[1], h->stream);
+  rc = sync_and_check(h);
+  h->hostIteration += n;
+  if (rc) return rc;
+  cudaEventElapsedTime(ms, h->profEv[0], h->profEv[1]);
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceStepKernelCount(gvizCudaForce *h) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (h->V == 0) return 0;
+  DeviceGuard guard(h->device);
+  int rc = ensure_graph(h);
+  return rc ? rc : h->kernelsPerStep;
+}
+
+int gvizCudaForceLastError(const gvizCudaForce *h) {
+  return h ? h->lastError : GVIZ_CUDA_ERR_ARG;
+}
+
+const char *gvizCudaErrorString(int code) {
+  switch (code) {
+    case GVIZ_CUDA_OK: return "ok";
+    case GVIZ_CUDA_ERR_ALLOC: return "allocation failed";
+    case GVIZ_CUDA_ERR_DIMENSION: return "only 2-D layouts are supported";
+    case GVIZ_CUDA_ERR_ARG: return "invalid argument";
+    case GVIZ_CUDA_ERR_CUDA: return "CUDA runtime error";
+    case GVIZ_CUDA_ERR_NOT_BEGUN: return "Begin has not been called";
+    case GVIZ_CUDA_ERR_NONFINITE: return "a vertex position is NaN or infinite";
+    case GVIZ_CUDA_ERR_DEEP_RUN: return "more than 4096 distinct points share one depth-32 quadtree cell";
+    case GVIZ_CUDA_ERR_NO_DEVICE: return "no usable CUDA device";
+    case GVIZ_CUDA_ERR_LIMIT: return "size beyond a supported limit";
+    default: return "unknown error";
+  }
+}
+
+int gvizCudaForceSetStream(gvizCudaForce *h, void *stream) {
+  if (!h || !stream) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  cudaStreamSynchronize(h->stream);
+  if (h->ownStream) cudaStreamDestroy(h->stream);
+  h->stream = (cudaStream_t)stream;
+  h->ownStream = false;
+  h->graphDirty = true;
+  return GVIZ_CUDA_OK;
+}
+
+}  // extern "C"

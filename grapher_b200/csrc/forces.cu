@@ -1,0 +1,367 @@
+// forces.cu -- FP32 force kernels (compiled with fused multiply-add).
+//
+//  * k_attr_f32: edge attraction over CSR (src/embedders/gvizForceEmbedder.c:93-100;
+//    FR include/core/gvizVec.h:320-334, LinLog :486-499).
+//  * k_walk_f32: Barnes-Hut repulsion (src/embedders/gvizForceEmbedder.c:35-74)
+//    as a warp-shared stackless traversal of the preorder tree: the 32 lanes
+//    of a warp hold 32 path-sorted (hence nearby) vertices and step through
+//    the union of the nodes they need, every lane making the reference's own
+//    accept / open / pairwise decision. Node records are read once per warp
+//    (one broadcast), the next node is the warp minimum of each lane's next.
+//  * k_exact_f32: exact all-pairs repulsion (:104-115), shared-memory tiles.
+//
+// Geometry is double-single: a coordinate is hi + lo floats, so a difference
+// (ah - bh) + (al - bl) keeps ~FP32 relative accuracy even at |x| ~ 1e3.
+// Per-vertex sums are Kahan-compensated FP32; the epilogue is FP64.
+#include <math.h>
+
+#include "epilogue.cuh"
+#include "internal.cuh"
+
+int dir_table_upload_forces(const double *t) {
+  return cudaMemcpyToSymbol(c_dirTable, t, sizeof(double) * 2 * GVIZ_DIR_TABLE) ==
+                 cudaSuccess ? 0 : -1;
+}
+
+namespace {
+
+constexpr int kWalkThreads = 128;
+constexpr int kAttrThreads = 256;
+constexpr int kExactThreads = 256;
+constexpr int kExactTile = 256;
+constexpr uint32_t kInf = 0xffffffffu;
+
+struct Kahan {
+  float s = 0.f, c = 0.f;
+  __device__ __forceinline__ void add(float x) {
+    float y = x - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const {
+    return (double)s - (double)c;
+  }
+};
+
+struct AttrArgs {
+  const uint32_t *rowOff, *cols, *gid, *active;
+  const double2 *pos;
+  float2 *out;
+  float invK;
+  uint32_t V;
+};
+
+template <int MODEL>
+__global__ __launch_bounds__(kAttrThreads) void k_attr_f32(AttrArgs a) {
+  const uint32_t v = blockIdx.x * kAttrThreads + threadIdx.x;
+  if (v >= a.V) return;
+  if (a.active && !a.active[a.gid ? a.gid[v] : 0u]) return;
+  const double2 p = a.pos[v];
+  Kahan kx, ky;
+  const uint32_t e1 = a.rowOff[v + 1];
+  for (uint32_t e = a.rowOff[v]; e < e1; e++) {
+    const double2 q = a.pos[a.cols[e]];
+    const float dx = (float)(q.x - p.x);
+    const float dy = (float)(q.y - p.y);
+    const float dist = sqrtf(dx * dx + dy * dy);
+    if (dist < 1e-9f) continue;
+    float s;
+    if (MODEL == GVIZ_CUDA_MODEL_FR)
+      s = dist * a.invK;
+    else
+      s = log1pf(dist) / dist;
+    kx.add(s * dx);
+    ky.add(s * dy);
+  }
+  a.out[v] = make_float2((float)kx.value(), (float)ky.value());
+}
+
+struct WalkArgs {
+  const NodeF *nodes;
+  const uint32_t *idx, *gid, *active, *graphBase, *rootT;
+  const double2 *pos;
+  const float *massF, *radiusF;
+  const float2 *attF;
+  EpiArgs epi;
+  float num;     // FR: k^2
+  uint32_t maxNodes;
+  float overlapC;
+  uint32_t V;
+  unsigned long long *counters;  // [0] interactions, [1] warp node visits
+};
+
+// One pair or pseudo-body term of FR / LinLog repulsion
+// (include/core/gvizVec.h:404-428, 552-578; FR mass truncation
+// src/embedders/gvizForceModel.c:20).
+template <int MODEL, bool OVERLAP>
+__device__ __forceinline__ void rep_term(float dx, float dy, float d2,
+                                         float mv, float mo, float radiusSum,
+                                         float num, float C, uint32_t self,
+                                         uint32_t other, float &fx, float &fy) {
+  const float numer = (MODEL == GVIZ_CUDA_MODEL_FR) ? num : mv * mo;
+  const float mult = (MODEL == GVIZ_CUDA_MODEL_FR) ? truncf(mo) : 1.0f;
+  if (d2 > 0.0f) {
+    if (OVERLAP) {
+      const float inv = rsqrtf(d2);
+      const float dist = d2 * inv;
+      const float gap = dist - radiusSum;
+      const float mag = gap > 0.0f ? __fdividef(numer, gap) : numer * C;
+      const float s = mag * inv * mult;
+      fx = -s * dx;
+      fy = -s * dy;
+    } else {
+      const float s = __fdividef(numer, d2) * mult;
+      fx = -s * dx;
+      fy = -s * dy;
+    }
+  } else {
+    double ux, uy;
+    coincident_dir(self, other, ux, uy);
+    const float mag = numer * C * mult;
+    fx = -mag * (float)ux;
+    fy = -mag * (float)uy;
+  }
+}
+
+template <int MODEL, bool OVERLAP, bool COUNT>
+__global__ __launch_bounds__(kWalkThreads) void k_walk_f32(WalkArgs a) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t s = ((blockIdx.x * kWalkThreads + threadIdx.x) >> 5) * 32u + lane;
+  const bool valid = s < a.V;
+  const uint32_t v = valid ? a.idx[s] : 0u;
+  const uint32_t g = (valid && a.gid) ? a.gid[v] : 0u;
+  const bool act = valid && (a.active == nullptr || a.active[g] != 0u);
+  uint32_t resume = 0, myEnd = 0;
+  if (act) {
+    resume = a.graphBase[g];
+    myEnd = min(resume + a.rootT[g], a.maxNodes);
+  }
+  float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
+  if (act) {
+    const double2 p = a.pos[v];
+    ds_split(p.x, vxh, vxl);
+    ds_split(p.y, vyh, vyl);
+    mv = a.massF[v];
+    if (OVERLAP) rv = a.radiusF[v];
+  }
+  Kahan kx, ky;
+  unsigned long long nInter = 0, nVisit = 0;
+  uint32_t nxt = resume < myEnd ? resume : kInf;
+  uint32_t cur = __reduce_min_sync(0xffffffffu, nxt);
+  while (cur != kInf) {
+    const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
+    const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+    const float nmass = n1.x, nsize = n1.y;
+    const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
+    const bool active = cur >= resume && cur < myEnd;
+    const float dx = (n0.x - vxh) + (n0.z - vxl);
+    const float dy = (n0.y - vyh) + (n0.w - vyl);
+    const float d2 = dx * dx + dy * dy;
+    const bool isLeaf = ninfo >= 0;
+    const bool massOk = nmass != 0.0f;
+    const bool accept = !isLeaf && nsize < d2;
+    const bool doForce =
+        active && massOk && (isLeaf ? ((uint32_t)ninfo != v) : accept);
+    const bool open = active && massOk && !isLeaf && !accept;
+    if (__any_sync(0xffffffffu, doForce)) {
+      if (doForce) {
+        float fx, fy;
+        rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass,
+                                 rv + (isLeaf ? nsize : 0.0f), a.num,
+                                 a.overlapC, v, isLeaf ? (uint32_t)ninfo : v,
+                                 fx, fy);
+        kx.add(fx);
+        ky.add(fy);
+        if (COUNT) nInter++;
+      }
+    }
+    if (active) resume = open ? cur + 1u : max((uint32_t)nnext, cur + 1u);
+    nxt = resume < myEnd ? resume : kInf;
+    if (COUNT) nVisit++;
+    cur = __reduce_min_sync(0xffffffffu, nxt);
+  }
+  if (COUNT) {
+    atomicAdd(a.counters, nInter);
+    if (lane == 0) atomicAdd(a.counters + 1, nVisit);
+  }
+  if (!act) return;
+  const float2 at = a.attF[v];
+  force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value(), ky.value());
+}
+
+struct ExactArgs {
+  const double2 *pos;
+  const float *massF, *radiusF;
+  const uint32_t *gid, *active;
+  const uint64_t *graphOff;
+  const float2 *attF;
+  EpiArgs epi;
+  float num, overlapC;
+  uint32_t V;
+};
+
+template <int MODEL, bool OVERLAP>
+__global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
+  __shared__ float4 sp[kExactTile];
+  __shared__ float2 sm[kExactTile];
+  __shared__ uint32_t sRange[2];
+  const uint32_t v = blockIdx.x * kExactThreads + threadIdx.x;
+  const bool valid = v < a.V;
+  const uint32_t g = (valid && a.gid) ? a.gid[v] : 0u;
+  const bool act = valid && (a.active == nullptr || a.active[g] != 0u);
+  uint32_t gb = 0, ge = 0;
+  if (act) {
+    gb = (uint32_t)a.graphOff[g];
+    ge = (uint32_t)a.graphOff[g + 1];
+  }
+  if (threadIdx.x == 0) {
+    sRange[0] = kInf;
+    sRange[1] = 0;
+  }
+  __syncthreads();
+  if (act) {
+    atomicMin(&sRange[0], gb);
+    atomicMax(&sRange[1], ge);
+  }
+  __syncthreads();
+  const uint32_t lo = sRange[0], hi = sRange[1];
+  float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
+  if (act) {
+    const double2 p = a.pos[v];
+    ds_split(p.x, vxh, vxl);
+    ds_split(p.y, vyh, vyl);
+    mv = a.massF[v];
+    if (OVERLAP) rv = a.radiusF[v];
+  }
+  Kahan kx, ky;
+  for (uint32_t t0 = lo; t0 < hi; t0 += kExactTile) {
+    __syncthreads();
+    const uint32_t j = t0 + threadIdx.x;
+    if (threadIdx.x < kExactTile) {
+      if (j < hi) {
+        const double2 q = a.pos[j];
+        float4 f;
+        ds_split(q.x, f.x, f.z);
+        ds_split(q.y, f.y, f.w);
+        sp[threadIdx.x] = f;
+        sm[threadIdx.x] = make_float2(a.massF[j], OVERLAP ? a.radiusF[j] : 0.f);
+      }
+    }
+    __syncthreads();
+    const uint32_t cnt = min((uint32_t)kExactTile, hi - t0);
+    if (act) {
+#pragma unroll 4
+      for (uint32_t q = 0; q < cnt; q++) {
+        const uint32_t jj = t0 + q;
+        if (jj == v || jj < gb || jj >= ge) continue;
+        const float4 f = sp[q];
+        const float2 m = sm[q];
+        const float dx = (f.x - vxh) + (f.z - vxl);
+        const float dy = (f.y - vyh) + (f.w - vyl);
+        const float d2 = dx * dx + dy * dy;
+        float fx, fy;
+        rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, m.x, rv + m.y, a.num,
+                                 a.overlapC, v, jj, fx, fy);
+        kx.add(fx);
+        ky.add(fy);
+      }
+    }
+  }
+  if (!act) return;
+  const float2 at = a.attF[v];
+  force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value(), ky.value());
+}
+
+inline uint32_t blocks(size_t n, int t) { return (uint32_t)((n + t - 1) / t); }
+
+}  // namespace
+
+void enqueue_attraction_f32(gvizCudaForce *h) {
+  AttrArgs a;
+  a.rowOff = h->d_rowOff;
+  a.cols = h->d_cols;
+  a.gid = h->d_gid;
+  a.active = h->d_active;
+  a.pos = h->d_pos;
+  a.out = h->d_attF;
+  a.invK = (float)(1.0 / h->params.edgeLength);
+  a.V = (uint32_t)h->V;
+  if (h->model == GVIZ_CUDA_MODEL_FR)
+    k_attr_f32<GVIZ_CUDA_MODEL_FR><<<blocks(h->V, kAttrThreads), kAttrThreads, 0, h->stream>>>(a);
+  else
+    k_attr_f32<GVIZ_CUDA_MODEL_LINLOG><<<blocks(h->V, kAttrThreads), kAttrThreads, 0, h->stream>>>(a);
+  prof_mark(h, "attraction_f32");
+}
+
+template <int MODEL, bool OVERLAP, bool COUNT>
+static void launch_walk(gvizCudaForce *h, const WalkArgs &a) {
+  uint32_t warps = (uint32_t)((h->V + 31) / 32);
+  uint32_t grid = blocks((size_t)warps * 32, kWalkThreads);
+  k_walk_f32<MODEL, OVERLAP, COUNT><<<grid, kWalkThreads, 0, h->stream>>>(a);
+}
+
+void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
+  WalkArgs a;
+  a.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
+  a.idx = h->d_idx;
+  a.gid = h->d_gid;
+  a.active = h->d_active;
+  a.graphBase = h->d_graphBase;
+  a.rootT = h->d_rootT;
+  a.pos = h->d_pos;
+  a.massF = h->d_massF;
+  a.radiusF = h->d_radiusF;
+  a.attF = h->d_attF;
+  a.epi = make_epi(h);
+  a.num = (float)(h->params.edgeLength * h->params.edgeLength);
+  a.overlapC = (float)h->params.overlapConstant;
+  a.V = (uint32_t)h->V;
+  a.counters = reinterpret_cast<unsigned long long *>(counters);
+  a.maxNodes = (uint32_t)h->maxNodes;
+  const bool ov = h->params.preventOverlap != 0;
+  const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
+  if (counters) {
+    if (fr) {
+      if (ov) launch_walk<GVIZ_CUDA_MODEL_FR, true, true>(h, a);
+      else launch_walk<GVIZ_CUDA_MODEL_FR, false, true>(h, a);
+    } else {
+      if (ov) launch_walk<GVIZ_CUDA_MODEL_LINLOG, true, true>(h, a);
+      else launch_walk<GVIZ_CUDA_MODEL_LINLOG, false, true>(h, a);
+    }
+  } else {
+    if (fr) {
+      if (ov) launch_walk<GVIZ_CUDA_MODEL_FR, true, false>(h, a);
+      else launch_walk<GVIZ_CUDA_MODEL_FR, false, false>(h, a);
+    } else {
+      if (ov) launch_walk<GVIZ_CUDA_MODEL_LINLOG, true, false>(h, a);
+      else launch_walk<GVIZ_CUDA_MODEL_LINLOG, false, false>(h, a);
+    }
+  }
+  prof_mark(h, "bh_walk_f32");
+}
+
+void enqueue_exact_f32(gvizCudaForce *h) {
+  ExactArgs a;
+  a.pos = h->d_pos;
+  a.massF = h->d_massF;
+  a.radiusF = h->d_radiusF;
+  a.gid = h->d_gid;
+  a.active = h->d_active;
+  a.graphOff = h->d_graphOff;
+  a.attF = h->d_attF;
+  a.epi = make_epi(h);
+  a.num = (float)(h->params.edgeLength * h->params.edgeLength);
+  a.overlapC = (float)h->params.overlapConstant;
+  a.V = (uint32_t)h->V;
+  const uint32_t grid = blocks(h->V, kExactThreads);
+  const bool ov = h->params.preventOverlap != 0;
+  if (h->model == GVIZ_CUDA_MODEL_FR) {
+    if (ov) k_exact_f32<GVIZ_CUDA_MODEL_FR, true><<<grid, kExactThreads, 0, h->stream>>>(a);
+    else k_exact_f32<GVIZ_CUDA_MODEL_FR, false><<<grid, kExactThreads, 0, h->stream>>>(a);
+  } else {
+    if (ov) k_exact_f32<GVIZ_CUDA_MODEL_LINLOG, true><<<grid, kExactThreads, 0, h->stream>>>(a);
+    else k_exact_f32<GVIZ_CUDA_MODEL_LINLOG, false><<<grid, kExactThreads, 0, h->stream>>>(a);
+  }
+  prof_mark(h, "exact_f32");
+}

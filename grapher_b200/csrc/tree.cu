@@ -1,0 +1,889 @@
+// tree.cu -- device rebuild of gviz's quadtree (src/ds/gvizQuadtree.c) as a
+// compressed, preorder-laid-out tree whose leaves hold exactly the point
+// sets of the reference's leaves.
+//
+// Pipeline (one launch each, no host synchronisation):
+//   bbox per chunk -> square root box per graph (gvizQuadtree.c:165-178)
+//   per point: quadrant path by replaying the reference's FP64 descent
+//     (QuadrantFor :65-73 against centres cx +/- halfSize/2, Subdivide :75-92)
+//   stable radix sort of (graph, path) -> fix-up sort of equal-prefix runs
+//   buckets = identical full paths -> Karras binary radix tree (2012)
+//   binary nodes merged into quadtree nodes (two path bits per level)
+//   bottom-up mass / centre-of-mass / subtree sizes (atomic counters)
+//   preorder index by walking up weighted parent links -> node records
+//
+// Why the compressed tree walks like the reference's: a chain of single-child
+// nodes shares one point set, hence one mass and centre of mass; the
+// reference accepts some chain node iff it accepts the deepest one (the
+// ratio only shrinks going down), so one node per chain, tested with the
+// deepest chain halfSize, gives the same pseudo-bodies. Leaves are never
+// tested (gvizForceEmbedder.c:41-53); an overflow leaf below a chain is
+// tested with its parent's halfSize. Empty children are skipped there too
+// (mass == 0, :38-39).
+#include <math.h>
+
+#include "internal.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ uint32_t ld_u32(const uint32_t *p) { return __ldcg(p); }
+
+// ---------------------------------------------------------------------------
+// bounding boxes and roots
+// ---------------------------------------------------------------------------
+
+__global__ __launch_bounds__(kThreads) void k_bbox_chunks(
+    const double2 *__restrict__ pos, const uint32_t *__restrict__ cb,
+    const uint32_t *__restrict__ ce, double4 *box, uint32_t *status) {
+  const uint32_t b = cb[blockIdx.x], e = ce[blockIdx.x];
+  double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
+  int bad = 0;
+  for (uint32_t i = b + threadIdx.x; i < e; i += kThreads) {
+    double2 p = pos[i];
+    if (!isfinite(p.x) || !isfinite(p.y)) bad = 1;
+    mnx = fmin(mnx, p.x);
+    mxx = fmax(mxx, p.x);
+    mny = fmin(mny, p.y);
+    mxy = fmax(mxy, p.y);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+  }
+  __shared__ double4 wb[kThreads / 32];
+  if (lane_id() == 0) wb[threadIdx.x >> 5] = make_double4(mnx, mxx, mny, mxy);
+  if (bad) atomicOr(status, GVIZ_ST_NONFINITE);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double4 r = wb[0];
+    for (int w = 1; w < kThreads / 32; w++) {
+      r.x = fmin(r.x, wb[w].x);
+      r.y = fmax(r.y, wb[w].y);
+      r.z = fmin(r.z, wb[w].z);
+      r.w = fmax(r.w, wb[w].w);
+    }
+    box[blockIdx.x] = r;
+  }
+}
+
+__global__ void k_graph_roots(const double4 *__restrict__ box,
+                              const uint32_t *__restrict__ gcb,
+                              const uint32_t *__restrict__ gce, GraphRoot *roots,
+                              uint32_t G, uint32_t *status) {
+  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
+  for (uint32_t c = gcb[g]; c < gce[g]; c++) {
+    double4 r = box[c];
+    mnx = fmin(mnx, r.x);
+    mxx = fmax(mxx, r.y);
+    mny = fmin(mny, r.z);
+    mxy = fmax(mxy, r.w);
+  }
+  GraphRoot R;
+  if (!(mnx <= mxx)) {  // empty graph
+    R.cx = 0.0;
+    R.cy = 0.0;
+    R.h0 = 1.0;
+    R.D = 0;
+    R.capped = 0;
+    roots[g] = R;
+    return;
+  }
+  double sx = mxx - mnx, sy = mxy - mny;
+  double span = sx > sy ? sx : sy;
+  R.h0 = span > 0.0 ? span / 2.0 : 1.0;
+  R.cx = (mnx + mxx) / 2.0;
+  R.cy = (mny + mxy) / 2.0;
+  double h = R.h0;
+  int d = 0;
+  while (h > 1e-9 && d < 64) {
+    h = h / 2.0;
+    d++;
+  }
+  R.D = d;
+  R.capped = h > 1e-9 ? 1 : 0;
+  if (R.capped) atomicOr(status, GVIZ_ST_DEPTH_CAP);
+  roots[g] = R;
+}
+
+// Quadrant path of every point: digit = (north ? 0 : 2) + (east ? 1 : 0),
+// i.e. NW=0 NE=1 SW=2 SE=3 (include/ds/gvizQuadtree.h:11-17), so sorted
+// paths are the reference's depth-first NW,NE,SW,SE order.
+__global__ __launch_bounds__(kThreads) void k_keys(
+    const double2 *__restrict__ pos, const uint32_t *__restrict__ gid,
+    const GraphRoot *__restrict__ roots, uint64_t *keyHi, uint64_t *keyLo,
+    uint64_t *ck, uint32_t *idx, uint32_t V, int gbits) {
+  uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= V) return;
+  const uint32_t g = gid ? gid[i] : 0u;
+  const GraphRoot R = roots[g];
+  const double2 p = pos[i];
+  double cx = R.cx, cy = R.cy, h = R.h0;
+  uint64_t hi = 0, lo = 0;
+  for (int d = 1; d <= R.D; d++) {
+    const bool east = p.x >= cx;
+    const bool north = p.y >= cy;
+    const uint64_t q = (north ? 0ull : 2ull) | (east ? 1ull : 0ull);
+    const double quarter = h / 2.0;
+    cx = east ? cx + quarter : cx + (-quarter);
+    cy = north ? cy + quarter : cy + (-quarter);
+    h = quarter;
+    if (d <= 32)
+      hi |= q << (64 - 2 * d);
+    else
+      lo |= q << (128 - 2 * d);
+  }
+  keyHi[i] = hi;
+  keyLo[i] = lo;
+  ck[i] = gbits ? (((uint64_t)g << (64 - gbits)) | (hi >> gbits)) : hi;
+  idx[i] = i;
+}
+
+__global__ __launch_bounds__(kThreads) void k_gather_keys(
+    const uint32_t *__restrict__ idx, const uint64_t *__restrict__ keyHi,
+    const uint64_t *__restrict__ keyLo, uint64_t *sHi, uint64_t *sLo,
+    uint32_t V) {
+  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
+  if (s >= V) return;
+  uint32_t i = idx[s];
+  sHi[s] = keyHi[i];
+  sLo[s] = keyLo[i];
+}
+
+// ---------------------------------------------------------------------------
+// runs of equal composite keys
+// ---------------------------------------------------------------------------
+
+__global__ __launch_bounds__(kThreads) void k_run_flags(
+    const uint64_t *__restrict__ ck, uint32_t *flag, uint32_t V) {
+  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
+  if (s >= V) return;
+  flag[s] = (s == 0 || ck[s] != ck[s - 1]) ? 1u : 0u;
+}
+
+__global__ __launch_bounds__(kThreads) void k_run_starts(
+    const uint32_t *__restrict__ flag, const uint32_t *__restrict__ scan,
+    uint32_t *runStart, uint32_t V) {
+  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
+  if (s >= V) return;
+  if (flag[s]) runStart[scan[s]] = s;
+}
+
+// Runs longer than the leaf capacity k need their deeper digits sorted;
+// runs of 2..k points lie in one leaf, so their keys are cut to the common
+// prefix (the leaf keeps them in vertex order, as the reference does).
+__global__ __launch_bounds__(kThreads) void k_run_classify(
+    const uint32_t *__restrict__ runStart, uint32_t *counts, uint32_t *deep,
+    uint64_t *sHi, uint64_t *sLo, uint32_t V, uint32_t k, int gbits) {
+  uint32_t r = blockIdx.x * kThreads + threadIdx.x;
+  uint32_t nRuns = counts[0];
+  if (r >= nRuns) return;
+  uint32_t start = runStart[r];
+  uint32_t end = (r + 1 < nRuns) ? runStart[r + 1] : V;
+  uint32_t len = end - start;
+  if (len > k) {
+    uint32_t slot = atomicAdd(&counts[1], 1u);
+    deep[2 * slot] = start;
+    deep[2 * slot + 1] = len;
+  } else if (len >= 2) {
+    uint64_t mask = gbits ? ~((1ull << gbits) - 1ull) : ~0ull;
+    for (uint32_t s = start; s < end; s++) {
+      sHi[s] &= mask;
+      sLo[s] = 0;
+    }
+  }
+}
+
+__device__ __forceinline__ bool key_less(uint64_t ah, uint64_t al, uint32_t av,
+                                         uint64_t bh, uint64_t bl, uint32_t bv) {
+  if (ah != bh) return ah < bh;
+  if (al != bl) return al < bl;
+  return av < bv;
+}
+
+// Bitonic sort of each deep run by (full path, vertex index) in shared memory.
+__global__ __launch_bounds__(512) void k_sort_runs(
+    uint64_t *sHi, uint64_t *sLo, uint32_t *idx, const uint32_t *__restrict__ deep,
+    const uint32_t *__restrict__ counts, uint32_t *status) {
+  extern __shared__ unsigned char smem[];
+  uint64_t *kh = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *kl = kh + GVIZ_FIX_MAX;
+  uint32_t *kv = reinterpret_cast<uint32_t *>(kl + GVIZ_FIX_MAX);
+  const uint32_t nDeep = counts[1];
+  for (uint32_t r = blockIdx.x; r < nDeep; r += gridDim.x) {
+    const uint32_t start = deep[2 * r], len = deep[2 * r + 1];
+    if (len > GVIZ_FIX_MAX) {
+      int diff = 0;
+      for (uint32_t j = threadIdx.x; j < len; j += blockDim.x) {
+        if (sHi[start + j] != sHi[start] || sLo[start + j] != sLo[start]) diff = 1;
+      }
+      if (__syncthreads_or(diff) && threadIdx.x == 0)
+        atomicOr(status, GVIZ_ST_DEEP_RUN);
+      continue;
+    }
+    uint32_t P = 1;
+    while (P < len) P <<= 1;
+    for (uint32_t j = threadIdx.x; j < P; j += blockDim.x) {
+      if (j < len) {
+        kh[j] = sHi[start + j];
+        kl[j] = sLo[start + j];
+        kv[j] = idx[start + j];
+      } else {
+        kh[j] = ~0ull;
+        kl[j] = ~0ull;
+        kv[j] = ~0u;
+      }
+    }
+    __syncthreads();
+    for (uint32_t size = 2; size <= P; size <<= 1) {
+      for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+        for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+          uint32_t j = i ^ stride;
+          if (j > i) {
+            bool asc = (i & size) == 0;
+            bool gt = key_less(kh[j], kl[j], kv[j], kh[i], kl[i], kv[i]);
+            if (gt == asc) {
+              uint64_t t64 = kh[i];
+              kh[i] = kh[j];
+              kh[j] = t64;
+              t64 = kl[i];
+              kl[i] = kl[j];
+              kl[j] = t64;
+              uint32_t t32 = kv[i];
+              kv[i] = kv[j];
+              kv[j] = t32;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (uint32_t j = threadIdx.x; j < len; j += blockDim.x) {
+      sHi[start + j] = kh[j];
+      sLo[start + j] = kl[j];
+      idx[start + j] = kv[j];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// buckets (identical full paths) and the binary radix tree
+// ---------------------------------------------------------------------------
+
+__global__ __launch_bounds__(kThreads) void k_bucket_flags(
+    const uint64_t *__restrict__ sHi, const uint64_t *__restrict__ sLo,
+    const uint32_t *__restrict__ idx, const uint32_t *__restrict__ gid,
+    uint32_t *flag, uint32_t V) {
+  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
+  if (s >= V) return;
+  uint32_t f = 1;
+  if (s > 0) {
+    f = (sHi[s] != sHi[s - 1] || sLo[s] != sLo[s - 1]) ? 1u : 0u;
+    if (!f && gid) f = gid[idx[s]] != gid[idx[s - 1]];
+  }
+  flag[s] = f;
+}
+
+__global__ __launch_bounds__(kThreads) void k_bucket_fill(
+    const uint32_t *__restrict__ flag, const uint32_t *__restrict__ scan,
+    const uint64_t *__restrict__ sHi, const uint64_t *__restrict__ sLo,
+    const uint32_t *__restrict__ idx, const uint32_t *__restrict__ gid,
+    uint32_t *bStart, uint64_t *bHi, uint64_t *bLo, uint32_t *bGid,
+    uint2 *upLeaf, uint32_t V) {
+  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
+  if (s >= V || !flag[s]) return;
+  uint32_t b = scan[s];
+  bStart[b] = s;
+  bHi[b] = sHi[s];
+  bLo[b] = sLo[s];
+  bGid[b] = gid ? gid[idx[s]] : 0u;
+  upLeaf[b] = make_uint2(GVIZ_NONE, 0u);
+}
+
+// Common-prefix length in bits of the composite keys (graph id:32,
+// path:128) of buckets a and b; -1 outside [0, U).
+__device__ __forceinline__ int bdelta(int a, int b, int U,
+                                      const uint64_t *__restrict__ bHi,
+                                      const uint64_t *__restrict__ bLo,
+                                      const uint32_t *__restrict__ bGid) {
+  if (b < 0 || b >= U) return -1;
+  uint32_t gx = bGid[a] ^ bGid[b];
+  if (gx) return __clz(gx);
+  uint64_t x = bHi[a] ^ bHi[b];
+  if (x) return 32 + __clzll(x);
+  x = bLo[a] ^ bLo[b];
+  if (x) return 96 + __clzll(x);
+  return 160;
+}
+
+// Karras, "Maximizing parallelism in the construction of BVHs, octrees and
+// k-d trees" (HPG 2012), algorithm of section 4 over unique bucket keys.
+__global__ __launch_bounds__(kThreads) void k_karras(
+    const uint64_t *__restrict__ bHi, const uint64_t *__restrict__ bLo,
+    const uint32_t *__restrict__ bGid, const uint32_t *__restrict__ counts,
+    uint32_t *nLeft, uint32_t *nRight, uint32_t *nFirst, uint32_t *nLast,
+    int32_t *nDelta, uint2 *upInt, uint2 *upLeaf) {
+  const int U = (int)counts[2];
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= U - 1) return;
+  const int dir = (bdelta(i, i + 1, U, bHi, bLo, bGid) -
+                   bdelta(i, i - 1, U, bHi, bLo, bGid)) >= 0 ? 1 : -1;
+  const int dmin = bdelta(i, i - dir, U, bHi, bLo, bGid);
+  int lmax = 2;
+  while (bdelta(i, i + lmax * dir, U, bHi, bLo, bGid) > dmin) lmax <<= 1;
+  int l = 0;
+  for (int t = lmax >> 1; t >= 1; t >>= 1)
+    if (bdelta(i, i + (l + t) * dir, U, bHi, bLo, bGid) > dmin) l += t;
+  const int j = i + l * dir;
+  const int dnode = bdelta(i, j, U, bHi, bLo, bGid);
+  int s = 0;
+  int div = 2;
+  int t;
+  do {
+    t = (l + div - 1) / div;
+    if (bdelta(i, i + (s + t) * dir, U, bHi, bLo, bGid) > dnode) s += t;
+    div <<= 1;
+  } while (t > 1);
+  const int gamma = i + s * dir + min(dir, 0);
+  const int first = min(i, j), last = max(i, j);
+  uint32_t left, right;
+  if (first == gamma) {
+    left = (uint32_t)gamma | GVIZ_LEAF_BIT;
+    upLeaf[gamma].x = (uint32_t)i;
+  } else {
+    left = (uint32_t)gamma;
+    upInt[gamma].x = (uint32_t)i;
+  }
+  if (last == gamma + 1) {
+    right = (uint32_t)(gamma + 1) | GVIZ_LEAF_BIT;
+    upLeaf[gamma + 1].x = (uint32_t)i;
+  } else {
+    right = (uint32_t)(gamma + 1);
+    upInt[gamma + 1].x = (uint32_t)i;
+  }
+  nLeft[i] = left;
+  nRight[i] = right;
+  nFirst[i] = (uint32_t)first;
+  nLast[i] = (uint32_t)last;
+  nDelta[i] = dnode;
+  if (i == 0) upInt[0].x = GVIZ_NONE;
+}
+
+struct BU {
+  const uint32_t *idx, *bStart, *bGid, *counts, *nLeft, *nRight;
+  const int32_t *nDelta;
+  const double *mass;
+  const double2 *pos;
+  uint2 *upInt, *upLeaf;
+  uint32_t *nCounter;
+  double *bM, *bSX, *bSY, *nM, *nSX, *nSY;
+  uint32_t *bCnt, *bT, *nCnt, *nT, *nFlag, *rootNode, *rootT, *status;
+  uint32_t V, k;
+};
+
+__device__ __forceinline__ void child_vals(const BU &a, uint32_t c, double &M,
+                                           double &SX, double &SY,
+                                           uint32_t &cnt, uint32_t &T) {
+  if (c & GVIZ_LEAF_BIT) {
+    uint32_t b = c & ~GVIZ_LEAF_BIT;
+    M = __ldcg(a.bM + b);
+    SX = __ldcg(a.bSX + b);
+    SY = __ldcg(a.bSY + b);
+    cnt = __ldcg(a.bCnt + b);
+    T = __ldcg(a.bT + b);
+  } else {
+    M = __ldcg(a.nM + c);
+    SX = __ldcg(a.nSX + c);
+    SY = __ldcg(a.nSY + c);
+    cnt = __ldcg(a.nCnt + c);
+    T = __ldcg(a.nT + c);
+  }
+}
+
+__device__ __forceinline__ uint2 *up_of(const BU &a, uint32_t c) {
+  return (c & GVIZ_LEAF_BIT) ? a.upLeaf + (c & ~GVIZ_LEAF_BIT) : a.upInt + c;
+}
+
+// Sums per bucket, then each thread climbs; the second child to arrive at a
+// node combines both (left first: fixed order, deterministic sums).
+__global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
+  const uint32_t U = a.counts[2];
+  const uint32_t b = blockIdx.x * kThreads + threadIdx.x;
+  if (b >= U) return;
+  const uint32_t start = a.bStart[b];
+  const uint32_t end = (b + 1 < U) ? a.bStart[b + 1] : a.V;
+  double M = 0.0, SX = 0.0, SY = 0.0;
+  for (uint32_t s = start; s < end; s++) {
+    uint32_t i = a.idx[s];
+    double m = a.mass[i];
+    double2 p = a.pos[i];
+    M += m;
+    SX += m * p.x;
+    SY += m * p.y;
+  }
+  uint32_t cnt = end - start;
+  uint32_t T = cnt == 1 ? 1u : 1u + cnt;
+  a.bM[b] = M;
+  a.bSX[b] = SX;
+  a.bSY[b] = SY;
+  a.bCnt[b] = cnt;
+  a.bT[b] = T;
+  const uint32_t g = a.bGid[b];
+  uint32_t x = b | GVIZ_LEAF_BIT;
+  for (int guard = 0;; guard++) {
+    if (guard > GVIZ_MAX_CLIMB) {
+      atomicOr(a.status, GVIZ_ST_TREE);
+      return;
+    }
+    uint2 *ux = up_of(a, x);
+    const uint32_t p = ux->x;
+    if (p == GVIZ_NONE || a.nDelta[p] < 32) {
+      a.rootNode[g] = x;
+      a.rootT[g] = T;
+      *ux = make_uint2(GVIZ_NONE, 0u);
+      return;
+    }
+    __threadfence();
+    if (atomicAdd(a.nCounter + p, 1u) == 0u) return;
+    a.nCounter[p] = 0u;
+    __threadfence();
+    const uint32_t l = a.nLeft[p], r = a.nRight[p];
+    double Ml, SXl, SYl, Mr, SXr, SYr;
+    uint32_t cl, Tl, cr, Tr;
+    child_vals(a, l, Ml, SXl, SYl, cl, Tl);
+    child_vals(a, r, Mr, SXr, SYr, cr, Tr);
+    M = Ml + Mr;
+    SX = SXl + SXr;
+    SY = SYl + SYr;
+    cnt = cl + cr;
+    const int dp = a.nDelta[p];
+    const uint32_t pp = a.upInt[p].x;
+    const bool absorbed = pp != GVIZ_NONE && a.nDelta[pp] >= 32 &&
+                          ((dp - 32) >> 1) == ((a.nDelta[pp] - 32) >> 1);
+    const bool collapsed = !absorbed && cnt <= a.k;
+    T = absorbed ? Tl + Tr : (collapsed ? 1u + cnt : 1u + Tl + Tr);
+    a.nM[p] = M;
+    a.nSX[p] = SX;
+    a.nSY[p] = SY;
+    a.nCnt[p] = cnt;
+    a.nT[p] = T;
+    a.nFlag[p] = (absorbed ? 1u : 0u) | (collapsed ? 2u : 0u);
+    const uint32_t base = absorbed ? 0u : 1u;
+    const uint32_t dead = collapsed ? 0x80000000u : 0u;
+    up_of(a, l)->y = base | dead;
+    up_of(a, r)->y = (base + Tl) | dead;
+    x = p;
+  }
+}
+
+// preorder position (without the graph base) and whether any ancestor is a
+// collapsed (capacity) leaf
+__device__ __forceinline__ void walk_up(uint2 u, const uint2 *__restrict__ upInt,
+                                        uint32_t &pre, uint32_t &dead) {
+  pre = 0;
+  dead = 0;
+  for (int guard = 0; u.x != GVIZ_NONE; guard++) {
+    if (guard > GVIZ_MAX_CLIMB) {  // never expected: report as dead
+      dead = 1;
+      return;
+    }
+    pre += u.y & 0x7fffffffu;
+    dead |= u.y >> 31;
+    u = upInt[u.x];
+  }
+}
+
+struct EM {
+  const uint32_t *idx, *bStart, *bGid, *bCnt, *counts, *nFirst, *nLast, *nFlag,
+      *nT, *nCnt, *graphBase;
+  const int32_t *nDelta;
+  const uint2 *upInt, *upLeaf;
+  const double *bM, *bSX, *bSY, *nM, *nSX, *nSY, *mass, *radius;
+  const double2 *pos;
+  const GraphRoot *roots;
+  void *nodes;
+  uint32_t *status;
+  double theta;
+  uint32_t V, k, maxNodes;
+  int f64;
+};
+
+__device__ void put_cell(const EM &a, uint32_t at, double M, double SX,
+                         double SY, double h, uint32_t next) {
+  if (at >= a.maxNodes) {
+    atomicOr(a.status, GVIZ_ST_TREE);
+    return;
+  }
+  double cx = 0.0, cy = 0.0;
+  if (M > 1e-9 || M < -1e-9) {
+    cx = SX / M;
+    cy = SY / M;
+  }
+  if (a.f64) {
+    NodeD n;
+    n.x = cx;
+    n.y = cy;
+    n.mass = M;
+    n.size = h;
+    n.next = (int32_t)next;
+    n.info = -1;
+    n.pad0 = n.pad1 = 0;
+    reinterpret_cast<NodeD *>(a.nodes)[at] = n;
+  } else {
+    NodeF n;
+    ds_split(cx, n.xh, n.xl);
+    ds_split(cy, n.yh, n.yl);
+    n.mass = (float)M;
+    if (isinf(h)) {
+      n.size = INFINITY;
+    } else {
+      double t = 2.0 * h / a.theta;
+      n.size = (float)(t * t);
+    }
+    n.next = (int32_t)next;
+    n.info = -1;
+    reinterpret_cast<NodeF *>(a.nodes)[at] = n;
+  }
+}
+
+__device__ void put_leaf(const EM &a, uint32_t at, uint32_t v) {
+  if (at >= a.maxNodes) {
+    atomicOr(a.status, GVIZ_ST_TREE);
+    return;
+  }
+  double2 p = a.pos[v];
+  if (a.f64) {
+    NodeD n;
+    n.x = p.x;
+    n.y = p.y;
+    n.mass = a.mass[v];
+    n.size = a.radius[v];
+    n.next = (int32_t)(at + 1);
+    n.info = (int32_t)v;
+    n.pad0 = n.pad1 = 0;
+    reinterpret_cast<NodeD *>(a.nodes)[at] = n;
+  } else {
+    NodeF n;
+    ds_split(p.x, n.xh, n.xl);
+    ds_split(p.y, n.yh, n.yl);
+    n.mass = (float)a.mass[v];
+    n.size = (float)a.radius[v];
+    n.next = (int32_t)(at + 1);
+    n.info = (int32_t)v;
+    reinterpret_cast<NodeF *>(a.nodes)[at] = n;
+  }
+}
+
+// depth of the nearest quadtree ancestor of a node whose binary parent is p
+__device__ __forceinline__ int quad_parent_depth(const EM &a, uint32_t p) {
+  if (p != GVIZ_NONE && (a.nFlag[p] & 1u)) p = a.upInt[p].x;
+  return p == GVIZ_NONE ? -1 : ((a.nDelta[p] - 32) >> 1);
+}
+
+__global__ __launch_bounds__(kThreads) void k_emit(EM a) {
+  const uint32_t U = a.counts[2];
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t nInt = U - 1;
+  if (t < nInt) {
+    const uint32_t p = t;
+    if (a.nDelta[p] < 32 || (a.nFlag[p] & 1u)) return;
+    uint32_t pre, dead;
+    walk_up(a.upInt[p], a.upInt, pre, dead);
+    if (dead) return;
+    const uint32_t fb = a.nFirst[p];
+    const uint32_t g = a.bGid[fb];
+    pre += a.graphBase[g];
+    const GraphRoot R = a.roots[g];
+    if (a.nFlag[p] & 2u) {  // capacity leaf: wrapper + points in vertex order
+      const uint32_t lb = a.nLast[p];
+      const uint32_t s0 = a.bStart[fb];
+      const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
+      put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], INFINITY,
+               pre + a.nT[p]);
+      uint32_t ids[GVIZ_MAX_NODES_PER_CELL];
+      uint32_t c = s1 - s0;
+      for (uint32_t j = 0; j < c; j++) {
+        uint32_t v = a.idx[s0 + j];
+        uint32_t q = j;
+        while (q > 0 && ids[q - 1] > v) {
+          ids[q] = ids[q - 1];
+          q--;
+        }
+        ids[q] = v;
+      }
+      for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, ids[j]);
+      return;
+    }
+    const int q = (a.nDelta[p] - 32) >> 1;
+    put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], ldexp(R.h0, -q),
+             pre + a.nT[p]);
+    return;
+  }
+  const uint32_t b = t - nInt;
+  if (t < nInt || b >= U) return;
+  uint32_t pre, dead;
+  const uint2 ub = a.upLeaf[b];
+  walk_up(ub, a.upInt, pre, dead);
+  if (dead) return;
+  const uint32_t g = a.bGid[b];
+  pre += a.graphBase[g];
+  const uint32_t c = a.bCnt[b];
+  const uint32_t s0 = a.bStart[b];
+  if (c == 1) {
+    put_leaf(a, pre, a.idx[s0]);
+    return;
+  }
+  const GraphRoot R = a.roots[g];
+  const int qp = quad_parent_depth(a, ub.x);
+  const bool testable = c > a.k && qp < R.D - 1;
+  const double h = testable ? ldexp(R.h0, -(R.D - 1)) : (double)INFINITY;
+  put_cell(a, pre, a.bM[b], a.bSX[b], a.bSY[b], h, pre + 1 + c);
+  for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, a.idx[s0 + j]);
+}
+
+// Inspection: per point, the depth of the reference leaf holding it.
+__global__ __launch_bounds__(kThreads) void k_leaf_depth(EM a, int32_t *depthOut) {
+  const uint32_t U = a.counts[2];
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t nInt = U - 1;
+  if (t < nInt) {
+    const uint32_t p = t;
+    if (a.nDelta[p] < 32 || !(a.nFlag[p] & 2u) || (a.nFlag[p] & 1u)) return;
+    uint32_t pre, dead;
+    walk_up(a.upInt[p], a.upInt, pre, dead);
+    if (dead) return;
+    const int d = quad_parent_depth(a, a.upInt[p].x) + 1;
+    const uint32_t fb = a.nFirst[p], lb = a.nLast[p];
+    const uint32_t s0 = a.bStart[fb];
+    const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
+    for (uint32_t s = s0; s < s1; s++) depthOut[a.idx[s]] = d;
+    return;
+  }
+  const uint32_t b = t - nInt;
+  if (t < nInt || b >= U) return;
+  uint32_t pre, dead;
+  walk_up(a.upLeaf[b], a.upInt, pre, dead);
+  if (dead) return;
+  const uint32_t c = a.bCnt[b];
+  const GraphRoot R = a.roots[a.bGid[b]];
+  const int d = c > a.k ? R.D : quad_parent_depth(a, a.upLeaf[b].x) + 1;
+  const uint32_t s0 = a.bStart[b];
+  for (uint32_t j = 0; j < c; j++) depthOut[a.idx[s0 + j]] = d;
+}
+
+EM make_em(gvizCudaForce *h) {
+  EM a;
+  a.idx = h->d_idx;
+  a.bStart = h->d_bStart;
+  a.bGid = h->d_bGid;
+  a.bCnt = h->d_bCnt;
+  a.counts = h->d_counts;
+  a.nFirst = h->d_nFirst;
+  a.nLast = h->d_nLast;
+  a.nFlag = h->d_nFlag;
+  a.nT = h->d_nT;
+  a.nCnt = h->d_nCnt;
+  a.graphBase = h->d_graphBase;
+  a.nDelta = h->d_nDelta;
+  a.upInt = h->d_upInt;
+  a.upLeaf = h->d_upLeaf;
+  a.bM = h->d_bM;
+  a.bSX = h->d_bSX;
+  a.bSY = h->d_bSY;
+  a.nM = h->d_nM;
+  a.nSX = h->d_nSX;
+  a.nSY = h->d_nSY;
+  a.mass = h->d_mass;
+  a.radius = h->d_radius;
+  a.pos = h->d_pos;
+  a.roots = h->d_roots;
+  a.nodes = h->d_nodes;
+  a.status = h->d_status;
+  a.maxNodes = (uint32_t)h->maxNodes;
+  a.theta = h->params.theta;
+  a.V = (uint32_t)h->V;
+  a.k = h->params.nodesPerCell;
+  a.f64 = h->params.precision == GVIZ_CUDA_FP64;
+  return a;
+}
+
+inline uint32_t blocks_for(size_t n) {
+  return (uint32_t)((n + kThreads - 1) / kThreads);
+}
+
+}  // namespace
+
+void enqueue_tree_build(gvizCudaForce *h) {
+  const uint32_t V = (uint32_t)h->V;
+  cudaStream_t st = h->stream;
+  cudaMemsetAsync(h->d_counts, 0, 8 * sizeof(uint32_t), st);
+  // graphs without vertices get no root: their subtree size must read 0
+  cudaMemsetAsync(h->d_rootT, 0, h->G * sizeof(uint32_t), st);
+  k_bbox_chunks<<<h->nChunks, kThreads, 0, st>>>(h->d_pos, h->d_chunkBegin,
+                                                  h->d_chunkEnd, h->d_chunkBox,
+                                                  h->d_status);
+  k_graph_roots<<<(uint32_t)((h->G + 127) / 128), 128, 0, st>>>(
+      h->d_chunkBox, h->d_gChunkBegin, h->d_gChunkEnd, h->d_roots,
+      (uint32_t)h->G, h->d_status);
+  k_keys<<<blocks_for(V), kThreads, 0, st>>>(h->d_pos, h->d_gid, h->d_roots,
+                                             h->d_keyHi, h->d_keyLo, h->d_ck,
+                                             h->d_idx, V, h->gbits);
+  prof_mark(h, "tree_keys");
+  radix_sort_pairs(h, h->d_ck, h->d_idx, h->d_ckAlt, h->d_idxAlt, V);
+  k_gather_keys<<<blocks_for(V), kThreads, 0, st>>>(h->d_idx, h->d_keyHi,
+                                                    h->d_keyLo, h->d_sHi,
+                                                    h->d_sLo, V);
+  k_run_flags<<<blocks_for(V), kThreads, 0, st>>>(h->d_ck, h->d_flag, V);
+  scan_exclusive(h, h->d_flag, h->d_scan, V, h->d_counts + 0);
+  k_run_starts<<<blocks_for(V), kThreads, 0, st>>>(h->d_flag, h->d_scan,
+                                                   h->d_runStart, V);
+  k_run_classify<<<blocks_for(V), kThreads, 0, st>>>(
+      h->d_runStart, h->d_counts, h->d_deepRuns, h->d_sHi, h->d_sLo, V,
+      h->params.nodesPerCell, h->gbits);
+  const size_t fixSmem = (size_t)GVIZ_FIX_MAX * 20;
+  k_sort_runs<<<148, 512, fixSmem, st>>>(h->d_sHi, h->d_sLo, h->d_idx,
+                                          h->d_deepRuns, h->d_counts,
+                                          h->d_status);
+  k_bucket_flags<<<blocks_for(V), kThreads, 0, st>>>(h->d_sHi, h->d_sLo,
+                                                     h->d_idx, h->d_gid,
+                                                     h->d_flag, V);
+  scan_exclusive(h, h->d_flag, h->d_scan, V, h->d_counts + 2);
+  k_bucket_fill<<<blocks_for(V), kThreads, 0, st>>>(
+      h->d_flag, h->d_scan, h->d_sHi, h->d_sLo, h->d_idx, h->d_gid,
+      h->d_bStart, h->d_bHi, h->d_bLo, h->d_bGid, h->d_upLeaf, V);
+  prof_mark(h, "tree_buckets");
+  k_karras<<<blocks_for(V), kThreads, 0, st>>>(
+      h->d_bHi, h->d_bLo, h->d_bGid, h->d_counts, h->d_nLeft, h->d_nRight,
+      h->d_nFirst, h->d_nLast, h->d_nDelta, h->d_upInt, h->d_upLeaf);
+  BU bu;
+  bu.idx = h->d_idx;
+  bu.bStart = h->d_bStart;
+  bu.bGid = h->d_bGid;
+  bu.counts = h->d_counts;
+  bu.nLeft = h->d_nLeft;
+  bu.nRight = h->d_nRight;
+  bu.nDelta = h->d_nDelta;
+  bu.mass = h->d_mass;
+  bu.pos = h->d_pos;
+  bu.upInt = h->d_upInt;
+  bu.upLeaf = h->d_upLeaf;
+  bu.nCounter = h->d_nCounter;
+  bu.bM = h->d_bM;
+  bu.bSX = h->d_bSX;
+  bu.bSY = h->d_bSY;
+  bu.nM = h->d_nM;
+  bu.nSX = h->d_nSX;
+  bu.nSY = h->d_nSY;
+  bu.bCnt = h->d_bCnt;
+  bu.bT = h->d_bT;
+  bu.nCnt = h->d_nCnt;
+  bu.nT = h->d_nT;
+  bu.nFlag = h->d_nFlag;
+  bu.rootNode = h->d_rootNode;
+  bu.rootT = h->d_rootT;
+  bu.status = h->d_status;
+  bu.V = V;
+  bu.k = h->params.nodesPerCell;
+  k_bottom_up<<<blocks_for(V), kThreads, 0, st>>>(bu);
+  scan_exclusive(h, h->d_rootT, h->d_graphBase, h->G, h->d_counts + 3);
+  EM em = make_em(h);
+  k_emit<<<blocks_for(2 * (size_t)V), kThreads, 0, st>>>(em);
+  prof_mark(h, "tree_nodes");
+}
+
+void enqueue_tree_export(gvizCudaForce *h, int32_t *leafDepth) {
+  EM em = make_em(h);
+  k_leaf_depth<<<blocks_for(2 * h->V), kThreads, 0, h->stream>>>(em,
+                                                                 leafDepth);
+}
+
+void tree_set_smem_limits() {
+  cudaFuncSetAttribute(k_sort_runs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       GVIZ_FIX_MAX * 20);
+}
+
+// Inspection: every cell of the compressed tree (branching nodes and
+// multi-point leaves) at its preorder slot, with the reference node it
+// stands for: depth, quadrant path, mass, centre of mass, point count.
+namespace {
+
+__device__ __forceinline__ uint64_t dmask_hi(int d) {
+  return d <= 0 ? 0ull : (d >= 32 ? ~0ull : (~0ull << (64 - 2 * d)));
+}
+__device__ __forceinline__ uint64_t dmask_lo(int d) {
+  return d <= 32 ? 0ull : (d >= 64 ? ~0ull : (~0ull << (128 - 2 * d)));
+}
+
+struct CellOut {
+  int32_t *depth;
+  uint64_t *hi, *lo, *cnt;
+  double *mass, *cx, *cy;
+  const uint64_t *bHi, *bLo;
+};
+
+__device__ void cell_out(const CellOut &o, uint32_t at, int d, uint32_t b,
+                         double M, double SX, double SY, uint64_t c) {
+  o.depth[at] = d;
+  o.hi[at] = o.bHi[b] & dmask_hi(d);
+  o.lo[at] = o.bLo[b] & dmask_lo(d);
+  o.mass[at] = M;
+  const bool ok = M > 1e-9 || M < -1e-9;
+  o.cx[at] = ok ? SX / M : 0.0;
+  o.cy[at] = ok ? SY / M : 0.0;
+  o.cnt[at] = c;
+}
+
+__global__ __launch_bounds__(kThreads) void k_cell_dump(EM a, CellOut o) {
+  const uint32_t U = a.counts[2];
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t nInt = U - 1;
+  if (t < nInt) {
+    const uint32_t p = t;
+    if (a.nDelta[p] < 32 || (a.nFlag[p] & 1u)) return;
+    uint32_t pre, dead;
+    walk_up(a.upInt[p], a.upInt, pre, dead);
+    if (dead) return;
+    const uint32_t fb = a.nFirst[p];
+    pre += a.graphBase[a.bGid[fb]];
+    const int d = (a.nFlag[p] & 2u) ? quad_parent_depth(a, a.upInt[p].x) + 1
+                                    : ((a.nDelta[p] - 32) >> 1);
+    cell_out(o, pre, d, fb, a.nM[p], a.nSX[p], a.nSY[p], a.nCnt[p]);
+    return;
+  }
+  const uint32_t b = t - nInt;
+  if (t < nInt || b >= U) return;
+  const uint32_t c = a.bCnt[b];
+  if (c < 2) return;
+  uint32_t pre, dead;
+  walk_up(a.upLeaf[b], a.upInt, pre, dead);
+  if (dead) return;
+  const GraphRoot R = a.roots[a.bGid[b]];
+  pre += a.graphBase[a.bGid[b]];
+  const int d = c > a.k ? R.D : quad_parent_depth(a, a.upLeaf[b].x) + 1;
+  cell_out(o, pre, d, b, a.bM[b], a.bSX[b], a.bSY[b], c);
+}
+
+}  // namespace
+
+void enqueue_cell_dump(gvizCudaForce *h, int32_t *depth, uint64_t *hi,
+                       uint64_t *lo, double *mass, double *cx, double *cy,
+                       uint64_t *cnt) {
+  EM em = make_em(h);
+  CellOut o;
+  o.depth = depth;
+  o.hi = hi;
+  o.lo = lo;
+  o.cnt = cnt;
+  o.mass = mass;
+  o.cx = cx;
+  o.cy = cy;
+  o.bHi = h->d_bHi;
+  o.bLo = h->d_bLo;
+  k_cell_dump<<<blocks_for(2 * h->V), kThreads, 0, h->stream>>>(em, o);
+}

@@ -1,0 +1,260 @@
+/*
+ * gvizcuda.h -- C ABI of libgvizcuda, the B200 (sm_100a) implementation of
+ * gviz's force-directed layout step.
+ *
+ * Plain pointers and sizes only. Every entry point names the reference
+ * interface it stands in for (paths inside the Pretz0za/Grapher tree). The
+ * gviz-side glue that attaches this library to an existing
+ * gvizForceEmbedderState and takes over the "forceEmbedder.step" action is
+ * declared in gvizCudaForceEmbedder.h.
+ *
+ * Layouts:
+ *   - vertices are in the embedder's compact order (state->vertices[i] -> i,
+ *     include/embedders/gvizForceEmbedder.h:44-46);
+ *   - positions / forces are interleaved x0,y0,x1,y1,... FP64, as in
+ *     state->positionsScratch (include/embedders/gvizForceEmbedder.h:85-87);
+ *   - adjacency is CSR over compact indices, rows in the order the subgraph
+ *     neighbour iterator yields them (src/ds/gvizSubgraph.c:466-519);
+ *   - a "batch" is several independent graphs concatenated: graph g owns the
+ *     vertices [graphOffsets[g], graphOffsets[g+1]) and has its own quadtree,
+ *     global speed and stat series.
+ *
+ * Threading: one handle is driven from one host thread at a time; every
+ * handle owns its CUDA stream. Errors are returned as negative codes and
+ * latched per handle (gvizCudaForceLastError); nothing aborts the process.
+ */
+#ifndef GVIZCUDA_H
+#define GVIZCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* force models: same values as gvizForceModelKind
+ * (include/embedders/gvizForceModel.h:8-11) */
+#define GVIZ_CUDA_MODEL_FR 0
+#define GVIZ_CUDA_MODEL_LINLOG 1
+
+/* arithmetic of the force walk (positions and speed reductions are FP64 in
+ * both): FP32 with Kahan-compensated per-vertex sums, or FP64 with the
+ * reference's operation order and no fused multiply-add */
+#define GVIZ_CUDA_FP32 0
+#define GVIZ_CUDA_FP64 1
+
+/* status codes; -1 and -2 keep the reference's meaning
+ * (include/embedders/gvizForceEmbedder.h:161) */
+#define GVIZ_CUDA_OK 0
+#define GVIZ_CUDA_ERR_ALLOC (-1)      /* device or host allocation failed */
+#define GVIZ_CUDA_ERR_DIMENSION (-2)  /* only 2-D layouts are supported */
+#define GVIZ_CUDA_ERR_ARG (-3)        /* invalid argument */
+#define GVIZ_CUDA_ERR_CUDA (-4)       /* a CUDA runtime call failed */
+#define GVIZ_CUDA_ERR_NOT_BEGUN (-5)  /* Run/Step before Begin */
+#define GVIZ_CUDA_ERR_NONFINITE (-6)  /* a position was NaN or infinite */
+#define GVIZ_CUDA_ERR_DEEP_RUN (-7)   /* > 4096 distinct points share one
+                                         depth-32 quadtree cell */
+#define GVIZ_CUDA_ERR_NO_DEVICE (-8)  /* no usable CUDA device */
+#define GVIZ_CUDA_ERR_LIMIT (-9)      /* size beyond a documented limit */
+
+typedef struct gvizCudaForce gvizCudaForce; /* opaque handle */
+
+/* Graph structure handed to gvizCudaForceCreate. */
+typedef struct gvizCudaGraphDesc {
+  size_t vertexCount;          /* total vertices over all graphs */
+  const uint64_t *rowOffsets;  /* vertexCount + 1 */
+  const uint32_t *neighbors;   /* rowOffsets[vertexCount] compact indices */
+  const uint64_t *degree;      /* vertexCount, or NULL for the row lengths */
+  size_t graphCount;           /* 1 for one layout, > 1 for a batch */
+  const uint64_t *graphOffsets;/* graphCount + 1, NULL when graphCount == 1 */
+  int32_t model;               /* GVIZ_CUDA_MODEL_* */
+  int32_t device;              /* CUDA device ordinal */
+} gvizCudaGraphDesc;
+
+/* Configuration, field for field the embedder's
+ * (include/embedders/gvizForceEmbedder.h:52-125). */
+typedef struct gvizCudaForceParams {
+  double edgeLength;        /* FR's k */
+  double theta;             /* Barnes-Hut opening threshold (side/distance) */
+  uint32_t nodesPerCell;    /* quadtree leaf capacity, 1..256 */
+  int32_t barnesHutEnabled; /* 0: exact all-pairs repulsion */
+  double gravityK;
+  double radiusBase;
+  double radiusPerDegree;
+  double overlapConstant;
+  int32_t preventOverlap;
+  int32_t precision;        /* GVIZ_CUDA_FP32 or GVIZ_CUDA_FP64 */
+  double jitterTolerance;
+  int32_t strictReductions; /* 1: sum swing/traction/magnitudes in vertex
+                               order like the reference's serial loops */
+  int32_t farField;         /* 0: monopole; 1: learned correction (needs
+                               gvizCudaForceSetFarFieldModel) */
+} gvizCudaForceParams;
+
+/* One step's entries of the five stat series the embedder appends
+ * (src/embedders/gvizForceEmbedder.c:484-492). */
+typedef struct gvizCudaStepStats {
+  double maxDisp;
+  double speed;
+  double meanAttractive;
+  double meanRepulsive;
+  double meanGravity;
+} gvizCudaStepStats;
+
+/* ---- lifecycle ------------------------------------------------------- */
+
+/* Defaults of gvizForceEmbedderInit (src/embedders/gvizForceEmbedder.c:283-294). */
+void gvizCudaForceDefaultParams(gvizCudaForceParams *out);
+
+/* Replaces gvizForceEmbedderInit (src/embedders/gvizForceEmbedder.c:219-325):
+ * copies the structure to the device, computes mass from degree per model
+ * (src/embedders/gvizForceModel.c:5-8, 31) and sizes every device buffer. */
+int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *graph);
+
+/* Replaces gvizForceEmbedderRelease (src/embedders/gvizForceEmbedder.c:327-355). */
+void gvizCudaForceDestroy(gvizCudaForce *h);
+
+/* Replaces the Configure* / Set*Enabled setters
+ * (src/embedders/gvizForceEmbedder.c:357-410); values are taken as given. */
+int gvizCudaForceSetParams(gvizCudaForce *h, const gvizCudaForceParams *p);
+int gvizCudaForceGetParams(const gvizCudaForce *h, gvizCudaForceParams *p);
+
+/* Positions in compact order (2 * vertexCount doubles). */
+int gvizCudaForceSetPositions(gvizCudaForce *h, const double *xy);
+int gvizCudaForceGetPositions(gvizCudaForce *h, double *xy);
+
+/* The FA2 part of gvizForceEmbedderBegin (src/embedders/gvizForceEmbedder.c:416-424):
+ * speed = 1, efficiency = 1, force history zero, iteration 0, stats cleared. */
+int gvizCudaForceBegin(gvizCudaForce *h);
+
+/* Reads / overwrites the FA2 state: structForce (2V, may be NULL) and the
+ * per-graph global speed and speed efficiency (graphCount each, may be NULL). */
+int gvizCudaForceSetFa2State(gvizCudaForce *h, const double *structForce,
+                             const double *speed, const double *efficiency);
+int gvizCudaForceGetFa2State(gvizCudaForce *h, double *structForce,
+                             double *speed, double *efficiency);
+
+/* ---- stepping -------------------------------------------------------- */
+
+/* Replaces gvizForceEmbedderStep (src/embedders/gvizForceEmbedder.c:445-495)
+ * with positions resident on the device. Waits for the step; returns graph
+ * 0's maxDisp (negative status on failure) and fills stats[graphCount]. */
+double gvizCudaForceStep(gvizCudaForce *h, gvizCudaStepStats *stats);
+
+/* The same step end to end over host memory: copies xy (2V, compact order)
+ * to the device, steps, copies the new positions back into xy. This is what
+ * the gviz action handler does per invocation. */
+double gvizCudaForceStepHost(gvizCudaForce *h, double *xy,
+                             gvizCudaStepStats *stats);
+
+/* Enqueues n steps without waiting (replayed from a captured CUDA graph). */
+int gvizCudaForceEnqueueSteps(gvizCudaForce *h, uint32_t n);
+int gvizCudaForceSynchronize(gvizCudaForce *h);
+
+/* Replaces gvizForceEmbedderRun (src/embedders/gvizForceEmbedder.c:497-510):
+ * every graph steps until its maxDisp < epsilon or maxIters rounds ran.
+ * rounds[graphCount] (may be NULL) receives each graph's round count. */
+int gvizCudaForceRun(gvizCudaForce *h, size_t maxIters, double epsilon,
+                     uint64_t *rounds);
+
+/* Stat history of graph g since Begin: up to cap rows of 5 doubles
+ * {maxDisp, speed, meanAtt, meanRep, meanGrav}; returns the row count. */
+int64_t gvizCudaForceStatHistory(gvizCudaForce *h, uint32_t graph,
+                                 double *out, size_t cap);
+
+/* Per-vertex results of the last step in compact order (any may be NULL):
+ * the state arrays of include/embedders/gvizForceEmbedder.h:82-108. */
+int gvizCudaForceGetForces(gvizCudaForce *h, double *disp, double *structForce,
+                           double *attMag, double *repMag, double *swing,
+                           double *traction, double *applied);
+
+/* ---- inspection ------------------------------------------------------ */
+
+/* Builds the quadtree on the current positions without stepping and
+ * reports each point's leaf as (depth, quadrant path; 2 bits per level,
+ * MSB first, digits 1..32 in pathHi, 33..64 in pathLo). Matches the leaves
+ * of gvizQuadtreeInit (src/ds/gvizQuadtree.c:200-225) point for point. */
+int gvizCudaForceTreeLeaves(gvizCudaForce *h, int32_t *leafDepth,
+                            uint64_t *pathHi, uint64_t *pathLo,
+                            uint64_t *nodeCount);
+
+/* Compressed-tree nodes of the last build (branching nodes and multi-point
+ * leaves): depth, path, mass, centre of mass, point count. Returns count. */
+int64_t gvizCudaForceTreeNodes(gvizCudaForce *h, size_t cap, int32_t *depth,
+                               uint64_t *pathHi, uint64_t *pathLo,
+                               double *mass, double *comX, double *comY,
+                               uint64_t *count);
+
+/* FP64 exact repulsion (src/embedders/gvizForceEmbedder.c:104-115) of the
+ * listed target vertices against all vertices of their graph, on the GPU:
+ * the judge of approximate walks. out: 2 * nTargets. */
+int gvizCudaForceExactRepulsion(gvizCudaForce *h, const uint32_t *targets,
+                                size_t nTargets, double *out);
+
+/* Repulsion of the current walk configuration (no step taken), for error
+ * measurements: out 2V compact order. */
+int gvizCudaForceRepulsion(gvizCudaForce *h, double *out);
+
+/* Number of pseudo-body + pair interactions the walk evaluates on the
+ * current positions (summed over vertices) and node visits per warp. */
+int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
+                                   uint64_t *warpNodeVisits);
+
+/* Per-kernel device time of the last profiled step (CUDA events on the
+ * handle's stream). names: up to cap C strings; ms: up to cap values. */
+int gvizCudaForceProfileStep(gvizCudaForce *h, size_t cap, const char **names,
+                             double *ms);
+
+/* Device time in ms of n back-to-back steps, measured with CUDA events on
+ * the handle's stream around the replays of the captured step. */
+int gvizCudaForceTimeSteps(gvizCudaForce *h, uint32_t n, float *ms);
+
+/* Number of this library's kernels one step launches (kernel nodes of the
+ * captured step graph for the current parameters). */
+int gvizCudaForceStepKernelCount(gvizCudaForce *h);
+
+int gvizCudaForceLastError(const gvizCudaForce *h);
+const char *gvizCudaErrorString(int code);
+
+/* Lets a caller supply the CUDA stream (a cudaStream_t) the handle uses. */
+int gvizCudaForceSetStream(gvizCudaForce *h, void *stream);
+
+/* ---- host helpers: workloads and initial placement ------------------- */
+
+/* Ordered undirected edge lists. Each returns the edge count; pass NULL
+ * buffers to query it first. */
+/* build_rect_mesh (src/utils/graphs.c:285-316) */
+size_t gvizCudaGenGrid(size_t rows, size_t cols, uint32_t *ea, uint32_t *eb);
+/* build_random_connected_graph (src/utils/graphs.c:598-639), same rand_r
+ * stream, same edge order */
+size_t gvizCudaGenRandomConnected(size_t n, double density, unsigned seed,
+                                  uint32_t *ea, uint32_t *eb);
+/* Barabasi-Albert: K_{m+1} seed, then each new vertex attaches m distinct
+ * targets chosen proportionally to degree; 4n - 10 edges for m = 4 */
+size_t gvizCudaGenBarabasiAlbert(size_t n, uint32_t m, uint64_t seed,
+                                 uint32_t *ea, uint32_t *eb);
+/* Erdos-Renyi G(n, m): m distinct non-loop edges */
+size_t gvizCudaGenErdosRenyi(size_t n, size_t m, uint64_t seed, uint32_t *ea,
+                             uint32_t *eb);
+/* R-MAT with (a, b, c, 1-a-b-c): `draws` edge draws, self-loops dropped,
+ * duplicates (either orientation) removed, first occurrence kept */
+size_t gvizCudaGenRmat(uint32_t scale, size_t draws, double a, double b,
+                       double c, uint64_t seed, uint32_t *ea, uint32_t *eb);
+
+/* CSR exactly as gvizGraphAddEdge builds adjacency lists for an undirected
+ * graph (src/ds/gvizGraph.c:163-172): edge (a,b) appends b to a's list and
+ * a to b's list, in edge order. rowOffsets: V+1; neighbors: 2E. */
+int gvizCudaEdgesToCsr(size_t V, const uint32_t *ea, const uint32_t *eb,
+                       size_t E, uint64_t *rowOffsets, uint32_t *neighbors);
+
+/* gvizEmbeddedGraphRandomizePositions (src/embedders/gvizEmbeddedGraph.c:406-426)
+ * for vertices 0..V-1 in order: the same rand_r draws, x then y. */
+void gvizCudaRandomizePositions(double *xy, size_t V, double boxExtent,
+                                unsigned seed);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GVIZCUDA_H */

@@ -1,0 +1,146 @@
+"""Device step vs the reference: golden trajectories made by the reference
+(teacher-forced: every step starts from the reference's previous state) and
+oracle comparisons on larger graphs.
+
+Tolerances:
+  FP64 path, exact mode, strict reductions: bit-exact (same operations in the
+      same order as the reference, no fused multiply-add).
+  FP64 path with Barnes-Hut: displacement relative error <= 1e-9 per vertex
+      (only the centre-of-mass summation order differs from the reference's
+      running mean, i.e. ~1e-16 relative in every pseudo-body position).
+  FP32 path (the fast path): per-vertex displacement relative error
+      median <= 1e-5, 99th percentile <= 1e-3, max <= 5e-2; the max bound
+      admits the rare opening decision that flips at FP32 rounding.
+"""
+import numpy as np
+import pytest
+
+from helpers import cfg, csr_of, degree_mass, golden, golden_cfg, make_layout, oracle_params, rel_err
+
+pytestmark = pytest.mark.gpu
+
+TRAJ = ["traj_grid32_fr_theta05", "traj_rc300_linlog_theta08_grav_overlap",
+        "traj_rc200_fr_exact", "traj_rc500_linlog_theta12_k3"]
+
+
+def _teacher_forced(g, c):
+    V = int(g["V"])
+    row, col = csr_of(V, g["ea"], g["eb"])
+    lay = make_layout(row, col, c)
+    lay.begin(0, positions=g["x0"])
+    prev_pos, prev_sf, prev_ss = g["x0"], np.zeros(2 * V), np.array([1.0, 1.0])
+    out = []
+    for s in range(g["pos"].shape[0]):
+        lay.set_positions(prev_pos)
+        lay.set_fa2_state(prev_sf, prev_ss[0], prev_ss[1])
+        md = lay.step()
+        pos = lay.positions()
+        sf, sp, ef = lay.fa2_state()
+        out.append(dict(md=md, pos=pos, sf=sf, speed=sp[0], eff=ef[0],
+                        stats=lay.stat_history()[-1], prev=prev_pos))
+        prev_pos, prev_sf, prev_ss = g["pos"][s], g["structForce"][s], g["speedState"][s]
+    lay.close()
+    return out
+
+
+@pytest.mark.parametrize("name", TRAJ)
+def test_fp64_matches_reference_golden(name):
+    g = golden(name)
+    c = golden_cfg(g)
+    c.update(precision="fp64", strict=True)
+    exact = not c["bh"]
+    for s, o in enumerate(_teacher_forced(g, c)):
+        if exact and c["model"] == 0:
+            assert np.array_equal(o["pos"], g["pos"][s]), f"step {s}"
+            assert np.array_equal(o["sf"], g["structForce"][s])
+            assert o["md"] == g["maxDisp"][s] and o["speed"] == g["speedState"][s][0]
+            assert np.array_equal(o["stats"], g["stats"][s])
+        else:
+            d_gpu = o["pos"] - o["prev"]
+            d_ref = g["pos"][s] - o["prev"]
+            assert rel_err(d_gpu, d_ref, 1e-300).max() <= 1e-9, f"step {s}"
+            np.testing.assert_allclose(o["sf"], g["structForce"][s], rtol=1e-9, atol=1e-12)
+            assert abs(o["speed"] - g["speedState"][s][0]) <= 1e-9 * g["speedState"][s][0]
+            np.testing.assert_allclose(o["stats"], g["stats"][s], rtol=1e-9, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", TRAJ)
+def test_fp32_matches_reference_golden(name):
+    g = golden(name)
+    c = golden_cfg(g)
+    c.update(precision="fp32")
+    for s, o in enumerate(_teacher_forced(g, c)):
+        e = rel_err(o["pos"] - o["prev"], g["pos"][s] - o["prev"], 1e-300)
+        assert np.median(e) <= 1e-5, (s, np.median(e))
+        assert np.quantile(e, 0.99) <= 1e-3, (s, np.quantile(e, 0.99))
+        assert e.max() <= 5e-2, (s, e.max())
+        assert abs(o["speed"] - g["speedState"][s][0]) <= 1e-3 * g["speedState"][s][0]
+
+
+def _random_case(model, V, seed):
+    from grapher_b200 import graphs
+    if model == 1:
+        a, b = graphs.barabasi_albert(V, 3, seed)
+    else:
+        a, b = graphs.erdos_renyi(V, 3 * V, seed)
+    return csr_of(V, a, b)
+
+
+CASES = [
+    dict(model=0, theta=0.5),
+    dict(model=0, theta=1.0, k=3),
+    dict(model=1, theta=0.8, gravity=1.0, radius_base=1.0, radius_per_degree=0.5,
+         prevent_overlap=True),
+    dict(model=1, theta=1.2, gravity=0.3),
+    dict(model=0, bh=False, prevent_overlap=True, radius_base=2.0),
+    dict(model=1, bh=False, gravity=1.0),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_one_step_matches_oracle(oracle, case):
+    kw = CASES[case]
+    V = 4000 if kw.get("bh", True) else 1500
+    row, col = _random_case(kw["model"], V, 17 + case)
+    deg, mass = degree_mass(row, kw["model"])
+    from grapher_b200 import graphs
+    x0 = graphs.randomize_positions(V, 300.0, 99 + case)
+    sf0 = np.random.default_rng(case).normal(0, 1.0, 2 * V)
+    ss0 = np.array([0.7, 0.6])
+    for prec in ("fp64", "fp32"):
+        c = cfg(precision=prec, **kw)
+        pos_o, sf_o, ss_o = x0.copy(), sf0.copy(), ss0.copy()
+        ref = oracle.step((row, col), mass, deg, oracle_params(c), pos_o, sf_o, ss_o)
+        lay = make_layout(row, col, c)
+        lay.begin(0, positions=x0)
+        lay.set_fa2_state(sf0, ss0[0], ss0[1])
+        lay.step()
+        f = lay.forces()
+        pos = lay.positions()
+        if prec == "fp64":
+            assert rel_err(f["disp"], ref["disp"], 1e-300).max() <= 1e-9
+            assert rel_err(pos - x0, pos_o - x0, 1e-300).max() <= 1e-9
+            np.testing.assert_allclose(f["attMag"], ref["attMag"], rtol=1e-12, atol=1e-300)
+            np.testing.assert_allclose(f["repMag"], ref["repMag"], rtol=1e-9, atol=1e-300)
+        else:
+            e = rel_err(f["disp"], ref["disp"], 1e-300)
+            assert np.median(e) <= 1e-5 and np.quantile(e, 0.99) <= 1e-3, (np.median(e), np.quantile(e, 0.99))
+        lay.close()
+
+
+def test_free_run_fp64_tracks_oracle(oracle):
+    from grapher_b200 import graphs
+    a, b = graphs.grid(32, 32)
+    row, col = csr_of(1024, a, b)
+    deg, mass = degree_mass(row, 0)
+    c = cfg(model=0, theta=0.5, precision="fp64")
+    x0 = graphs.randomize_positions(1024, 1.0, 7)
+    pos_o, sf_o, ss_o = x0.copy(), np.zeros(2048), np.array([1.0, 1.0])
+    lay = make_layout(row, col, c)
+    lay.begin(0, positions=x0)
+    for _ in range(30):
+        oracle.step((row, col), mass, deg, oracle_params(c), pos_o, sf_o, ss_o)
+        lay.step()
+    p = lay.positions()
+    assert np.abs(p - pos_o).max() <= 1e-6 * max(1.0, np.abs(pos_o).max())
+    lay.close()
