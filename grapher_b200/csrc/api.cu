@@ -82,6 +82,8 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_chunkGraph);
   dfree(h->d_gChunkBegin);
   dfree(h->d_gChunkEnd);
+  dfree(h->d_attrLight);
+  dfree(h->d_attrHeavy);
   dfree(h->d_pos);
   dfree(h->d_sf);
   dfree(h->d_sfOld);
@@ -437,6 +439,11 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
     gce[gg] = (uint32_t)cb.size();
   }
   h->nChunks = (uint32_t)cb.size();
+  std::vector<uint32_t> light, heavy;
+  for (size_t v = 0; v < V; v++)
+    (row[v + 1] - row[v] > GVIZ_HEAVY_DEGREE ? heavy : light).push_back((uint32_t)v);
+  h->nAttrLight = (uint32_t)light.size();
+  h->nAttrHeavy = (uint32_t)heavy.size();
   h->h_graphOff = (uint64_t *)malloc(sizeof(uint64_t) * (G + 1));
   h->h_meanDegPlusOne = (double *)malloc(sizeof(double) * G);
   memcpy(h->h_graphOff, goff.data(), sizeof(uint64_t) * (G + 1));
@@ -466,6 +473,8 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_chunkGraph, C);
   rc |= dalloc(h, &h->d_gChunkBegin, G);
   rc |= dalloc(h, &h->d_gChunkEnd, G);
+  rc |= dalloc(h, &h->d_attrLight, light.size());
+  rc |= dalloc(h, &h->d_attrHeavy, heavy.size());
   rc |= dalloc(h, &h->d_pos, Vs);
   rc |= dalloc(h, &h->d_sf, Vs);
   rc |= dalloc(h, &h->d_sfOld, Vs);
@@ -557,6 +566,8 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   up(h->d_chunkGraph, cg.data(), cg.size() * 4);
   up(h->d_gChunkBegin, gcb.data(), G * 4);
   up(h->d_gChunkEnd, gce.data(), G * 4);
+  up(h->d_attrLight, light.data(), light.size() * 4);
+  up(h->d_attrHeavy, heavy.data(), heavy.size() * 4);
   ok = ok && cudaMemset(h->d_nCounter, 0, Vs * 4) == cudaSuccess;
   ok = ok && cudaMemset(h->d_pos, 0, Vs * 16) == cudaSuccess;
   ok = ok && cudaMemset(h->d_counters, 0, 32) == cudaSuccess;

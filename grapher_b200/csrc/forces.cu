@@ -45,36 +45,72 @@ struct Kahan {
 };
 
 struct AttrArgs {
-  const uint32_t *rowOff, *cols, *gid, *active;
+  const uint32_t *rowOff, *cols, *gid, *active, *list;
   const double2 *pos;
   float2 *out;
   float invK;
-  uint32_t V;
+  uint32_t n;  // entries of list
 };
 
+// one attraction term of vertex at p towards q
 template <int MODEL>
-__global__ __launch_bounds__(kAttrThreads) void k_attr_f32(AttrArgs a) {
-  const uint32_t v = blockIdx.x * kAttrThreads + threadIdx.x;
-  if (v >= a.V) return;
+__device__ __forceinline__ bool attr_term(const double2 p, const double2 q,
+                                          float invK, float &tx, float &ty) {
+  const float dx = (float)(q.x - p.x);
+  const float dy = (float)(q.y - p.y);
+  const float dist = sqrtf(dx * dx + dy * dy);
+  if (dist < 1e-9f) return false;
+  const float s = (MODEL == GVIZ_CUDA_MODEL_FR) ? dist * invK : log1pf(dist) / dist;
+  tx = s * dx;
+  ty = s * dy;
+  return true;
+}
+
+// Vertices with at most kHeavyDegree neighbours: one thread each.
+template <int MODEL>
+__global__ __launch_bounds__(kAttrThreads) void k_attr_f32_light(AttrArgs a) {
+  const uint32_t i = blockIdx.x * kAttrThreads + threadIdx.x;
+  if (i >= a.n) return;
+  const uint32_t v = a.list[i];
   if (a.active && !a.active[a.gid ? a.gid[v] : 0u]) return;
   const double2 p = a.pos[v];
   Kahan kx, ky;
   const uint32_t e1 = a.rowOff[v + 1];
   for (uint32_t e = a.rowOff[v]; e < e1; e++) {
-    const double2 q = a.pos[a.cols[e]];
-    const float dx = (float)(q.x - p.x);
-    const float dy = (float)(q.y - p.y);
-    const float dist = sqrtf(dx * dx + dy * dy);
-    if (dist < 1e-9f) continue;
-    float s;
-    if (MODEL == GVIZ_CUDA_MODEL_FR)
-      s = dist * a.invK;
-    else
-      s = log1pf(dist) / dist;
-    kx.add(s * dx);
-    ky.add(s * dy);
+    float tx, ty;
+    if (attr_term<MODEL>(p, a.pos[a.cols[e]], a.invK, tx, ty)) {
+      kx.add(tx);
+      ky.add(ty);
+    }
   }
   a.out[v] = make_float2((float)kx.value(), (float)ky.value());
+}
+
+// Hubs (scale-free graphs reach degrees in the thousands): one warp each,
+// lane-strided Kahan sums combined by a fixed shuffle tree in FP64.
+template <int MODEL>
+__global__ __launch_bounds__(kAttrThreads) void k_attr_f32_heavy(AttrArgs a) {
+  const uint32_t w = (blockIdx.x * kAttrThreads + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (w >= a.n) return;
+  const uint32_t v = a.list[w];
+  if (a.active && !a.active[a.gid ? a.gid[v] : 0u]) return;
+  const double2 p = a.pos[v];
+  Kahan kx, ky;
+  const uint32_t e1 = a.rowOff[v + 1];
+  for (uint32_t e = a.rowOff[v] + lane; e < e1; e += 32) {
+    float tx, ty;
+    if (attr_term<MODEL>(p, a.pos[a.cols[e]], a.invK, tx, ty)) {
+      kx.add(tx);
+      ky.add(ty);
+    }
+  }
+  double sx = kx.value(), sy = ky.value();
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+  }
+  if (lane == 0) a.out[v] = make_float2((float)sx, (float)sy);
 }
 
 struct WalkArgs {
@@ -286,11 +322,21 @@ void enqueue_attraction_f32(gvizCudaForce *h) {
   a.pos = h->d_pos;
   a.out = h->d_attF;
   a.invK = (float)(1.0 / h->params.edgeLength);
-  a.V = (uint32_t)h->V;
-  if (h->model == GVIZ_CUDA_MODEL_FR)
-    k_attr_f32<GVIZ_CUDA_MODEL_FR><<<blocks(h->V, kAttrThreads), kAttrThreads, 0, h->stream>>>(a);
-  else
-    k_attr_f32<GVIZ_CUDA_MODEL_LINLOG><<<blocks(h->V, kAttrThreads), kAttrThreads, 0, h->stream>>>(a);
+  const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
+  if (h->nAttrLight) {
+    a.list = h->d_attrLight;
+    a.n = h->nAttrLight;
+    const uint32_t g = blocks(a.n, kAttrThreads);
+    if (fr) k_attr_f32_light<GVIZ_CUDA_MODEL_FR><<<g, kAttrThreads, 0, h->stream>>>(a);
+    else k_attr_f32_light<GVIZ_CUDA_MODEL_LINLOG><<<g, kAttrThreads, 0, h->stream>>>(a);
+  }
+  if (h->nAttrHeavy) {
+    a.list = h->d_attrHeavy;
+    a.n = h->nAttrHeavy;
+    const uint32_t g = blocks((size_t)a.n * 32, kAttrThreads);
+    if (fr) k_attr_f32_heavy<GVIZ_CUDA_MODEL_FR><<<g, kAttrThreads, 0, h->stream>>>(a);
+    else k_attr_f32_heavy<GVIZ_CUDA_MODEL_LINLOG><<<g, kAttrThreads, 0, h->stream>>>(a);
+  }
   prof_mark(h, "attraction_f32");
 }
 

@@ -13,6 +13,7 @@
 #define GVIZ_FIX_MAX 4096        // largest deep run sorted in shared memory
 #define GVIZ_DIR_TABLE 256       // coincident-direction table entries
 #define GVIZ_STATS_CAP 4096      // stat rows kept per graph (ring)
+#define GVIZ_HEAVY_DEGREE 16     // attraction: warp per vertex above this
 
 // device status bits (OR-ed into ctx->d_status by kernels)
 #define GVIZ_ST_NONFINITE 1u
@@ -85,6 +86,10 @@ struct gvizCudaForce {
   double *d_meanDegPlusOne = nullptr;
   uint32_t *d_chunkBegin = nullptr, *d_chunkEnd = nullptr, *d_chunkGraph = nullptr;
   uint32_t *d_gChunkBegin = nullptr, *d_gChunkEnd = nullptr;
+  // attraction work lists: vertices of degree <= GVIZ_HEAVY_DEGREE get a
+  // thread, hubs above it a warp
+  uint32_t *d_attrLight = nullptr, *d_attrHeavy = nullptr;
+  uint32_t nAttrLight = 0, nAttrHeavy = 0;
 
   // --- layout state (device) ---
   double2 *d_pos = nullptr;

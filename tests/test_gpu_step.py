@@ -129,18 +129,29 @@ def test_one_step_matches_oracle(oracle, case):
 
 
 def test_free_run_fp64_tracks_oracle(oracle):
+    """Free-running (not teacher-forced) trajectories: the layout dynamics
+    amplify last-bit differences (centre-of-mass rounding) step after step, so
+    the bound is tight for a few steps and statistical after many."""
     from grapher_b200 import graphs
     a, b = graphs.grid(32, 32)
     row, col = csr_of(1024, a, b)
     deg, mass = degree_mass(row, 0)
-    c = cfg(model=0, theta=0.5, precision="fp64")
+    c = cfg(model=0, theta=0.5, precision="fp64", strict=True)
     x0 = graphs.randomize_positions(1024, 1.0, 7)
     pos_o, sf_o, ss_o = x0.copy(), np.zeros(2048), np.array([1.0, 1.0])
     lay = make_layout(row, col, c)
     lay.begin(0, positions=x0)
-    for _ in range(30):
+    for s in range(30):
         oracle.step((row, col), mass, deg, oracle_params(c), pos_o, sf_o, ss_o)
         lay.step()
-    p = lay.positions()
-    assert np.abs(p - pos_o).max() <= 1e-6 * max(1.0, np.abs(pos_o).max())
+        p = lay.positions()
+        scale = max(1.0, np.abs(pos_o).max())
+        if s < 5:
+            assert np.abs(p - pos_o).max() <= 1e-9 * scale, s
+    dp = np.abs(p - pos_o) / scale
+    assert np.median(dp) <= 1e-6 and dp.max() <= 1e-3
+    # the layouts agree as layouts: mean edge length within 0.1 %
+    e_gpu = np.linalg.norm(p.reshape(-1, 2)[a] - p.reshape(-1, 2)[b], axis=1).mean()
+    e_ref = np.linalg.norm(pos_o.reshape(-1, 2)[a] - pos_o.reshape(-1, 2)[b], axis=1).mean()
+    assert abs(e_gpu - e_ref) <= 1e-3 * e_ref
     lay.close()
