@@ -115,6 +115,7 @@ _SIGS = {
     "gvizCudaForceLastError": (C.c_int, [P]),
     "gvizCudaErrorString": (C.c_char_p, [C.c_int]),
     "gvizCudaForceSetStream": (C.c_int, [P, P]),
+    "gvizCudaFa2SpeedUpdateNoAlloc": (C.c_int, [P, P, P, SZ, D, P, P, P]),
     "gvizCudaGenGrid": (SZ, [SZ, SZ, U32P, U32P]),
     "gvizCudaGenRandomConnected": (SZ, [SZ, D, C.c_uint, U32P, U32P]),
     "gvizCudaGenBarabasiAlbert": (SZ, [SZ, C.c_uint32, C.c_uint64, U32P, U32P]),

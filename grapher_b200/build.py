@@ -31,6 +31,7 @@ SOURCES = {
     "tree.cu": [],
     "forces.cu": [],
     "precise.cu": ["--fmad=false"],
+    "noalloc.cu": ["--fmad=false"],
     "mlp.cu": [],
     "api.cu": [],
     "host_graphs.cpp": [],

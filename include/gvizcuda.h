@@ -220,6 +220,32 @@ const char *gvizCudaErrorString(int code);
 /* Lets a caller supply the CUDA stream (a cudaStream_t) the handle uses. */
 int gvizCudaForceSetStream(gvizCudaForce *h, void *stream);
 
+/* ---- allocation-free speed update ------------------------------------- */
+
+/* No counterpart in the reference. For callers that may not allocate device
+ * memory while they run (a per-frame render loop that must not stall on the
+ * device allocator, or a host program whose GPU memory belongs to another
+ * allocator): the ForceAtlas2 global speed update of one layout, computed
+ * from structForce and the previous round's structForce that the caller
+ * keeps in device memory. Writes swing_i = m_i |f - f_old| to d_swing (may
+ * be NULL) and updates d_speedState = {globalSpeed, speedEfficiency} in place
+ * with the rule of updateGlobalSpeed (src/embedders/gvizForceEmbedder.c:140-185).
+ * All pointers are device pointers; the work is enqueued on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream) and the call returns
+ * without waiting.
+ * Allocates nothing: its scratch is a 64 KiB array built into the library,
+ * which every GPU that loads the library holds until the process exits.
+ * Limit: vertexCount <= 4096 * 2048 (8,388,608); larger counts return
+ * GVIZ_CUDA_ERR_LIMIT. The first call on each device looks up that array's
+ * device address with the device current; make that first call before any
+ * stream capture. All calls share the array, so calls that overlap on the
+ * GPU (different streams without ordering between them) race. */
+int gvizCudaFa2SpeedUpdateNoAlloc(const double *d_structForce,
+                                  const double *d_oldStructForce,
+                                  const double *d_mass, size_t vertexCount,
+                                  double jitterTolerance, double *d_swing,
+                                  double *d_speedState, void *stream);
+
 /* ---- host helpers: workloads and initial placement ------------------- */
 
 /* Ordered undirected edge lists. Each returns the edge count; pass NULL
