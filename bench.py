@@ -1,12 +1,15 @@
 """Benchmark of the B200 force-layout step (libgvizcuda).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ba1m|grid32|er65k_exact]
+                    [--workload ba1m|batch4096|grid32|er65k_exact]
 
 Default workload (the headline configuration): Barabasi-Albert graph,
 n = 1,048,576, m = 4 (4,194,294 edges, seeded), LinLog with gravity 1.0 and
 degree-sized prevent-overlap (r = 1.0 * (1 + 0.5 sqrt(deg))), Barnes-Hut
 theta = 0.8, start uniform in [-1000, 1000]^2 (rand_r, seed 7), FP32 walk.
+batch4096: 4096 independent graphs, sizes log-uniform in [32, 8192], each an
+Erdos-Renyi graph (mean degree U[3,6]), a random tree or a square grid,
+FR theta = 0.7, laid out together in one handle (one step = every graph steps).
 
 A step is one full gvizForceEmbedderStep equivalent: quadtree rebuild,
 attraction, Barnes-Hut repulsion, gravity, FA2 speed and position update.
@@ -33,48 +36,96 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOADS = {
-    "ba1m": dict(kind="ba", V=1 << 20, m=4, model=1, theta=0.8, gravity=1.0,
-                 radius_base=1.0, radius_per_degree=0.5, overlap=True, box=1000.0, bh=True),
-    "grid32": dict(kind="grid", V=1024, model=0, theta=0.5, gravity=0.0, radius_base=0.0,
-                   radius_per_degree=0.0, overlap=False, box=1.0, bh=True),
-    "er65k_exact": dict(kind="er", V=65536, E=262144, model=0, theta=1.0, gravity=0.0,
-                        radius_base=0.0, radius_per_degree=0.0, overlap=False, box=1.0,
-                        bh=False),
-}
 SEED = 7
 FLOP_PER_INTERACTION = 20  # pair or pseudo-body term (GPU Gems 3 ch. 31 convention)
 
-
-def describe(w):
-    d = dict(w)
-    d["workload"] = {"ba": f"barabasi_albert n={w['V']} m={w.get('m')}",
-                     "grid": "grid 32x32", "er": f"erdos_renyi n={w['V']} m={w.get('E')}"}[w["kind"]]
-    d["model"] = "linlog" if w["model"] == 1 else "fr"
-    return d
-
-
-def make_edges(w):
-    from grapher_b200 import graphs
-    if w["kind"] == "ba":
-        return graphs.barabasi_albert(w["V"], w["m"], SEED)
-    if w["kind"] == "grid":
-        return graphs.grid(32, 32)
-    return graphs.erdos_renyi(w["V"], w["E"], SEED)
+SPECS = {
+    "ba1m": dict(model=1, theta=0.8, gravity=1.0, radius_base=1.0, radius_per_degree=0.5,
+                 overlap=True, bh=True),
+    "batch4096": dict(model=0, theta=0.7, gravity=0.0, radius_base=0.0,
+                      radius_per_degree=0.0, overlap=False, bh=True),
+    "grid32": dict(model=0, theta=0.5, gravity=0.0, radius_base=0.0, radius_per_degree=0.0,
+                   overlap=False, bh=True),
+    "er65k_exact": dict(model=0, theta=1.0, gravity=0.0, radius_base=0.0,
+                        radius_per_degree=0.0, overlap=False, bh=False),
+}
 
 
-def configure(lay, w):
-    lay.set_params(theta=w["theta"], gravityK=w["gravity"], radiusBase=w["radius_base"],
-                   radiusPerDegree=w["radius_per_degree"], preventOverlap=int(w["overlap"]),
-                   barnesHutEnabled=int(w["bh"]), precision=0)
-    lay.box_extent = w["box"]
+class Workload:
+    """Graphs (edge lists in gvizGraphAddEdge order), their combined CSR and
+    the initial positions; one entry per graph of a batch."""
 
+    def __init__(self, name):
+        from grapher_b200 import graphs
+        self.name = name
+        self.spec = SPECS[name]
+        self.graphs = []  # (V, a, b, box, seed)
+        if name == "ba1m":
+            V = 1 << 20
+            a, b = graphs.barabasi_albert(V, 4, SEED)
+            self.graphs.append((V, a, b, 1000.0, SEED))
+            self.desc = f"barabasi_albert n={V} m=4 edges={len(a)}"
+        elif name == "grid32":
+            a, b = graphs.grid(32, 32)
+            self.graphs.append((1024, a, b, 1.0, SEED))
+            self.desc = "grid 32x32"
+        elif name == "er65k_exact":
+            a, b = graphs.erdos_renyi(65536, 262144, SEED)
+            self.graphs.append((65536, a, b, None, SEED))
+            self.desc = "erdos_renyi n=65536 m=262144, unit disk"
+        else:
+            rng = np.random.default_rng(SEED)
+            for g in range(4096):
+                V = int(round(math.exp(rng.uniform(math.log(32), math.log(8192)))))
+                kind = int(rng.integers(3))
+                if kind == 0:
+                    m = int(round(V * rng.uniform(3.0, 6.0) / 2))
+                    a, b = graphs.erdos_renyi(V, m, 1000 + g)
+                elif kind == 1:
+                    a, b = graphs.random_connected(V, 0.0, 1000 + g)
+                else:
+                    s = max(1, int(round(math.sqrt(V))))
+                    V = s * s
+                    a, b = graphs.grid(s, s)
+                # the embedder's default box (src/embedders/gvizForceEmbedder.c:12-17)
+                self.graphs.append((V, a, b, 0.5 * math.sqrt(V) * 10.0, 1000 + g))
+            self.desc = "4096 graphs, V log-uniform [32, 8192], ER/random tree/grid"
+        self.G = len(self.graphs)
+        if self.G == 1:
+            V, a, b, _, _ = self.graphs[0]
+            self.row, self.col = graphs.to_csr(V, a, b)
+            self.goff = None
+        else:
+            self.row, self.col, self.goff = graphs.batch([(V, a, b) for V, a, b, _, _ in self.graphs])
+        self.V = int(self.row.shape[0] - 1)
+        xs = []
+        for V, a, b, box, seed in self.graphs:
+            xs.append(graphs.unit_disk_positions(V, seed) if box is None
+                      else graphs.randomize_positions(V, box, seed))
+        self.x0 = np.concatenate(xs)
 
-def initial_positions(w):
-    from grapher_b200 import graphs
-    if w["kind"] == "er":
-        return graphs.unit_disk_positions(w["V"], SEED)
-    return graphs.randomize_positions(w["V"], w["box"], SEED)
+    def configure(self, lay):
+        s = self.spec
+        lay.set_params(theta=s["theta"], gravityK=s["gravity"], radiusBase=s["radius_base"],
+                       radiusPerDegree=s["radius_per_degree"], preventOverlap=int(s["overlap"]),
+                       barnesHutEnabled=int(s["bh"]), precision=0)
+
+    def oracle_params(self):
+        from oracle.bindings import make_params
+        s = self.spec
+        return make_params(model=s["model"], theta=s["theta"], bh=s["bh"], gravity=s["gravity"],
+                           radius_base=s["radius_base"], radius_per_degree=s["radius_per_degree"],
+                           prevent_overlap=s["overlap"])
+
+    def config(self, args):
+        s = self.spec
+        return {"workload": f"{self.name}: {self.desc}", "model": "linlog" if s["model"] else "fr",
+                "theta": s["theta"], "barnes_hut": s["bh"], "gravity": s["gravity"],
+                "overlap_radius": (f"{s['radius_base']}*(1+{s['radius_per_degree']}*sqrt(deg))"
+                                   if s["overlap"] else None),
+                "graphs": self.G, "vertices": self.V, "seed": SEED, "precision": "fp32-walk",
+                "parallelism": f"replicas{args.gpus}",
+                "l2": "per-step working set > L2 (tree rebuilt every step)"}
 
 
 class ClockSampler:
@@ -95,8 +146,7 @@ class ClockSampler:
                 ["nvidia-smi", "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
                  "-i", str(self.device), "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except Exception:
             self.proc = None
         time.sleep(0.3)
@@ -141,99 +191,94 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------- reference CPU
-def reference_layout(w, a, b):
-    from oracle.bindings import Reference, make_params
+def reference_graph(w, g):
+    """The reference embedder for graph g of the workload, begun."""
+    from oracle.bindings import Reference
     ref = Reference()
-    lay = ref.create_edges(w["V"], a, b, w["model"])
-    p = make_params(model=w["model"], theta=w["theta"], bh=w["bh"], gravity=w["gravity"],
-                    radius_base=w["radius_base"], radius_per_degree=w["radius_per_degree"],
-                    prevent_overlap=w["overlap"])
-    lay.configure(p, w["box"])
-    lay.begin(SEED)
-    if w["kind"] == "er":
-        lay.set_positions(initial_positions(w))
+    V, a, b, box, seed = w.graphs[g]
+    lay = ref.create_edges(V, a, b, w.spec["model"])
+    lay.configure(w.oracle_params(), box if box else 0.0)
+    lay.begin(seed)
+    if box is None:
+        s = 2 * int(sum(x[0] for x in w.graphs[:g]))
+        lay.set_positions(w.x0[s:s + 2 * V])
     return ref, lay
 
 
-def cpu_baseline(w, a, b, budget_s=20.0, max_steps=5):
-    """The reference's own multithreaded step on this host, a bounded sample."""
+def reference_iteration_time(w, budget_s=20.0, max_steps=5):
+    """Seconds per iteration of the whole workload for the reference's own
+    multithreaded step (one embedder per graph, as gviz runs them), from a
+    bounded sample: up to max_steps steps, or for a batch the first graphs
+    until the budget is spent, scaled by vertex count to the whole batch."""
     from oracle.bindings import Reference
-    if Reference.available():
-        ref, lay = reference_layout(w, a, b)
+    t_start = time.perf_counter()
+    if w.G == 1:
+        ref, lay = reference_graph(w, 0)
         times = []
-        t_start = time.perf_counter()
         while len(times) < max_steps and time.perf_counter() - t_start < budget_s:
             times.append(float(lay.time_steps(1)[0]))
         lay.close()
-        v = len(times) / sum(times)
-        return {"value": v, "unit": "iters/s", "cores": ref.pool_threads(), "kind": "reference",
-                "sample": f"{len(times)} full reference steps (gvizForceEmbedderStep, "
-                          f"gvizThreadPool over {ref.pool_threads()} threads) of the same workload"}
-    from oracle.bindings import Oracle, make_params
-    from grapher_b200 import graphs
+        return float(np.mean(times)), ref.pool_threads(), (
+            f"{len(times)} full reference steps (gvizForceEmbedderStep, gvizThreadPool over "
+            f"{ref.pool_threads()} threads) of the same workload")
+    total, sampled_v, n = 0.0, 0, 0
+    threads = Reference().pool_threads()
+    while n < w.G and time.perf_counter() - t_start < budget_s:
+        _, lay = reference_graph(w, n)
+        total += float(np.mean(lay.time_steps(3)))
+        sampled_v += w.graphs[n][0]
+        lay.close()
+        n += 1
+    return total * w.V / sampled_v, threads, (
+        f"first {n} of {w.G} graphs, 3 reference steps each (one embedder per graph, "
+        f"gvizThreadPool over {threads} threads), scaled by vertex count to the batch")
+
+
+def cpu_baseline(w):
+    from oracle.bindings import Reference
+    if Reference.available():
+        t, cores, sample = reference_iteration_time(w)
+        return {"value": 1.0 / t, "unit": "iters/s", "cores": cores, "kind": "reference",
+                "sample": sample}
+    from oracle.bindings import Oracle
     o = Oracle()
-    row, col = graphs.to_csr(w["V"], a, b)
+    V, a, b, _, _ = w.graphs[0]
+    row, col = w.row, w.col
     deg = np.diff(row).astype(np.uint64)
-    mass = np.ones(w["V"]) if w["model"] == 0 else 1.0 + deg
-    p = make_params(model=w["model"], theta=w["theta"], bh=w["bh"], gravity=w["gravity"],
-                    radius_base=w["radius_base"], radius_per_degree=w["radius_per_degree"],
-                    prevent_overlap=w["overlap"])
-    pos = initial_positions(w)
-    sf = np.zeros(2 * w["V"])
-    ss = np.array([1.0, 1.0])
+    mass = np.ones(w.V) if w.spec["model"] == 0 else 1.0 + deg
+    pos, sf, ss = w.x0.copy(), np.zeros(2 * w.V), np.array([1.0, 1.0])
     t0 = time.perf_counter()
-    o.step((row, col), mass, deg, p, pos, sf, ss)
-    dt = time.perf_counter() - t0
-    return {"value": 1.0 / dt, "unit": "iters/s", "cores": 1, "kind": "port",
-            "sample": "1 step of the single-threaded oracle restatement (reference library absent)"}
+    o.step((row, col), mass, deg, w.oracle_params(), pos, sf, ss)
+    return {"value": 1.0 / (time.perf_counter() - t0), "unit": "iters/s", "cores": 1,
+            "kind": "port", "sample": "1 step of the single-thread oracle (reference library absent)"}
 
 
 def run_reference_arm(args, w):
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
+    if int(os.environ.get("RANK", "0")) != 0:
         return 0
-    a, b = make_edges(w)
     from oracle.bindings import Reference
-    if not Reference.available():
-        base = cpu_baseline(w, a, b)
-        line = {"impl": "reference", "metric": metric_name(w), "value": base["value"],
-                "unit": "iters/s", "n_gpus": args.gpus, "steps": 1, "warmup": 0,
-                "higher_is_better": True, "config": config_of(w, args), "cpu_baseline": base,
-                "e2e": {"value": base["value"], "unit": "iters/s", "h2d_bytes_per_step": 0,
-                        "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
-        return 0
-    ref, lay = reference_layout(w, a, b)
-    if args.warmup:
-        lay.time_steps(args.warmup)
-    t = lay.time_steps(args.steps)
-    lay.close()
-    v = args.steps / float(t.sum())
-    base = {"value": v, "unit": "iters/s", "cores": ref.pool_threads(), "kind": "reference",
-            "sample": f"{args.steps} full reference steps after {args.warmup} warm-up steps"}
-    line = {"impl": "reference", "metric": metric_name(w), "value": v, "unit": "iters/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * float(t.mean()), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_of(w, args),
-            "cpu_baseline": base,
-            "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line = {"impl": "reference", "metric": "layout iters/sec", "unit": "iters/s",
+            "n_gpus": args.gpus, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": w.config(args)}
+    if Reference.available() and w.G == 1:
+        ref, lay = reference_graph(w, 0)
+        if args.warmup:
+            lay.time_steps(args.warmup)
+        t = lay.time_steps(args.steps)
+        lay.close()
+        v = args.steps / float(t.sum())
+        line.update(steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * float(t.mean()))
+        base = {"value": v, "unit": "iters/s", "cores": ref.pool_threads(), "kind": "reference",
+                "sample": f"{args.steps} full reference steps after {args.warmup} warm-up steps"}
+    else:
+        base = cpu_baseline(w)
+        v = base["value"]
+        line.update(steps=1, warmup=0)
+    line.update(value=v, cpu_baseline=base,
+                e2e={"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
     print(json.dumps(line))
     return 0
-
-
-def metric_name(w):
-    return "layout iters/sec"
-
-
-def config_of(w, args):
-    d = describe(w)
-    return {"workload": d["workload"], "model": d["model"], "theta": w["theta"],
-            "barnes_hut": w["bh"], "gravity": w["gravity"],
-            "overlap_radius": (f"{w['radius_base']}*(1+{w['radius_per_degree']}*sqrt(deg))"
-                               if w["overlap"] else None),
-            "vertices": w["V"], "box_extent": w["box"], "seed": SEED, "precision": "fp32-walk",
-            "parallelism": f"replicas{args.gpus}",
-            "l2": "per-step working set > L2 (tree rebuilt every step, ~300 MB touched)"}
 
 
 # ---------------------------------------------------------------------- ours
@@ -243,11 +288,11 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ba1m", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="ba1m", choices=sorted(SPECS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    w = WORKLOADS[args.workload]
+    w = Workload(args.workload)
     if args.impl == "reference":
         return run_reference_arm(args, w)
 
@@ -263,13 +308,10 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from grapher_b200 import ForceLayout, graphs
-    a, b = make_edges(w)
-    row, col = graphs.to_csr(w["V"], a, b)
-    lay = ForceLayout(row, col, model=w["model"], device=local)
-    configure(lay, w)
-    x0 = initial_positions(w)
-    lay.begin(0, positions=x0)
+    from grapher_b200 import ForceLayout
+    lay = ForceLayout(w.row, w.col, model=w.spec["model"], graph_offsets=w.goff, device=local)
+    w.configure(lay)
+    lay.begin(0, positions=w.x0)
     for _ in range(args.warmup):
         lay.step()
 
@@ -277,22 +319,26 @@ def main():
         if dist:
             dist.barrier()
 
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
     ms = lay.time_steps(args.steps)
     barrier()
     clocks = sampler.stop()
-    if dist:
-        import torch
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms)
     value = world * args.steps / (ms / 1e3)
 
     # e2e: host buffers through gvizCudaForceStepHost
     import torch
-    V = w["V"]
+    V = w.V
     pinned = torch.empty(2 * V, dtype=torch.float64, pin_memory=True)
     pinned.numpy()[:] = lay.positions()
     xy = pinned.numpy()
@@ -302,13 +348,9 @@ def main():
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         lay.step_host(xy)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * e2e_steps / e2e_s, "unit": "iters/s",
-           "h2d_bytes_per_step": 16 * V, "d2h_bytes_per_step": 16 * V + 40,
+           "h2d_bytes_per_step": 16 * V, "d2h_bytes_per_step": 16 * V + 40 * w.G,
            "steps": e2e_steps, "timer": "host wall clock around synchronous calls"}
 
     # per-kernel breakdown and roofline of the dominant kernel
@@ -316,29 +358,31 @@ def main():
     kernels = lay.L.gvizCudaForceStepKernelCount(lay.h)
     inter, visits = lay.count_interactions()
     peaks, peak_src = load_peaks()
-    walk_ms = dict(prof).get("bh_walk_f32") or dict(prof).get("exact_f32")
+    pd = dict(prof)
+    kname = "bh_walk_f32" if w.spec["bh"] else "exact_f32"
+    walk_ms = pd.get(kname)
     step_ms = sum(t for _, t in prof)
     flops = FLOP_PER_INTERACTION * inter
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-    roofline = {"kernel": "bh_walk_f32" if w["bh"] else "exact_f32", "bound": "fp32",
-                "achieved": flops / (walk_ms * 1e-3) / 1e12, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": flops / (walk_ms * 1e-3) / 1e12 / fp32_peak,
-                "traffic": None,
-                "peak_source": "nominal FP32 (148 SM x 128 lanes x 2) at MEASURED_PEAKS sm_max_mhz",
+    achieved = flops / (walk_ms * 1e-3) / 1e12
+    roofline = {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 FLOP) at the "
+                               "MEASURED_PEAKS.json max SM clock (no measured FP32 figure)",
                 "algorithmic": f"{FLOP_PER_INTERACTION} FLOP x {inter} interactions per launch",
                 "share_of_step": walk_ms / step_ms, "warp_node_visits": visits}
 
     line = {
-        "metric": metric_name(w), "value": value, "unit": "iters/s", "n_gpus": world,
+        "metric": "layout iters/sec", "value": value, "unit": "iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": config_of(w, args), "clocks": clocks, "e2e": e2e,
+        "data": "synthetic", "config": w.config(args), "clocks": clocks, "e2e": e2e,
         "gpu_launches": kernels * args.steps, "kernels_per_step": kernels,
         "vertex_updates_per_s": value * V, "roofline": roofline,
         "kernel_ms": {k: round(v, 4) for k, v in prof}, "peaks": peak_src,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(w, a, b)
+        line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:
         print(json.dumps(line))
     lay.close()

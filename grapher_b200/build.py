@@ -66,6 +66,29 @@ def _compile(src: str, extra: list[str], hdr: float, verbose: bool) -> str:
     return obj
 
 
+ADAPTER_SRC = os.path.join(HERE, "gviz", "gvizCudaForceEmbedder.c")
+ADAPTER_LIB = os.path.join(LIBDIR, "libgvizcuda_gviz.so")
+
+
+def build_gviz_adapter(gviz_include: str | None = None) -> str | None:
+    """Compiles the gviz-side glue against gviz's headers. The gviz symbols
+    stay undefined: the program that loads it (gviz itself) provides them."""
+    inc = gviz_include or os.environ.get("GVIZ_INCLUDE") or "/root/reference/include"
+    if not os.path.isdir(inc):
+        return None
+    if os.path.exists(ADAPTER_LIB) and os.path.getmtime(ADAPTER_LIB) >= max(
+            os.path.getmtime(ADAPTER_SRC), os.path.getmtime(LIB),
+            os.path.getmtime(os.path.join(INCLUDE, "gvizCudaForceEmbedder.h"))):
+        return ADAPTER_LIB
+    cmd = ["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-include", "stdint.h",
+           "-I" + INCLUDE, "-I" + inc, ADAPTER_SRC, "-o", ADAPTER_LIB,
+           "-L" + LIBDIR, "-lgvizcuda", "-Wl,-rpath,$ORIGIN"]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError(f"adapter build failed: {' '.join(cmd)}\n{out.stdout}{out.stderr}")
+    return ADAPTER_LIB
+
+
 def build(verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
@@ -79,6 +102,7 @@ def build(verbose: bool = False) -> str:
         out = subprocess.run(cmd, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{out.stdout}{out.stderr}")
+    build_gviz_adapter()
     return LIB
 
 

@@ -14,6 +14,10 @@
 #define GVIZ_DIR_TABLE 256       // coincident-direction table entries
 #define GVIZ_STATS_CAP 4096      // stat rows kept per graph (ring)
 #define GVIZ_HEAVY_DEGREE 16     // attraction: warp per vertex above this
+// The radix sort orders the top 48 bits of the composite (graph, path) key:
+// 24 quadtree levels of one graph. Runs equal in those bits and longer than
+// the leaf capacity are finished by the shared-memory fix-up sort.
+#define GVIZ_SORT_SKIP_BITS 16
 
 // device status bits (OR-ed into ctx->d_status by kernels)
 #define GVIZ_ST_NONFINITE 1u

@@ -320,21 +320,27 @@ __global__ __launch_bounds__(kThreads) void k_fa2_chunks(Fa2Args a) {
 }
 
 // updateGlobalSpeed, src/embedders/gvizForceEmbedder.c:140-185, per graph
-__global__ void k_fa2_speed(Fa2Args a) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= a.G || !a.active[g]) return;
+// One block per graph; thread 0 applies the rule to the block's sums.
+__global__ __launch_bounds__(kThreads) void k_fa2_speed(Fa2Args a) {
+  __shared__ double sh[kThreads / 32];
+  const uint32_t g = blockIdx.x;
+  if (!a.active[g]) return;
   double totalSwing = 0.0, totalTraction = 0.0;
   if (a.strict) {
-    for (uint64_t v = a.graphOff[g]; v < a.graphOff[g + 1]; v++) {
-      totalSwing += a.swing[v];
-      totalTraction += a.trac[v];
-    }
+    if (threadIdx.x == 0)
+      for (uint64_t v = a.graphOff[g]; v < a.graphOff[g + 1]; v++) {
+        totalSwing += a.swing[v];
+        totalTraction += a.trac[v];
+      }
   } else {
-    for (uint32_t c = a.gChunkBegin[g]; c < a.gChunkEnd[g]; c++) {
+    for (uint32_t c = a.gChunkBegin[g] + threadIdx.x; c < a.gChunkEnd[g]; c += kThreads) {
       totalSwing += a.chunkStat[c].a;
       totalTraction += a.chunkStat[c].b;
     }
+    totalSwing = block_sum(totalSwing, sh);
+    totalTraction = block_sum(totalTraction, sh);
   }
+  if (threadIdx.x != 0) return;
   if (totalTraction < 1e-7) return;
   double speed = a.speed[g], eff = a.eff[g];
   const double n = (double)(a.graphOff[g + 1] - a.graphOff[g]);
@@ -395,25 +401,31 @@ __global__ __launch_bounds__(kThreads) void k_fa2_apply(Fa2Args a) {
   }
 }
 
-__global__ void k_fa2_stats(Fa2Args a) {
-  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= a.G || !a.active[g]) return;
+__global__ __launch_bounds__(kThreads) void k_fa2_stats(Fa2Args a) {
+  __shared__ double sh[kThreads / 32];
+  const uint32_t g = blockIdx.x;
+  if (!a.active[g]) return;
   double mx = 0.0, sAtt = 0.0, sRep = 0.0;
   if (a.strict) {
-    for (uint64_t v = a.graphOff[g]; v < a.graphOff[g + 1]; v++) {
-      const double2 o = a.applied[v];
-      const double nrm = sqrt(o.x * o.x + o.y * o.y);
-      if (nrm > mx) mx = nrm;
-      sAtt += a.att[v];
-      sRep += a.rep[v];
-    }
+    if (threadIdx.x == 0)
+      for (uint64_t v = a.graphOff[g]; v < a.graphOff[g + 1]; v++) {
+        const double2 o = a.applied[v];
+        const double nrm = sqrt(o.x * o.x + o.y * o.y);
+        if (nrm > mx) mx = nrm;
+        sAtt += a.att[v];
+        sRep += a.rep[v];
+      }
   } else {
-    for (uint32_t c = a.gChunkBegin[g]; c < a.gChunkEnd[g]; c++) {
+    for (uint32_t c = a.gChunkBegin[g] + threadIdx.x; c < a.gChunkEnd[g]; c += kThreads) {
       mx = fmax(mx, a.chunkStat[c].a);
       sAtt += a.chunkStat[c].b;
       sRep += a.chunkStat[c].c;
     }
+    mx = block_max(mx, sh);
+    sAtt = block_sum(sAtt, sh);
+    sRep = block_sum(sRep, sh);
   }
+  if (threadIdx.x != 0) return;
   const uint64_t n = a.graphOff[g + 1] - a.graphOff[g];
   const uint64_t it = a.iter[g];
   double *row = a.stats + ((it % GVIZ_STATS_CAP) * a.G + g) * 5;
@@ -553,11 +565,11 @@ void enqueue_exact_judge(gvizCudaForce *h, const uint32_t *d_targets, size_t n,
 
 void enqueue_fa2(gvizCudaForce *h) {
   Fa2Args a = make_fa2(h);
-  const uint32_t gb = blocks(h->G, 128);
+  const uint32_t G = (uint32_t)h->G;
   if (!h->params.strictReductions)
     k_fa2_chunks<<<h->nChunks, kThreads, 0, h->stream>>>(a);
-  k_fa2_speed<<<gb, 128, 0, h->stream>>>(a);
+  k_fa2_speed<<<G, kThreads, 0, h->stream>>>(a);
   k_fa2_apply<<<h->nChunks, kThreads, 0, h->stream>>>(a);
-  k_fa2_stats<<<gb, 128, 0, h->stream>>>(a);
+  k_fa2_stats<<<G, kThreads, 0, h->stream>>>(a);
   prof_mark(h, "fa2_update");
 }

@@ -99,6 +99,32 @@ __global__ __launch_bounds__(kTopThreads) void k_scan_top(uint32_t *tileSums,
   if (threadIdx.x == 0 && total) *total = tot;
 }
 
+// Whole scan in one block: each thread owns a contiguous run of ceil(n/1024)
+// entries (n <= kSingleMax), one launch instead of three.
+constexpr uint32_t kSingleMax = 1u << 13;  // one SM: only for small arrays
+
+__global__ __launch_bounds__(kTopThreads) void k_scan_single(
+    const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total) {
+  const uint32_t per = (n + kTopThreads - 1) / kTopThreads;
+  const uint32_t b = threadIdx.x * per;
+  uint32_t s = 0;
+  for (uint32_t j = 0; j < per; j++) {
+    const uint32_t i = b + j;
+    if (i < n) s += in[i];
+  }
+  uint32_t excl;
+  const uint32_t tot = block_exclusive_scan<kTopThreads>(s, excl);
+  for (uint32_t j = 0; j < per; j++) {
+    const uint32_t i = b + j;
+    if (i < n) {
+      const uint32_t t = in[i];
+      out[i] = excl;
+      excl += t;
+    }
+  }
+  if (threadIdx.x == 0 && total) *total = tot;
+}
+
 __global__ void k_scan_add(uint32_t *out, uint32_t n,
                            const uint32_t *__restrict__ tileSums) {
   uint32_t add = tileSums[blockIdx.x];
@@ -198,6 +224,10 @@ void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
     if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), h->stream);
     return;
   }
+  if (n <= kSingleMax) {
+    k_scan_single<<<1, kTopThreads, 0, h->stream>>>(in, out, (uint32_t)n, total);
+    return;
+  }
   uint32_t tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
   k_scan_tiles<<<tiles, kScanThreads, 0, h->stream>>>(in, out, (uint32_t)n,
                                                       h->d_scanTile);
@@ -206,14 +236,16 @@ void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
     k_scan_add<<<tiles, 256, 0, h->stream>>>(out, (uint32_t)n, h->d_scanTile);
 }
 
-// Stable sort by all 64 key bits; result ends in (keys, vals).
+// Stable sort by the key bits above GVIZ_SORT_SKIP_BITS (an even number of
+// 8-bit passes, so the result ends in (keys, vals)); keys equal in those bits
+// keep their input order.
 void radix_sort_pairs(gvizCudaForce *h, uint64_t *keys, uint32_t *vals,
                       uint64_t *keysAlt, uint32_t *valsAlt, size_t n) {
   if (n <= 1) return;
   uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
   uint64_t *ka = keys, *kb = keysAlt;
   uint32_t *va = vals, *vb = valsAlt;
-  for (int shift = 0; shift < 64; shift += 8) {
+  for (int shift = GVIZ_SORT_SKIP_BITS; shift < 64; shift += 8) {
     k_radix_hist<<<tiles, kSortThreads, 0, h->stream>>>(ka, (uint32_t)n, shift,
                                                         h->d_radixHist, tiles);
     scan_exclusive(h, h->d_radixHist, h->d_radixHist, (size_t)256 * tiles,

@@ -22,6 +22,8 @@
 // (mass == 0, :38-39).
 #include <math.h>
 
+#include <cuda/atomic>
+
 #include "internal.cuh"
 
 namespace {
@@ -70,20 +72,41 @@ __global__ __launch_bounds__(kThreads) void k_bbox_chunks(
   }
 }
 
-__global__ void k_graph_roots(const double4 *__restrict__ box,
-                              const uint32_t *__restrict__ gcb,
-                              const uint32_t *__restrict__ gce, GraphRoot *roots,
-                              uint32_t G, uint32_t *status) {
-  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= G) return;
+// One block per graph: min/max over the graph's chunk boxes (order-free, so
+// exact), then the root box of gvizQuadtreeBuild.
+__global__ __launch_bounds__(kThreads) void k_graph_roots(
+    const double4 *__restrict__ box, const uint32_t *__restrict__ gcb,
+    const uint32_t *__restrict__ gce, GraphRoot *roots, uint32_t G,
+    uint32_t *status) {
+  const uint32_t g = blockIdx.x;
   double mnx = INFINITY, mxx = -INFINITY, mny = INFINITY, mxy = -INFINITY;
-  for (uint32_t c = gcb[g]; c < gce[g]; c++) {
+  for (uint32_t c = gcb[g] + threadIdx.x; c < gce[g]; c += kThreads) {
     double4 r = box[c];
     mnx = fmin(mnx, r.x);
     mxx = fmax(mxx, r.y);
     mny = fmin(mny, r.z);
     mxy = fmax(mxy, r.w);
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = fmin(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+    mxx = fmax(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+    mny = fmin(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+    mxy = fmax(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+  }
+  __shared__ double4 wb[kThreads / 32];
+  if (lane_id() == 0) wb[threadIdx.x >> 5] = make_double4(mnx, mxx, mny, mxy);
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (int w = 1; w < kThreads / 32; w++) {
+    mnx = fmin(mnx, wb[w].x);
+    mxx = fmax(mxx, wb[w].y);
+    mny = fmin(mny, wb[w].z);
+    mxy = fmax(mxy, wb[w].w);
+  }
+  mnx = fmin(mnx, wb[0].x);
+  mxx = fmax(mxx, wb[0].y);
+  mny = fmin(mny, wb[0].z);
+  mxy = fmax(mxy, wb[0].w);
   GraphRoot R;
   if (!(mnx <= mxx)) {  // empty graph
     R.cx = 0.0;
@@ -163,7 +186,8 @@ __global__ __launch_bounds__(kThreads) void k_run_flags(
     const uint64_t *__restrict__ ck, uint32_t *flag, uint32_t V) {
   uint32_t s = blockIdx.x * kThreads + threadIdx.x;
   if (s >= V) return;
-  flag[s] = (s == 0 || ck[s] != ck[s - 1]) ? 1u : 0u;
+  flag[s] = (s == 0 || (ck[s] >> GVIZ_SORT_SKIP_BITS) !=
+                           (ck[s - 1] >> GVIZ_SORT_SKIP_BITS)) ? 1u : 0u;
 }
 
 __global__ __launch_bounds__(kThreads) void k_run_starts(
@@ -191,7 +215,9 @@ __global__ __launch_bounds__(kThreads) void k_run_classify(
     deep[2 * slot] = start;
     deep[2 * slot + 1] = len;
   } else if (len >= 2) {
-    uint64_t mask = gbits ? ~((1ull << gbits) - 1ull) : ~0ull;
+    // path bits covered by the sorted prefix of the composite key
+    const int covered = 64 - GVIZ_SORT_SKIP_BITS - gbits;
+    const uint64_t mask = covered >= 64 ? ~0ull : (~0ull << (64 - covered));
     for (uint32_t s = start; s < end; s++) {
       sHi[s] &= mask;
       sLo[s] = 0;
@@ -449,10 +475,11 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       *ux = make_uint2(GVIZ_NONE, 0u);
       return;
     }
-    __threadfence();
-    if (atomicAdd(a.nCounter + p, 1u) == 0u) return;
+    // release this child's sums / acquire the sibling's: the second thread
+    // to arrive combines both
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrivals(a.nCounter[p]);
+    if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
     a.nCounter[p] = 0u;
-    __threadfence();
     const uint32_t l = a.nLeft[p], r = a.nRight[p];
     double Ml, SXl, SYl, Mr, SXr, SYr;
     uint32_t cl, Tl, cr, Tr;
@@ -728,7 +755,7 @@ void enqueue_tree_build(gvizCudaForce *h) {
   k_bbox_chunks<<<h->nChunks, kThreads, 0, st>>>(h->d_pos, h->d_chunkBegin,
                                                   h->d_chunkEnd, h->d_chunkBox,
                                                   h->d_status);
-  k_graph_roots<<<(uint32_t)((h->G + 127) / 128), 128, 0, st>>>(
+  k_graph_roots<<<(uint32_t)h->G, kThreads, 0, st>>>(
       h->d_chunkBox, h->d_gChunkBegin, h->d_gChunkEnd, h->d_roots,
       (uint32_t)h->G, h->d_status);
   k_keys<<<blocks_for(V), kThreads, 0, st>>>(h->d_pos, h->d_gid, h->d_roots,

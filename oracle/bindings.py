@@ -208,7 +208,8 @@ class Reference:
     def __init__(self, path: str = REF_SO):
         if not os.path.exists(path):
             raise FileNotFoundError(path)
-        self.lib = C.CDLL(path)
+        # global symbols: glue libraries loaded later resolve gviz's API here
+        self.lib = C.CDLL(path, mode=C.RTLD_GLOBAL)
         L = self.lib
         for name in ("ref_create_edges", "ref_create_builtin"):
             getattr(L, name).restype = C.c_void_p
@@ -218,6 +219,7 @@ class Reference:
         L.ref_get_stats.restype = C.c_size_t
         L.ref_pool_threads.restype = C.c_long
         L.ref_quadtree_nodes.restype = C.c_size_t
+        L.ref_state.restype = C.c_void_p
         for name in ("ref_step", "ref_vertex_count", "ref_box_extent", "ref_begin",
                      "ref_init_result", "ref_run", "ref_release", "ref_configure",
                      "ref_get_csr", "ref_get_degree_mass", "ref_get_positions",
@@ -315,6 +317,12 @@ class RefLayout:
 
     def invoke_step_action(self):
         return self.L.ref_invoke_step_action(self.h)
+
+    def invoke_toggle_overlap(self):
+        return self.L.ref_invoke_toggle_overlap(self.h)
+
+    def state_ptr(self):
+        return C.c_void_p(self.L.ref_state(self.h))
 
     def run(self, max_iters, eps):
         return self.L.ref_run(self.h, C.c_size_t(max_iters), D(eps))

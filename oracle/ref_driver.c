@@ -79,6 +79,14 @@ refLayout *ref_create_builtin(int kind, size_t a, size_t b, double density,
 }
 
 int ref_init_result(refLayout *r) { return r->initRes; }
+
+/* The embedder state, for glue that attaches to it (gvizForceEmbedderState *). */
+void *ref_state(refLayout *r) { return &r->s; }
+
+int ref_invoke_toggle_overlap(refLayout *r) {
+  return gvizEmbeddedGraphInvokeAction((gvizEmbeddedGraph *)&r->s,
+                                       "forceEmbedder.toggleOverlapPrevention", NULL);
+}
 size_t ref_vertex_count(refLayout *r) { return r->s.vertexCount; }
 
 void ref_configure(refLayout *r, const refParams *p, double boxExtent) {
