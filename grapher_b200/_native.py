@@ -50,6 +50,7 @@ class ForceParams(C.Structure):
         ("jitterTolerance", C.c_double),
         ("strictReductions", C.c_int32),
         ("farField", C.c_int32),
+        ("farGroupSpread", C.c_double),
     ]
 
 
@@ -109,6 +110,7 @@ _SIGS = {
     "gvizCudaForceExactRepulsion": (C.c_int, [P, U32P, SZ, DP]),
     "gvizCudaForceRepulsion": (C.c_int, [P, DP]),
     "gvizCudaForceCountInteractions": (C.c_int, [P, U64P, U64P]),
+    "gvizCudaForceCountFarRows": (C.c_int, [P, U64P, U64P]),
     "gvizCudaForceProfileStep": (C.c_int, [P, SZ, C.POINTER(C.c_char_p), DP]),
     "gvizCudaForceTimeSteps": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_float)]),
     "gvizCudaForceStepKernelCount": (C.c_int, [P]),
@@ -116,6 +118,22 @@ _SIGS = {
     "gvizCudaErrorString": (C.c_char_p, [C.c_int]),
     "gvizCudaForceSetStream": (C.c_int, [P, P]),
     "gvizCudaFa2SpeedUpdateNoAlloc": (C.c_int, [P, P, P, SZ, D, P, P, P]),
+    "gvizCudaMlpCreate": (C.c_int, [C.POINTER(P), C.c_int, C.c_uint64]),
+    "gvizCudaMlpDestroy": (None, [P]),
+    "gvizCudaMlpParamCount": (C.c_int, []),
+    "gvizCudaMlpSetWeights": (C.c_int, [P, C.POINTER(C.c_float)]),
+    "gvizCudaMlpGetWeights": (C.c_int, [P, C.POINTER(C.c_float)]),
+    "gvizCudaMlpGradient": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float), SZ, C.POINTER(C.c_float),
+                                      C.POINTER(C.c_float)]),
+    "gvizCudaMlpTrain": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), SZ, C.c_uint32, C.c_uint32,
+                                   C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "gvizCudaMlpInfer": (C.c_int, [P, C.POINTER(C.c_float), SZ, C.POINTER(C.c_float)]),
+    "gvizCudaForceSetFarFieldModel": (C.c_int, [P, P]),
+    "gvizCudaForceHarvestFarField": (C.c_int64, [P, U32P, SZ, D, C.POINTER(C.c_float),
+                                                 C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                                 U32P, SZ]),
     "gvizCudaGenGrid": (SZ, [SZ, SZ, U32P, U32P]),
     "gvizCudaGenRandomConnected": (SZ, [SZ, D, C.c_uint, U32P, U32P]),
     "gvizCudaGenBarabasiAlbert": (SZ, [SZ, C.c_uint32, C.c_uint64, U32P, U32P]),

@@ -332,6 +332,7 @@ void gvizCudaForceDefaultParams(gvizCudaForceParams *p) {
   p->jitterTolerance = 1.0;    // GVIZ_FORCE_EMBEDDER_JITTER_TOLERANCE_DEFAULT
   p->strictReductions = 0;
   p->farField = 0;
+  p->farGroupSpread = 0.25;
 }
 
 int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
@@ -602,6 +603,7 @@ void gvizCudaForceDestroy(gvizCudaForce *h) {
     if (h->profEv[i]) cudaEventDestroy(h->profEv[i]);
   free_all(h);
   mlp_free(h);
+  far_side_free(h);
   if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
   free(h->h_graphOff);
   free(h->h_meanDegPlusOne);
@@ -615,12 +617,17 @@ int gvizCudaForceSetParams(gvizCudaForce *h, const gvizCudaForceParams *p) {
   if (!(p->theta > 0.0) || !(p->edgeLength > 0.0) ||
       (p->precision != GVIZ_CUDA_FP32 && p->precision != GVIZ_CUDA_FP64))
     return set_err(h, GVIZ_CUDA_ERR_ARG);
-  if (p->farField && !h->d_mlp) return set_err(h, GVIZ_CUDA_ERR_ARG);
+  // the learned correction lives in the FP32 walk and needs a model
+  if (p->farField && (!h->d_mlp || p->precision != GVIZ_CUDA_FP32 || !p->barnesHutEnabled))
+    return set_err(h, GVIZ_CUDA_ERR_ARG);
+  if (!(p->farGroupSpread >= 0.0 && p->farGroupSpread <= 1.0))
+    return set_err(h, GVIZ_CUDA_ERR_ARG);
   DeviceGuard guard(h->device);
   const bool radiusChanged = p->preventOverlap != h->params.preventOverlap ||
                              p->radiusBase != h->params.radiusBase ||
                              p->radiusPerDegree != h->params.radiusPerDegree;
   h->params = *p;
+  h->farSide = p->farField != 0;
   h->graphDirty = true;
   if (radiusChanged) return upload_radius(h);
   return GVIZ_CUDA_OK;
@@ -970,16 +977,9 @@ int gvizCudaForceRepulsion(gvizCudaForce *h, double *out) {
   return rc;
 }
 
-int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
-                                   uint64_t *warpNodeVisits) {
-  if (!h) return GVIZ_CUDA_ERR_ARG;
-  DeviceGuard guard(h->device);
-  if (h->V == 0 || !h->params.barnesHutEnabled) {
-    const uint64_t n = h->V;
-    if (interactions) *interactions = h->params.barnesHutEnabled ? 0 : n * (n ? n - 1 : 0);
-    if (warpNodeVisits) *warpNodeVisits = 0;
-    return GVIZ_CUDA_OK;
-  }
+// One instrumented force evaluation: c = {pair interactions, warp node
+// visits, learned-correction group rows, lane rows}.
+static int count_walk(gvizCudaForce *h, uint64_t c[4]) {
   const gvizCudaForceParams saved = h->params;
   h->params.precision = GVIZ_CUDA_FP32;
   h->forceOnly = true;
@@ -991,10 +991,36 @@ int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
   h->forceOnly = false;
   h->params = saved;
   int rc = sync_and_check(h);
-  uint64_t c[2] = {0, 0};
-  cudaMemcpy(c, h->d_counters, 16, cudaMemcpyDeviceToHost);
+  if (cudaMemcpy(c, h->d_counters, 32, cudaMemcpyDeviceToHost) != cudaSuccess && !rc)
+    rc = set_err(h, GVIZ_CUDA_ERR_CUDA);
+  return rc;
+}
+
+int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
+                                   uint64_t *warpNodeVisits) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (h->V == 0 || !h->params.barnesHutEnabled) {
+    const uint64_t n = h->V;
+    if (interactions) *interactions = h->params.barnesHutEnabled ? 0 : n * (n ? n - 1 : 0);
+    if (warpNodeVisits) *warpNodeVisits = 0;
+    return GVIZ_CUDA_OK;
+  }
+  uint64_t c[4] = {0, 0, 0, 0};
+  const int rc = count_walk(h, c);
   if (interactions) *interactions = c[0];
   if (warpNodeVisits) *warpNodeVisits = c[1];
+  return rc;
+}
+
+int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows, uint64_t *laneRows) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  uint64_t c[4] = {0, 0, 0, 0};
+  int rc = GVIZ_CUDA_OK;
+  if (h->V > 0 && h->params.barnesHutEnabled && h->params.farField) rc = count_walk(h, c);
+  if (groupRows) *groupRows = c[2];
+  if (laneRows) *laneRows = c[3];
   return rc;
 }
 

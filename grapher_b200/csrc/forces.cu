@@ -17,6 +17,7 @@
 
 #include "epilogue.cuh"
 #include "internal.cuh"
+#include "mlp.cuh"
 
 int dir_table_upload_forces(const double *t) {
   return cudaMemcpyToSymbol(c_dirTable, t, sizeof(double) * 2 * GVIZ_DIR_TABLE) ==
@@ -226,6 +227,231 @@ __global__ __launch_bounds__(kWalkThreads) void k_walk_f32(WalkArgs a) {
   force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value(), ky.value());
 }
 
+// ---------------------------------------------------------------------------
+// The learned walk: as k_walk_f32, with two changes that define the learned
+// method (it has no reference counterpart): a cell containing the target is
+// never accepted, and every accepted cell's monopole force F gets the MLP's
+// correction p1 F + p2 rot90(F) (p is the relative correction in the frame
+// of F). The MLP runs on the tensor cores over 16-row tiles queued per warp
+// in shared memory, in two queues:
+//   group rows - the lanes that accept the current cell lie close together
+//     compared with their distance to it (spread <= farGroupSpread times the
+//     mean distance, and the cell passes the opening test from their
+//     centroid): one row with the features seen from the centroid serves
+//     all of them; each lane keeps its own F for that row;
+//   lane rows - otherwise one row per accepting lane.
+// Rows are applied in queue order, so the sums are deterministic.
+// ---------------------------------------------------------------------------
+
+constexpr int kFarThreads = 128;
+constexpr int kFarTile = 16;
+constexpr int kFarLaneCap = 48;  // a tile plus one warp's worth of overflow
+constexpr int kFarGroupMin = 3;  // fewer accepting lanes: lane rows
+
+struct FarArgs {
+  WalkArgs w;
+  const FarCell *cells;
+  const uint32_t *leafPre;
+  const MlpDev *mlp;
+  float spread2;  // farGroupSpread^2
+};
+
+struct __align__(16) FarWarpSmem {
+  __nv_bfloat16 gx[kFarTile * MLP_XS];     // group rows
+  __nv_bfloat16 lx[kFarLaneCap * MLP_XS];  // lane rows
+  float2 gF[kFarTile][32];                 // each lane's F in each group row
+  float2 lF[kFarLaneCap];                  // the owner's F of each lane row
+  float2 out[kFarTile];
+};
+
+__device__ __forceinline__ void far_put_row(__nv_bfloat16 *row, const float *f) {
+  uint4 lo, hi;
+  lo.x = pack_bf16(f[0], f[1]);
+  lo.y = pack_bf16(f[2], f[3]);
+  lo.z = pack_bf16(f[4], f[5]);
+  lo.w = pack_bf16(f[6], f[7]);
+  hi.x = pack_bf16(f[8], f[9]);
+  hi.y = hi.z = hi.w = 0u;
+  reinterpret_cast<uint4 *>(row)[0] = lo;
+  reinterpret_cast<uint4 *>(row)[1] = hi;
+}
+
+__device__ __forceinline__ void far_apply(float2 p, float2 F, float &cx, float &cy) {
+  cx += p.x * F.x - p.y * F.y;
+  cy += p.x * F.y + p.y * F.x;
+}
+
+__device__ __forceinline__ float warp_sum(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;  // the same bits in every lane: each step adds a commuted pair
+}
+
+__device__ __forceinline__ float warp_max(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+
+template <int MODEL, bool OVERLAP, bool COUNT>
+__global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
+  __shared__ MlpSmem W;
+  __shared__ FarWarpSmem Q[kFarThreads / 32];
+  mlp_stage(W, fa.mlp);
+  __syncthreads();
+  const WalkArgs &a = fa.w;
+  FarWarpSmem &q = Q[threadIdx.x >> 5];
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t s = ((blockIdx.x * kFarThreads + threadIdx.x) >> 5) * 32u + lane;
+  const bool valid = s < a.V;
+  const uint32_t v = valid ? a.idx[s] : 0u;
+  const uint32_t g = (valid && a.gid) ? a.gid[v] : 0u;
+  const bool act = valid && (a.active == nullptr || a.active[g] != 0u);
+  uint32_t resume = 0, myEnd = 0, myLeaf = 0;
+  float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
+  if (act) {
+    resume = a.graphBase[g];
+    myEnd = min(resume + a.rootT[g], a.maxNodes);
+    myLeaf = fa.leafPre[v];
+    const double2 p = a.pos[v];
+    ds_split(p.x, vxh, vxl);
+    ds_split(p.y, vyh, vyl);
+    mv = a.massF[v];
+    if (OVERLAP) rv = a.radiusF[v];
+  }
+  Kahan kx, ky;
+  float corrx = 0.f, corry = 0.f;
+  int qg = 0, ql = 0;  // warp-uniform queue lengths
+  uint64_t mine = 0;   // this lane's slots in the lane queue
+  unsigned long long nInter = 0, nVisit = 0, nGroup = 0, nLane = 0;
+  uint32_t nxt = resume < myEnd ? resume : kInf;
+  uint32_t cur = __reduce_min_sync(0xffffffffu, nxt);
+  while (cur != kInf) {
+    const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
+    const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+    const float nmass = n1.x, nsize = n1.y;
+    const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
+    const bool active = cur >= resume && cur < myEnd;
+    const float dx = (n0.x - vxh) + (n0.z - vxl);
+    const float dy = (n0.y - vyh) + (n0.w - vyl);
+    const float d2 = dx * dx + dy * dy;
+    const bool isLeaf = ninfo >= 0;
+    const bool massOk = nmass != 0.0f;
+    const uint32_t skip = max((uint32_t)nnext, cur + 1u);
+    const bool contains = cur <= myLeaf && myLeaf < skip;
+    const bool accept = !isLeaf && nsize < d2 && !contains;
+    const bool doForce = active && massOk && (isLeaf ? ((uint32_t)ninfo != v) : accept);
+    const bool open = active && massOk && !isLeaf && !accept;
+    float fx = 0.f, fy = 0.f;
+    if (__any_sync(0xffffffffu, doForce)) {
+      if (doForce) {
+        rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + (isLeaf ? nsize : 0.0f), a.num,
+                                 a.overlapC, v, isLeaf ? (uint32_t)ninfo : v, fx, fy);
+        kx.add(fx);
+        ky.add(fy);
+        if (COUNT) nInter++;
+      }
+    }
+    const bool wantMlp = doForce && !isLeaf;
+    const uint32_t ball = __ballot_sync(0xffffffffu, wantMlp);
+    if (ball) {
+      const FarCell c = fa.cells[cur];
+      const int k = __popc(ball);
+      bool grouped = false;
+      float gdx = 0.f, gdy = 0.f, gd2 = 0.f, grv = 0.f;
+      if (k >= kFarGroupMin && fa.spread2 > 0.0f) {
+        const float inv = 1.0f / (float)k;
+        gdx = warp_sum(wantMlp ? dx : 0.f) * inv;
+        gdy = warp_sum(wantMlp ? dy : 0.f) * inv;
+        if (OVERLAP) grv = warp_sum(wantMlp ? rv : 0.f) * inv;
+        gd2 = gdx * gdx + gdy * gdy;
+        const float ex = dx - gdx, ey = dy - gdy;
+        const float spread = warp_max(wantMlp ? ex * ex + ey * ey : 0.f);
+        grouped = spread <= fa.spread2 * gd2 && nsize < gd2;
+      }
+      if (grouped) {
+        float f[MLP_IN], e1x, e1y;
+        far_features(gdx, gdy, gd2, c, nmass, grv, f, e1x, e1y);
+        if (lane == 0) far_put_row(q.gx + qg * MLP_XS, f);
+        q.gF[qg][lane] = wantMlp ? make_float2(fx, fy) : make_float2(0.f, 0.f);
+        if (COUNT && lane == 0) nGroup++;
+        if (++qg == kFarTile) {
+          __syncwarp();
+          mlp_forward_tile(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
+          __syncwarp();
+#pragma unroll 4
+          for (int r = 0; r < kFarTile; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
+          __syncwarp();
+          qg = 0;
+        }
+      } else {
+        if (wantMlp) {
+          float f[MLP_IN], e1x, e1y;
+          far_features(dx, dy, d2, c, nmass, rv, f, e1x, e1y);
+          const int slot = ql + __popc(ball & ((1u << lane) - 1u));
+          far_put_row(q.lx + slot * MLP_XS, f);
+          q.lF[slot] = make_float2(fx, fy);
+          mine |= 1ull << slot;
+          if (COUNT) nLane++;
+        }
+        ql += k;
+        while (ql >= kFarTile) {
+          __syncwarp();
+          mlp_forward_tile(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
+          __syncwarp();
+          for (uint32_t m = (uint32_t)(mine & 0xffffu); m; m &= m - 1u) {
+            const int e = __ffs(m) - 1;
+            far_apply(q.out[e], q.lF[e], corrx, corry);
+          }
+          __syncwarp();
+          // move the rows past the tile (at most 31) to the front
+          for (int e = kFarTile + (int)lane; e < ql; e += 32) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(q.lx + e * MLP_XS);
+            uint4 *dst = reinterpret_cast<uint4 *>(q.lx + (e - kFarTile) * MLP_XS);
+            dst[0] = src[0];
+            dst[1] = src[1];
+            q.lF[e - kFarTile] = q.lF[e];
+          }
+          mine >>= kFarTile;
+          ql -= kFarTile;
+          __syncwarp();
+        }
+      }
+    }
+    if (active) resume = open ? cur + 1u : skip;
+    nxt = resume < myEnd ? resume : kInf;
+    if (COUNT) nVisit++;
+    cur = __reduce_min_sync(0xffffffffu, nxt);
+  }
+  if (qg > 0) {
+    __syncwarp();
+    mlp_forward_tile(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
+    __syncwarp();
+    for (int r = 0; r < qg; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
+  }
+  if (ql > 0) {
+    __syncwarp();
+    mlp_forward_tile(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
+    __syncwarp();
+    for (uint32_t m = (uint32_t)(mine & 0xffffu); m; m &= m - 1u) {
+      const int e = __ffs(m) - 1;
+      far_apply(q.out[e], q.lF[e], corrx, corry);
+    }
+  }
+  if (COUNT) {
+    atomicAdd(a.counters, nInter);
+    atomicAdd(a.counters + 3, nLane);
+    if (lane == 0) {
+      atomicAdd(a.counters + 1, nVisit);
+      atomicAdd(a.counters + 2, nGroup);
+    }
+  }
+  if (!act) return;
+  const float2 at = a.attF[v];
+  force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value() + (double)corrx,
+                 ky.value() + (double)corry);
+}
+
 struct ExactArgs {
   const double2 *pos;
   const float *massF, *radiusF;
@@ -347,6 +573,13 @@ static void launch_walk(gvizCudaForce *h, const WalkArgs &a) {
   k_walk_f32<MODEL, OVERLAP, COUNT><<<grid, kWalkThreads, 0, h->stream>>>(a);
 }
 
+template <int MODEL, bool OVERLAP>
+static void launch_far(gvizCudaForce *h, const FarArgs &fa, bool count) {
+  const uint32_t grid = blocks(((h->V + 31) / 32) * 32, kFarThreads);
+  if (count) k_walk_f32_far<MODEL, OVERLAP, true><<<grid, kFarThreads, 0, h->stream>>>(fa);
+  else k_walk_f32_far<MODEL, OVERLAP, false><<<grid, kFarThreads, 0, h->stream>>>(fa);
+}
+
 void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   WalkArgs a;
   a.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
@@ -367,6 +600,23 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   a.maxNodes = (uint32_t)h->maxNodes;
   const bool ov = h->params.preventOverlap != 0;
   const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
+  if (h->params.farField && h->d_mlp) {
+    FarArgs fa;
+    fa.w = a;
+    fa.cells = h->d_cells;
+    fa.leafPre = h->d_leafPre;
+    fa.mlp = reinterpret_cast<const MlpDev *>(h->d_mlp);
+    fa.spread2 = (float)(h->params.farGroupSpread * h->params.farGroupSpread);
+    if (fr) {
+      if (ov) launch_far<GVIZ_CUDA_MODEL_FR, true>(h, fa, counters != nullptr);
+      else launch_far<GVIZ_CUDA_MODEL_FR, false>(h, fa, counters != nullptr);
+    } else {
+      if (ov) launch_far<GVIZ_CUDA_MODEL_LINLOG, true>(h, fa, counters != nullptr);
+      else launch_far<GVIZ_CUDA_MODEL_LINLOG, false>(h, fa, counters != nullptr);
+    }
+    prof_mark(h, "bh_walk_f32_learned");
+    return;
+  }
   if (counters) {
     if (fr) {
       if (ov) launch_walk<GVIZ_CUDA_MODEL_FR, true, true>(h, a);

@@ -55,6 +55,17 @@ struct __align__(16) NodeD {
   int32_t pad0, pad1;
 };
 
+// Side record of a cell (same preorder index as its node record) for the
+// learned far-field correction and its training: the cell's second central
+// moments, the halfSize its opening test uses, the geometric centre relative
+// to the centre of mass, and its points' range in path-sorted order.
+struct __align__(16) FarCell {
+  float qxx, qxy, qyy;
+  float h;
+  float ox, oy;
+  uint32_t s0, s1;
+};
+
 struct ChunkStat {
   double a, b, c;  // generic partials
   double pad;
@@ -149,6 +160,10 @@ struct gvizCudaForce {
 
   // --- learned far-field (mlp.cu) ---
   void *d_mlp = nullptr;
+  bool farSide = false;             // build writes FarCell records
+  double4 *d_bQ = nullptr, *d_nQ = nullptr;
+  FarCell *d_cells = nullptr;       // maxNodes records
+  uint32_t *d_leafPre = nullptr;    // per vertex: preorder index of its leaf
 
   // --- CUDA graph of one step ---
   cudaGraphExec_t stepExec = nullptr;
@@ -229,6 +244,8 @@ void enqueue_tree_build(gvizCudaForce *h);
 void enqueue_tree_export(gvizCudaForce *h, int32_t *leafDepth);
 
 void mlp_free(gvizCudaForce *h);  // mlp.cu
+int far_side_alloc(gvizCudaForce *h);
+void far_side_free(gvizCudaForce *h);
 int dir_table_upload_forces(const double *t);
 int dir_table_upload_precise(const double *t);
 

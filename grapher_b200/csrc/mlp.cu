@@ -1,7 +1,831 @@
-// mlp.cu -- learned far-field correction (filled in by the far-field work).
-#include "internal.cuh"
+// mlp.cu -- learned far-field correction: training-pair harvest, BF16
+// tensor-core training (forward + backward + Adam) and batch inference.
+//
+// Training pairs come from this library's own tree: for sampled targets the
+// walk is replayed with the learned opening rule (theta test, and a cell that
+// contains the target is never accepted), and for every accepted cell the
+// exact FP64 force of its points (the all-pairs formula of
+// src/embedders/gvizForceEmbedder.c:104-115 restricted to the cell) is set
+// against its monopole (the pseudo-body term of :63-69).
+//
+// Training: mini-batch gradient of the weighted mean squared error of the
+// relative correction, one warp per block over 32-sample tiles; activations
+// and gradients pass through shared memory in BF16, every GEMM is
+// mma.sync m16n8k16 (BF16 in, FP32 accumulate); per-block gradient partials
+// are summed in block order (deterministic), then Adam on FP32 masters.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "mlp.cuh"
+
+// FP32 master layout (padded like MlpDev): w1t[64][16], b1[64], w2t[64][64],
+// b2[64], w3t[8][64], b3[8]
+#define MLP_PAD (MLP_HID * MLP_INP + MLP_HID + MLP_HID * MLP_HID + MLP_HID + MLP_OUTP * MLP_HID + MLP_OUTP)
+#define OFF_W1 0
+#define OFF_B1 (OFF_W1 + MLP_HID * MLP_INP)
+#define OFF_W2 (OFF_B1 + MLP_HID)
+#define OFF_B2 (OFF_W2 + MLP_HID * MLP_HID)
+#define OFF_W3 (OFF_B2 + MLP_HID)
+#define OFF_B3 (OFF_W3 + MLP_OUTP * MLP_HID)
+
+struct gvizCudaMlp {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  float *d_w = nullptr;      // FP32 masters (MLP_PAD)
+  float *d_m = nullptr, *d_v = nullptr;  // Adam moments
+  MlpDev *d_dev = nullptr;   // BF16 copy used by the kernels
+  float *d_grad = nullptr;   // per-block partials [blocks][MLP_PAD + 1]
+  float *d_gsum = nullptr;   // reduced gradient + loss
+  size_t gradBlocks = 0;
+  uint64_t step = 0;
+};
+
+namespace {
+
+constexpr int kTilesPerBlock = 4;
+
+__device__ __forceinline__ bool is_real_param(int i) {
+  if (i < OFF_B1) return (i % MLP_INP) < MLP_IN;          // w1t columns >= 10
+  if (i >= OFF_W3 && i < OFF_B3) return (i - OFF_W3) / MLP_HID < MLP_OUT;
+  if (i >= OFF_B3) return (i - OFF_B3) < MLP_OUT;
+  return true;
+}
+
+__global__ void k_mlp_to_dev(const float *w, MlpDev *d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= MLP_PAD) return;
+  const float x = is_real_param(i) ? w[i] : 0.f;
+  if (i < OFF_B1) d->w1t[i] = __float2bfloat16_rn(x);
+  else if (i < OFF_W2) d->b1[i - OFF_B1] = x;
+  else if (i < OFF_B2) d->w2t[i - OFF_W2] = __float2bfloat16_rn(x);
+  else if (i < OFF_W3) d->b2[i - OFF_B2] = x;
+  else if (i < OFF_B3) d->w3t[i - OFF_W3] = __float2bfloat16_rn(x);
+  else d->b3[i - OFF_B3] = x;
+}
+
+// Per-block shared layout of the training kernel (one warp per block).
+struct TrainSmem {
+  __nv_bfloat16 w1t[MLP_HID * MLP_INP];
+  __nv_bfloat16 w2t[MLP_HID * MLP_HID];
+  __nv_bfloat16 w3p[16 * MLP_HID];  // w3t padded to 16 rows (rows >= 8 zero)
+  float b1[MLP_HID], b2[MLP_HID], b3[MLP_OUTP];
+  __nv_bfloat16 x[32 * MLP_INP];
+  __nv_bfloat16 h1[32 * MLP_HID];
+  __nv_bfloat16 h2[32 * MLP_HID];
+  __nv_bfloat16 dy[32 * 16];
+  __nv_bfloat16 dh2[32 * MLP_HID];
+  __nv_bfloat16 dh1[32 * MLP_HID];
+  float g[MLP_PAD];  // gradient accumulator (same layout as the masters)
+  float loss;
+};
+
+// Gradient of sum_s w_s |Y_s - T_s|^2 * scale over `n` samples (through the
+// index list `order`, or in order when null).
+__global__ __launch_bounds__(32) void k_mlp_grad(const float *__restrict__ w,
+                                                 const float *__restrict__ X,
+                                                 const float *__restrict__ T,
+                                                 const float *__restrict__ Wt,
+                                                 const uint32_t *__restrict__ order,
+                                                 uint32_t n, float scale,
+                                                 float *partial) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  TrainSmem &S = *reinterpret_cast<TrainSmem *>(smraw);
+  const int l = threadIdx.x;
+  const int g = l >> 2, t = l & 3;
+  for (int i = l; i < MLP_HID * MLP_INP; i += 32)
+    S.w1t[i] = __float2bfloat16_rn((i % MLP_INP) < MLP_IN ? w[OFF_W1 + i] : 0.f);
+  for (int i = l; i < MLP_HID * MLP_HID; i += 32) S.w2t[i] = __float2bfloat16_rn(w[OFF_W2 + i]);
+  for (int i = l; i < 16 * MLP_HID; i += 32)
+    S.w3p[i] = __float2bfloat16_rn(i / MLP_HID < MLP_OUT ? w[OFF_W3 + i] : 0.f);
+  for (int i = l; i < MLP_HID; i += 32) {
+    S.b1[i] = w[OFF_B1 + i];
+    S.b2[i] = w[OFF_B2 + i];
+  }
+  if (l < MLP_OUTP) S.b3[l] = l < MLP_OUT ? w[OFF_B3 + l] : 0.f;
+  for (int i = l; i < MLP_PAD; i += 32) S.g[i] = 0.f;
+  if (l == 0) S.loss = 0.f;
+  __syncwarp();
+
+  const uint32_t nTiles = (n + 31) / 32;
+  const uint32_t tile0 = blockIdx.x * kTilesPerBlock;
+  for (uint32_t tile = tile0; tile < min(tile0 + kTilesPerBlock, nTiles); tile++) {
+    // ---- load 32 samples (row l) -------------------------------------
+    const uint32_t sIdx = tile * 32 + l;
+    const bool valid = sIdx < n;
+    const uint32_t src = valid ? (order ? order[sIdx] : sIdx) : 0u;
+    float tgt0 = 0.f, tgt1 = 0.f, wt = 0.f;
+#pragma unroll
+    for (int f = 0; f < MLP_INP; f++)
+      S.x[l * MLP_INP + f] = __float2bfloat16_rn(valid && f < MLP_IN ? X[(size_t)src * MLP_IN + f] : 0.f);
+    if (valid) {
+      tgt0 = T[(size_t)src * 2];
+      tgt1 = T[(size_t)src * 2 + 1];
+      wt = Wt ? Wt[src] : 1.f;
+    }
+#pragma unroll
+    for (int f = 0; f < 16; f++) S.dy[l * 16 + f] = __float2bfloat16_rn(0.f);
+    __syncwarp();
+    // ---- forward: layer 1 ------------------------------------------------
+    for (int mt = 0; mt < 2; mt++) {
+      uint32_t a[4];
+      load_a(a, S.x, MLP_INP, mt * 16, 0);
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        uint32_t b[2];
+        load_b_nk(b, S.w1t, MLP_INP, 0, nt * 8);
+        mma16816(c, a, b);
+        const int col = nt * 8 + 2 * t, r0 = mt * 16 + g;
+        S.h1[r0 * MLP_HID + col] = __float2bfloat16_rn(fmaxf(c[0] + S.b1[col], 0.f));
+        S.h1[r0 * MLP_HID + col + 1] = __float2bfloat16_rn(fmaxf(c[1] + S.b1[col + 1], 0.f));
+        S.h1[(r0 + 8) * MLP_HID + col] = __float2bfloat16_rn(fmaxf(c[2] + S.b1[col], 0.f));
+        S.h1[(r0 + 8) * MLP_HID + col + 1] = __float2bfloat16_rn(fmaxf(c[3] + S.b1[col + 1], 0.f));
+      }
+    }
+    __syncwarp();
+    // ---- layer 2 ---------------------------------------------------------
+    for (int mt = 0; mt < 2; mt++) {
+      uint32_t a[4][4];
+      for (int kt = 0; kt < 4; kt++) load_a(a[kt], S.h1, MLP_HID, mt * 16, kt * 16);
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 4; kt++) {
+          uint32_t b[2];
+          load_b_nk(b, S.w2t, MLP_HID, kt * 16, nt * 8);
+          mma16816(c, a[kt], b);
+        }
+        const int col = nt * 8 + 2 * t, r0 = mt * 16 + g;
+        S.h2[r0 * MLP_HID + col] = __float2bfloat16_rn(fmaxf(c[0] + S.b2[col], 0.f));
+        S.h2[r0 * MLP_HID + col + 1] = __float2bfloat16_rn(fmaxf(c[1] + S.b2[col + 1], 0.f));
+        S.h2[(r0 + 8) * MLP_HID + col] = __float2bfloat16_rn(fmaxf(c[2] + S.b2[col], 0.f));
+        S.h2[(r0 + 8) * MLP_HID + col + 1] = __float2bfloat16_rn(fmaxf(c[3] + S.b2[col + 1], 0.f));
+      }
+    }
+    __syncwarp();
+    // ---- layer 3, loss and dY ---------------------------------------------
+    __shared__ float yS[32 * 2];
+    for (int mt = 0; mt < 2; mt++) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+      for (int kt = 0; kt < 4; kt++) {
+        uint32_t a[4], b[2];
+        load_a(a, S.h2, MLP_HID, mt * 16, kt * 16);
+        load_b_nk(b, S.w3p, MLP_HID, kt * 16, 0);
+        mma16816(c, a, b);
+      }
+      if (t == 0) {
+        const int r0 = mt * 16 + g;
+        yS[r0 * 2] = c[0] + S.b3[0];
+        yS[r0 * 2 + 1] = c[1] + S.b3[1];
+        yS[(r0 + 8) * 2] = c[2] + S.b3[0];
+        yS[(r0 + 8) * 2 + 1] = c[3] + S.b3[1];
+      }
+    }
+    __syncwarp();
+    {
+      const float e0 = yS[l * 2] - tgt0, e1 = yS[l * 2 + 1] - tgt1;
+      const float d0 = 2.f * scale * wt * e0, d1 = 2.f * scale * wt * e1;
+      float ls = scale * wt * (e0 * e0 + e1 * e1);
+      S.dy[l * 16 + 0] = __float2bfloat16_rn(d0);
+      S.dy[l * 16 + 1] = __float2bfloat16_rn(d1);
+      float s0 = d0, s1 = d1;
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        ls += __shfl_xor_sync(0xffffffffu, ls, o);
+      }
+      if (l == 0) {
+        S.g[OFF_B3] += s0;
+        S.g[OFF_B3 + 1] += s1;
+        S.loss += ls;
+      }
+    }
+    __syncwarp();
+    // ---- dW3t[o][j] += sum_s dY[s][o] H2[s][j] ------------------------------
+    for (int nt = 0; nt < 8; nt++) {
+      float c[4] = {0.f, 0.f, 0.f, 0.f};
+      for (int kt = 0; kt < 2; kt++) {
+        uint32_t a[4], b[2];
+        load_a_t(a, S.dy, 16, 0, kt * 16);
+        load_b_kn(b, S.h2, MLP_HID, kt * 16, nt * 8);
+        mma16816(c, a, b);
+      }
+      const int col = nt * 8 + 2 * t;  // rows g (outputs 0..7); g+8 are padding
+      S.g[OFF_W3 + g * MLP_HID + col] += c[0];
+      S.g[OFF_W3 + g * MLP_HID + col + 1] += c[1];
+    }
+    // ---- dH2 = dY W3 (masked), db2 ------------------------------------------
+    for (int mt = 0; mt < 2; mt++) {
+      uint32_t a[4];
+      load_a(a, S.dy, 16, mt * 16, 0);
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        uint32_t b[2];
+        load_b_kn(b, S.w3p, MLP_HID, 0, nt * 8);
+        mma16816(c, a, b);
+        const int col = nt * 8 + 2 * t, r0 = mt * 16 + g;
+        const int i00 = r0 * MLP_HID + col, i10 = (r0 + 8) * MLP_HID + col;
+        const float v00 = __bfloat162float(S.h2[i00]) > 0.f ? c[0] : 0.f;
+        const float v01 = __bfloat162float(S.h2[i00 + 1]) > 0.f ? c[1] : 0.f;
+        const float v10 = __bfloat162float(S.h2[i10]) > 0.f ? c[2] : 0.f;
+        const float v11 = __bfloat162float(S.h2[i10 + 1]) > 0.f ? c[3] : 0.f;
+        S.dh2[i00] = __float2bfloat16_rn(v00);
+        S.dh2[i00 + 1] = __float2bfloat16_rn(v01);
+        S.dh2[i10] = __float2bfloat16_rn(v10);
+        S.dh2[i10 + 1] = __float2bfloat16_rn(v11);
+        float s0 = v00 + v10, s1 = v01 + v11;
+        for (int o = 4; o < 32; o <<= 1) {  // sum over g (lanes with equal t)
+          s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        }
+        if (g == 0) {
+          S.g[OFF_B2 + col] += s0;
+          S.g[OFF_B2 + col + 1] += s1;
+        }
+      }
+    }
+    __syncwarp();
+    // ---- dW2t[j2][j1] += sum_s dH2[s][j2] H1[s][j1] --------------------------
+    for (int mt = 0; mt < 4; mt++) {
+      uint32_t a[2][4];
+      for (int kt = 0; kt < 2; kt++) load_a_t(a[kt], S.dh2, MLP_HID, mt * 16, kt * 16);
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 2; kt++) {
+          uint32_t b[2];
+          load_b_kn(b, S.h1, MLP_HID, kt * 16, nt * 8);
+          mma16816(c, a[kt], b);
+        }
+        const int col = nt * 8 + 2 * t, r0 = mt * 16 + g;
+        S.g[OFF_W2 + r0 * MLP_HID + col] += c[0];
+        S.g[OFF_W2 + r0 * MLP_HID + col + 1] += c[1];
+        S.g[OFF_W2 + (r0 + 8) * MLP_HID + col] += c[2];
+        S.g[OFF_W2 + (r0 + 8) * MLP_HID + col + 1] += c[3];
+      }
+    }
+    // ---- dH1 = dH2 W2 (masked), db1 ------------------------------------------
+    for (int mt = 0; mt < 2; mt++) {
+      uint32_t a[4][4];
+      for (int kt = 0; kt < 4; kt++) load_a(a[kt], S.dh2, MLP_HID, mt * 16, kt * 16);
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 4; kt++) {
+          uint32_t b[2];
+          load_b_kn(b, S.w2t, MLP_HID, kt * 16, nt * 8);
+          mma16816(c, a[kt], b);
+        }
+        const int col = nt * 8 + 2 * t, r0 = mt * 16 + g;
+        const int i00 = r0 * MLP_HID + col, i10 = (r0 + 8) * MLP_HID + col;
+        const float v00 = __bfloat162float(S.h1[i00]) > 0.f ? c[0] : 0.f;
+        const float v01 = __bfloat162float(S.h1[i00 + 1]) > 0.f ? c[1] : 0.f;
+        const float v10 = __bfloat162float(S.h1[i10]) > 0.f ? c[2] : 0.f;
+        const float v11 = __bfloat162float(S.h1[i10 + 1]) > 0.f ? c[3] : 0.f;
+        S.dh1[i00] = __float2bfloat16_rn(v00);
+        S.dh1[i00 + 1] = __float2bfloat16_rn(v01);
+        S.dh1[i10] = __float2bfloat16_rn(v10);
+        S.dh1[i10 + 1] = __float2bfloat16_rn(v11);
+        float s0 = v00 + v10, s1 = v01 + v11;
+        for (int o = 4; o < 32; o <<= 1) {
+          s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+          s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        }
+        if (g == 0) {
+          S.g[OFF_B1 + col] += s0;
+          S.g[OFF_B1 + col + 1] += s1;
+        }
+      }
+    }
+    __syncwarp();
+    // ---- dW1t[j1][f] += sum_s dH1[s][j1] X[s][f] ------------------------------
+    for (int mt = 0; mt < 4; mt++) {
+      uint32_t a[2][4];
+      for (int kt = 0; kt < 2; kt++) load_a_t(a[kt], S.dh1, MLP_HID, mt * 16, kt * 16);
+      for (int nt = 0; nt < 2; nt++) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int kt = 0; kt < 2; kt++) {
+          uint32_t b[2];
+          load_b_kn(b, S.x, MLP_INP, kt * 16, nt * 8);
+          mma16816(c, a[kt], b);
+        }
+        const int col = nt * 8 + 2 * t, r0 = mt * 16 + g;
+        S.g[OFF_W1 + r0 * MLP_INP + col] += c[0];
+        S.g[OFF_W1 + r0 * MLP_INP + col + 1] += c[1];
+        S.g[OFF_W1 + (r0 + 8) * MLP_INP + col] += c[2];
+        S.g[OFF_W1 + (r0 + 8) * MLP_INP + col + 1] += c[3];
+      }
+    }
+    __syncwarp();
+  }
+  float *out = partial + (size_t)blockIdx.x * (MLP_PAD + 1);
+  for (int i = l; i < MLP_PAD; i += 32) out[i] = S.g[i];
+  if (l == 0) out[MLP_PAD] = S.loss;
+}
+
+// Sum of the per-block partials in block order.
+__global__ void k_mlp_reduce(const float *partial, uint32_t blocks, float *sum) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > MLP_PAD) return;
+  float s = 0.f;
+  for (uint32_t b = 0; b < blocks; b++) s += partial[(size_t)b * (MLP_PAD + 1) + i];
+  sum[i] = s;
+}
+
+__global__ void k_mlp_adam(float *w, float *m, float *v, const float *grad,
+                           float lr, float b1, float b2, float eps,
+                           float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= MLP_PAD) return;
+  if (!is_real_param(i)) {
+    w[i] = 0.f;
+    return;
+  }
+  const float gr = grad[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gr;
+  const float vi = b2 * v[i] + (1.f - b2) * gr * gr;
+  m[i] = mi;
+  v[i] = vi;
+  w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// Batch inference (tests, the error monitor): one warp per 32 rows.
+__global__ __launch_bounds__(128) void k_mlp_infer(const MlpDev *__restrict__ Wg,
+                                                   const float *__restrict__ X,
+                                                   uint32_t n, float *Y) {
+  __shared__ MlpSmem W;
+  __shared__ __align__(16) __nv_bfloat16 xs[4][32 * MLP_XS];
+  __shared__ float ys[4][32 * 2];
+  mlp_stage(W, Wg);
+  __syncthreads();
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  const uint32_t row = (blockIdx.x * 4 + w) * 32 + l;
+  for (int f = 0; f < MLP_INP; f++)
+    xs[w][l * MLP_XS + f] = __float2bfloat16_rn(row < n && f < MLP_IN ? X[(size_t)row * MLP_IN + f] : 0.f);
+  __syncwarp();
+  mlp_forward_tile(W, xs[w], MLP_XS, ys[w]);
+  mlp_forward_tile(W, xs[w] + 16 * MLP_XS, MLP_XS, ys[w] + 32);
+  __syncwarp();
+  if (row < n) {
+    Y[(size_t)row * 2] = ys[w][l * 2];
+    Y[(size_t)row * 2 + 1] = ys[w][l * 2 + 1];
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// harvest of training pairs (one warp per target, uniform traversal)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct HarvestArgs {
+  const NodeF *nodes;
+  const FarCell *cells;
+  const uint32_t *targets, *idx, *gid, *graphBase, *rootT, *leafPre;
+  const double2 *pos;
+  const double *mass, *radius;
+  float *feat, *tgt, *fmono;
+  uint32_t *vert, *count;
+  uint32_t n, cap, maxNodes;
+  double kk, overlapC;
+  int model;
+};
+
+// pair repulsion, reference formulas in FP64 (no coincident pairs here:
+// the target is never inside an accepted cell)
+__device__ __forceinline__ void pair64(const HarvestArgs &a, double vx, double vy,
+                                       double ux, double uy, double mv, double mu,
+                                       double rs, double &fx, double &fy) {
+  const double dx = ux - vx, dy = uy - vy;
+  const double dist = sqrt(dx * dx + dy * dy);
+  const double gap = dist - rs;
+  const double num = a.model == GVIZ_CUDA_MODEL_FR ? a.kk : mv * mu;
+  double mag = gap > 0.0 ? num / gap : num * a.overlapC;
+  if (a.model == GVIZ_CUDA_MODEL_FR) mag *= (double)(unsigned long long)mu;
+  if (dist > 0.0) {
+    fx -= mag * dx / dist;
+    fy -= mag * dy / dist;
+  }
+}
+
+__global__ __launch_bounds__(128) void k_far_harvest(HarvestArgs a) {
+  const uint32_t w = (blockIdx.x * 128 + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (w >= a.n) return;
+  const uint32_t v = a.targets[w];
+  const uint32_t g = a.gid ? a.gid[v] : 0u;
+  const uint32_t begin = a.graphBase[g], end = min(begin + a.rootT[g], a.maxNodes);
+  const uint32_t myLeaf = a.leafPre[v];
+  const double2 p = a.pos[v];
+  float vxh, vxl, vyh, vyl;
+  ds_split(p.x, vxh, vxl);
+  ds_split(p.y, vyh, vyl);
+  const double mv = a.mass[v], rv = a.radius[v];
+  uint32_t cur = begin;
+  while (cur < end) {
+    const NodeF n = a.nodes[cur];
+    if (n.info >= 0) {  // a single point: evaluated exactly by the walk
+      cur++;
+      continue;
+    }
+    const uint32_t next = max((uint32_t)n.next, cur + 1);
+    if (n.mass == 0.0f) {
+      cur = next;
+      continue;
+    }
+    const float dx = (n.xh - vxh) + (n.xl - vxl);
+    const float dy = (n.yh - vyh) + (n.yl - vyl);
+    const float d2 = dx * dx + dy * dy;
+    const bool containsTarget = cur <= myLeaf && myLeaf < next;
+    if (!(n.size < d2) || containsTarget) {
+      cur++;
+      continue;
+    }
+    // accepted: exact force of the cell's points (lane-strided, FP64)
+    const FarCell c = a.cells[cur];
+    double fx = 0.0, fy = 0.0;
+    for (uint32_t s = c.s0 + lane; s < c.s1; s += 32) {
+      const uint32_t u = a.idx[s];
+      const double2 q = a.pos[u];
+      pair64(a, p.x, p.y, q.x, q.y, mv, a.mass[u], rv + a.radius[u], fx, fy);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    }
+    if (lane == 0) {
+      const double comx = (double)n.xh + (double)n.xl, comy = (double)n.yh + (double)n.yl;
+      double mx = 0.0, my = 0.0;
+      pair64(a, p.x, p.y, comx, comy, mv, (double)n.mass, rv, mx, my);
+      const double fm = sqrt(mx * mx + my * my);
+      float f[MLP_IN], e1x, e1y;
+      far_features(dx, dy, d2, c, n.mass, (float)rv, f, e1x, e1y);
+      const uint32_t slot = atomicAdd(a.count, 1u);
+      if (slot < a.cap && fm > 0.0) {
+        for (int k = 0; k < MLP_IN; k++) a.feat[(size_t)slot * MLP_IN + k] = f[k];
+        const double ex = fx - mx, ey = fy - my;
+        a.tgt[(size_t)slot * 2] = (float)((ex * e1x + ey * e1y) / fm);
+        a.tgt[(size_t)slot * 2 + 1] = (float)((-ex * e1y + ey * e1x) / fm);
+        a.fmono[slot] = (float)fm;
+        a.vert[slot] = v;
+      }
+    }
+    cur = next;
+  }
+}
+
+}  // namespace
 
 void mlp_free(gvizCudaForce *h) {
   if (h->d_mlp) cudaFree(h->d_mlp);
   h->d_mlp = nullptr;
 }
+
+// far-field side arrays of a handle (allocated on first use)
+int far_side_alloc(gvizCudaForce *h) {
+  if (h->d_cells) return GVIZ_CUDA_OK;
+  const size_t Vs = h->V ? h->V : 1;
+  if (cudaMalloc(&h->d_bQ, Vs * sizeof(double4)) != cudaSuccess ||
+      cudaMalloc(&h->d_nQ, Vs * sizeof(double4)) != cudaSuccess ||
+      cudaMalloc(&h->d_cells, h->maxNodes * sizeof(FarCell)) != cudaSuccess ||
+      cudaMalloc(&h->d_leafPre, Vs * sizeof(uint32_t)) != cudaSuccess)
+    return GVIZ_CUDA_ERR_ALLOC;
+  return GVIZ_CUDA_OK;
+}
+
+void far_side_free(gvizCudaForce *h) {
+  cudaFree(h->d_bQ);
+  cudaFree(h->d_nQ);
+  cudaFree(h->d_cells);
+  cudaFree(h->d_leafPre);
+  h->d_bQ = h->d_nQ = nullptr;
+  h->d_cells = nullptr;
+  h->d_leafPre = nullptr;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" {
+
+int gvizCudaMlpCreate(gvizCudaMlp **out, int device, uint64_t seed) {
+  if (!out) return GVIZ_CUDA_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return GVIZ_CUDA_ERR_NO_DEVICE;
+  if (device < 0 || device >= ndev) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(device);
+  gvizCudaMlp *m = new (std::nothrow) gvizCudaMlp();
+  if (!m) return GVIZ_CUDA_ERR_ALLOC;
+  m->device = device;
+  if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&m->d_w, MLP_PAD * 4) != cudaSuccess ||
+      cudaMalloc(&m->d_m, MLP_PAD * 4) != cudaSuccess ||
+      cudaMalloc(&m->d_v, MLP_PAD * 4) != cudaSuccess ||
+      cudaMalloc(&m->d_dev, sizeof(MlpDev)) != cudaSuccess ||
+      cudaMalloc(&m->d_gsum, (MLP_PAD + 1) * 4) != cudaSuccess) {
+    gvizCudaMlpDestroy(m);
+    return GVIZ_CUDA_ERR_ALLOC;
+  }
+  // He-style initialisation from a seeded splitmix stream; zero biases
+  std::vector<float> w(MLP_PAD, 0.f);
+  uint64_t s = seed * 0x9e3779b97f4a7c15ULL + 1;
+  auto uni = [&s]() {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * 0x1.0p-53 * 2.0 - 1.0;
+  };
+  for (int j = 0; j < MLP_HID; j++)
+    for (int f = 0; f < MLP_IN; f++) w[OFF_W1 + j * MLP_INP + f] = (float)(uni() * sqrt(6.0 / MLP_IN));
+  for (int i = 0; i < MLP_HID * MLP_HID; i++) w[OFF_W2 + i] = (float)(uni() * sqrt(6.0 / MLP_HID));
+  for (int o = 0; o < MLP_OUT; o++)
+    for (int j = 0; j < MLP_HID; j++) w[OFF_W3 + o * MLP_HID + j] = (float)(uni() * 0.1 * sqrt(3.0 / MLP_HID));
+  int rc = gvizCudaMlpSetWeights(m, w.data());
+  if (rc) {
+    gvizCudaMlpDestroy(m);
+    return rc;
+  }
+  *out = m;
+  return GVIZ_CUDA_OK;
+}
+
+void gvizCudaMlpDestroy(gvizCudaMlp *m) {
+  if (!m) return;
+  cudaSetDevice(m->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  cudaFree(m->d_w);
+  cudaFree(m->d_m);
+  cudaFree(m->d_v);
+  cudaFree(m->d_dev);
+  cudaFree(m->d_grad);
+  cudaFree(m->d_gsum);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+}
+
+int gvizCudaMlpParamCount(void) { return MLP_PAD; }
+
+int gvizCudaMlpSetWeights(gvizCudaMlp *m, const float *w) {
+  if (!m || !w) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(m->device);
+  if (cudaMemcpy(m->d_w, w, MLP_PAD * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(m->d_m, 0, MLP_PAD * 4) != cudaSuccess ||
+      cudaMemset(m->d_v, 0, MLP_PAD * 4) != cudaSuccess)
+    return GVIZ_CUDA_ERR_CUDA;
+  m->step = 0;
+  k_mlp_to_dev<<<(MLP_PAD + 255) / 256, 256, 0, m->stream>>>(m->d_w, m->d_dev);
+  return cudaStreamSynchronize(m->stream) == cudaSuccess ? GVIZ_CUDA_OK : GVIZ_CUDA_ERR_CUDA;
+}
+
+int gvizCudaMlpGetWeights(gvizCudaMlp *m, float *w) {
+  if (!m || !w) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(m->device);
+  cudaStreamSynchronize(m->stream);
+  return cudaMemcpy(w, m->d_w, MLP_PAD * 4, cudaMemcpyDeviceToHost) == cudaSuccess
+             ? GVIZ_CUDA_OK : GVIZ_CUDA_ERR_CUDA;
+}
+
+static int mlp_grad_launch(gvizCudaMlp *m, const float *dX, const float *dT,
+                           const float *dW, const uint32_t *dOrder, uint32_t n,
+                           float scale) {
+  const uint32_t tiles = (n + 31) / 32;
+  const uint32_t blocks = (tiles + kTilesPerBlock - 1) / kTilesPerBlock;
+  if (blocks > m->gradBlocks) {
+    cudaFree(m->d_grad);
+    m->d_grad = nullptr;
+    if (cudaMalloc(&m->d_grad, (size_t)blocks * (MLP_PAD + 1) * 4) != cudaSuccess)
+      return GVIZ_CUDA_ERR_ALLOC;
+    m->gradBlocks = blocks;
+  }
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(TrainSmem));
+    attr = true;
+  }
+  k_mlp_grad<<<blocks, 32, sizeof(TrainSmem), m->stream>>>(m->d_w, dX, dT, dW, dOrder, n,
+                                                           scale, m->d_grad);
+  k_mlp_reduce<<<(MLP_PAD + 1 + 255) / 256, 256, 0, m->stream>>>(m->d_grad, blocks, m->d_gsum);
+  return GVIZ_CUDA_OK;
+}
+
+// Gradient of the weighted mean squared error over n samples (host arrays:
+// X n*10, T n*2, W n or NULL for unit weights). grad: MLP_PAD floats in the
+// master layout; loss: the weighted mean.
+int gvizCudaMlpGradient(gvizCudaMlp *m, const float *X, const float *T,
+                        const float *W, size_t n, float *grad, float *loss) {
+  if (!m || !X || !T || n == 0) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(m->device);
+  float *dX, *dT, *dW = nullptr;
+  double wsum = 0.0;
+  for (size_t i = 0; i < n; i++) wsum += W ? W[i] : 1.0;
+  if (cudaMalloc(&dX, n * MLP_IN * 4) != cudaSuccess || cudaMalloc(&dT, n * 8) != cudaSuccess)
+    return GVIZ_CUDA_ERR_ALLOC;
+  cudaMemcpy(dX, X, n * MLP_IN * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dT, T, n * 8, cudaMemcpyHostToDevice);
+  if (W) {
+    cudaMalloc(&dW, n * 4);
+    cudaMemcpy(dW, W, n * 4, cudaMemcpyHostToDevice);
+  }
+  int rc = mlp_grad_launch(m, dX, dT, dW, nullptr, (uint32_t)n, (float)(1.0 / wsum));
+  std::vector<float> gs(MLP_PAD + 1);
+  if (!rc && cudaMemcpyAsync(gs.data(), m->d_gsum, (MLP_PAD + 1) * 4, cudaMemcpyDeviceToHost,
+                             m->stream) == cudaSuccess &&
+      cudaStreamSynchronize(m->stream) == cudaSuccess) {
+    if (grad) memcpy(grad, gs.data(), MLP_PAD * 4);
+    if (loss) *loss = gs[MLP_PAD];
+  } else if (!rc) {
+    rc = GVIZ_CUDA_ERR_CUDA;
+  }
+  cudaFree(dX);
+  cudaFree(dT);
+  cudaFree(dW);
+  return rc;
+}
+
+// Adam training on n samples (host arrays as in gvizCudaMlpGradient):
+// `epochs` passes in mini-batches of `batch`, samples shuffled per epoch
+// with a seeded permutation. lossOut[epochs] (may be NULL) receives each
+// epoch's mean training loss.
+int gvizCudaMlpTrain(gvizCudaMlp *m, const float *X, const float *T,
+                     const float *W, size_t n, uint32_t epochs, uint32_t batch,
+                     float lr, uint64_t seed, float *lossOut) {
+  if (!m || !X || !T || n == 0 || batch == 0) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(m->device);
+  float *dX = nullptr, *dT = nullptr, *dW = nullptr;
+  uint32_t *dOrder = nullptr;
+  int rc = GVIZ_CUDA_OK;
+  if (cudaMalloc(&dX, n * MLP_IN * 4) != cudaSuccess || cudaMalloc(&dT, n * 8) != cudaSuccess ||
+      cudaMalloc(&dOrder, n * 4) != cudaSuccess || (W && cudaMalloc(&dW, n * 4) != cudaSuccess))
+    rc = GVIZ_CUDA_ERR_ALLOC;
+  std::vector<float> wn;
+  if (!rc) {
+    cudaMemcpy(dX, X, n * MLP_IN * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(dT, T, n * 8, cudaMemcpyHostToDevice);
+    if (W) cudaMemcpy(dW, W, n * 4, cudaMemcpyHostToDevice);
+  }
+  std::vector<uint32_t> order(n);
+  for (size_t i = 0; i < n; i++) order[i] = (uint32_t)i;
+  uint64_t s = seed ^ 0xD1B54A32D192ED03ULL;
+  auto rnd = [&s]() {
+    uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  };
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  std::vector<float> gs(MLP_PAD + 1);
+  for (uint32_t ep = 0; ep < epochs && !rc; ep++) {
+    for (size_t i = n - 1; i > 0; i--) std::swap(order[i], order[rnd() % (i + 1)]);
+    cudaMemcpyAsync(dOrder, order.data(), n * 4, cudaMemcpyHostToDevice, m->stream);
+    double epochLoss = 0.0;
+    for (size_t b0 = 0; b0 < n && !rc; b0 += batch) {
+      const uint32_t nb = (uint32_t)std::min<size_t>(batch, n - b0);
+      double wsum = 0.0;
+      for (uint32_t i = 0; i < nb; i++) wsum += W ? W[order[b0 + i]] : 1.0;
+      rc = mlp_grad_launch(m, dX, dT, dW, dOrder + b0, nb, (float)(1.0 / wsum));
+      if (rc) break;
+      m->step++;
+      const float c1 = 1.f - powf(b1, (float)m->step), c2 = 1.f - powf(b2, (float)m->step);
+      k_mlp_adam<<<(MLP_PAD + 255) / 256, 256, 0, m->stream>>>(m->d_w, m->d_m, m->d_v,
+                                                               m->d_gsum, lr, b1, b2, eps, c1, c2);
+      if (lossOut) {
+        float lv = 0.f;
+        cudaMemcpyAsync(&lv, m->d_gsum + MLP_PAD, 4, cudaMemcpyDeviceToHost, m->stream);
+        cudaStreamSynchronize(m->stream);
+        epochLoss += (double)lv * nb;
+      }
+    }
+    if (lossOut) lossOut[ep] = (float)(epochLoss / (double)n);
+  }
+  k_mlp_to_dev<<<(MLP_PAD + 255) / 256, 256, 0, m->stream>>>(m->d_w, m->d_dev);
+  if (cudaStreamSynchronize(m->stream) != cudaSuccess && !rc) rc = GVIZ_CUDA_ERR_CUDA;
+  cudaFree(dX);
+  cudaFree(dT);
+  cudaFree(dW);
+  cudaFree(dOrder);
+  return rc;
+}
+
+// Batch inference with the BF16 tensor-core forward pass: Y (n*2) from X (n*10).
+int gvizCudaMlpInfer(gvizCudaMlp *m, const float *X, size_t n, float *Y) {
+  if (!m || !X || !Y) return GVIZ_CUDA_ERR_ARG;
+  if (n == 0) return GVIZ_CUDA_OK;
+  cudaSetDevice(m->device);
+  float *dX, *dY;
+  if (cudaMalloc(&dX, n * MLP_IN * 4) != cudaSuccess || cudaMalloc(&dY, n * 8) != cudaSuccess)
+    return GVIZ_CUDA_ERR_ALLOC;
+  cudaMemcpy(dX, X, n * MLP_IN * 4, cudaMemcpyHostToDevice);
+  const uint32_t blocks = (uint32_t)((n + 127) / 128);
+  k_mlp_infer<<<blocks, 128, 0, m->stream>>>(m->d_dev, dX, (uint32_t)n, dY);
+  int rc = cudaStreamSynchronize(m->stream) == cudaSuccess ? GVIZ_CUDA_OK : GVIZ_CUDA_ERR_CUDA;
+  if (!rc) cudaMemcpy(Y, dY, n * 8, cudaMemcpyDeviceToHost);
+  cudaFree(dX);
+  cudaFree(dY);
+  return rc;
+}
+
+// Attaches a trained model to a layout (copies its BF16 weights).
+int gvizCudaForceSetFarFieldModel(gvizCudaForce *h, gvizCudaMlp *m) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(h->device);
+  if (!m) {
+    mlp_free(h);
+    h->params.farField = 0;  // nothing to apply any more
+    h->farSide = false;
+    h->graphDirty = true;
+    return GVIZ_CUDA_OK;
+  }
+  if (!h->d_mlp && cudaMalloc(&h->d_mlp, sizeof(MlpDev)) != cudaSuccess)
+    return GVIZ_CUDA_ERR_ALLOC;
+  cudaStreamSynchronize(m->stream);
+  if (cudaMemcpy(h->d_mlp, m->d_dev, sizeof(MlpDev), cudaMemcpyDeviceToDevice) != cudaSuccess)
+    return GVIZ_CUDA_ERR_CUDA;
+  int rc = far_side_alloc(h);
+  h->graphDirty = true;
+  return rc;
+}
+
+// Training pairs for the learned correction at opening threshold `theta`
+// on the current positions: for each listed target vertex, every accepted
+// cell gives features[10], the relative correction target[2] in the pair
+// frame, the monopole magnitude and the target vertex. Returns the number of
+// pairs found (may exceed cap; only cap are written).
+int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
+                                     size_t nTargets, double theta, float *features,
+                                     float *target, float *fmono, uint32_t *vertex,
+                                     size_t cap) {
+  if (!h || (nTargets && !targets)) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(h->device);
+  int rc = far_side_alloc(h);
+  if (rc) return rc;
+  const gvizCudaForceParams saved = h->params;
+  h->params.theta = theta;
+  h->params.precision = GVIZ_CUDA_FP32;
+  const bool savedSide = h->farSide;
+  h->farSide = true;
+  cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+  enqueue_tree_build(h);
+  h->farSide = savedSide;
+  h->params = saved;
+  uint32_t *dT = nullptr, *dCount = nullptr, *dV = nullptr;
+  float *dF = nullptr, *dG = nullptr, *dM = nullptr;
+  const size_t c = cap ? cap : 1;
+  if (cudaMalloc(&dT, (nTargets ? nTargets : 1) * 4) != cudaSuccess ||
+      cudaMalloc(&dCount, 4) != cudaSuccess || cudaMalloc(&dF, c * MLP_IN * 4) != cudaSuccess ||
+      cudaMalloc(&dG, c * 8) != cudaSuccess || cudaMalloc(&dM, c * 4) != cudaSuccess ||
+      cudaMalloc(&dV, c * 4) != cudaSuccess) {
+    rc = GVIZ_CUDA_ERR_ALLOC;
+  }
+  uint32_t count = 0;
+  if (!rc) {
+    cudaMemcpyAsync(dT, targets, nTargets * 4, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(dCount, 0, 4, h->stream);
+    HarvestArgs a;
+    a.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
+    a.cells = h->d_cells;
+    a.targets = dT;
+    a.idx = h->d_idx;
+    a.gid = h->d_gid;
+    a.graphBase = h->d_graphBase;
+    a.rootT = h->d_rootT;
+    a.leafPre = h->d_leafPre;
+    a.pos = h->d_pos;
+    a.mass = h->d_mass;
+    a.radius = h->d_radius;
+    a.feat = dF;
+    a.tgt = dG;
+    a.fmono = dM;
+    a.vert = dV;
+    a.count = dCount;
+    a.n = (uint32_t)nTargets;
+    a.cap = (uint32_t)cap;
+    a.maxNodes = (uint32_t)h->maxNodes;
+    a.kk = h->params.edgeLength * h->params.edgeLength;
+    a.overlapC = h->params.overlapConstant;
+    a.model = h->model;
+    if (nTargets)
+      k_far_harvest<<<(uint32_t)((nTargets * 32 + 127) / 128), 128, 0, h->stream>>>(a);
+    cudaMemcpyAsync(&count, dCount, 4, cudaMemcpyDeviceToHost, h->stream);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = GVIZ_CUDA_ERR_CUDA;
+  }
+  if (!rc) {
+    const size_t w = std::min<size_t>(count, cap);
+    if (features) cudaMemcpy(features, dF, w * MLP_IN * 4, cudaMemcpyDeviceToHost);
+    if (target) cudaMemcpy(target, dG, w * 8, cudaMemcpyDeviceToHost);
+    if (fmono) cudaMemcpy(fmono, dM, w * 4, cudaMemcpyDeviceToHost);
+    if (vertex) cudaMemcpy(vertex, dV, w * 4, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dT);
+  cudaFree(dCount);
+  cudaFree(dF);
+  cudaFree(dG);
+  cudaFree(dM);
+  cudaFree(dV);
+  return rc ? (int64_t)rc : (int64_t)count;
+}
+
+}  // extern "C"

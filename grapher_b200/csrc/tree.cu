@@ -410,8 +410,32 @@ struct BU {
   uint32_t *nCounter;
   double *bM, *bSX, *bSY, *nM, *nSX, *nSY;
   uint32_t *bCnt, *bT, *nCnt, *nT, *nFlag, *rootNode, *rootT, *status;
+  double4 *bQ, *nQ;  // second central moments {Qxx, Qxy, Qyy, -}, or null
   uint32_t V, k;
 };
+
+// second central moments of a child about its own centre of mass
+__device__ __forceinline__ double4 child_q(const BU &a, uint32_t c) {
+  const double4 *p = (c & GVIZ_LEAF_BIT) ? a.bQ + (c & ~GVIZ_LEAF_BIT) : a.nQ + c;
+  const double2 lo = __ldcg(reinterpret_cast<const double2 *>(p));
+  const double2 hi = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+  return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+// parallel-axis shift of a child's moments to the parent's centre of mass
+__device__ __forceinline__ void add_shifted(double4 &q, const double4 qc,
+                                            double M, double SX, double SY,
+                                            double px, double py) {
+  double cx = 0.0, cy = 0.0;
+  if (M > 1e-9 || M < -1e-9) {
+    cx = SX / M;
+    cy = SY / M;
+  }
+  const double dx = cx - px, dy = cy - py;
+  q.x += qc.x + M * dx * dx;
+  q.y += qc.y + M * dx * dy;
+  q.z += qc.z + M * dy * dy;
+}
 
 __device__ __forceinline__ void child_vals(const BU &a, uint32_t c, double &M,
                                            double &SX, double &SY,
@@ -455,6 +479,24 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
   }
   uint32_t cnt = end - start;
   uint32_t T = cnt == 1 ? 1u : 1u + cnt;
+  if (a.bQ) {
+    double cx = 0.0, cy = 0.0;
+    if (M > 1e-9 || M < -1e-9) {
+      cx = SX / M;
+      cy = SY / M;
+    }
+    double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (uint32_t s = start; s < end; s++) {
+      const uint32_t i = a.idx[s];
+      const double m = a.mass[i];
+      const double2 p = a.pos[i];
+      const double dx = p.x - cx, dy = p.y - cy;
+      q.x += m * dx * dx;
+      q.y += m * dx * dy;
+      q.z += m * dy * dy;
+    }
+    a.bQ[b] = q;
+  }
   a.bM[b] = M;
   a.bSX[b] = SX;
   a.bSY[b] = SY;
@@ -495,6 +537,17 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
                           ((dp - 32) >> 1) == ((a.nDelta[pp] - 32) >> 1);
     const bool collapsed = !absorbed && cnt <= a.k;
     T = absorbed ? Tl + Tr : (collapsed ? 1u + cnt : 1u + Tl + Tr);
+    if (a.nQ) {
+      double px = 0.0, py = 0.0;
+      if (M > 1e-9 || M < -1e-9) {
+        px = SX / M;
+        py = SY / M;
+      }
+      double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
+      add_shifted(q, child_q(a, l), Ml, SXl, SYl, px, py);
+      add_shifted(q, child_q(a, r), Mr, SXr, SYr, px, py);
+      a.nQ[p] = q;
+    }
     a.nM[p] = M;
     a.nSX[p] = SX;
     a.nSY[p] = SY;
@@ -539,7 +592,52 @@ struct EM {
   double theta;
   uint32_t V, k, maxNodes;
   int f64;
+  // far-field side records (null unless requested)
+  const double4 *bQ, *nQ;
+  const uint64_t *bHi, *bLo;
+  FarCell *cells;
+  uint32_t *leafPre;
 };
+
+// Geometric centre of the cell at `depth` on the path (hi, lo): the same
+// FP64 descent as k_keys (centres c +/- halfSize/2).
+__device__ void cell_center(const GraphRoot &R, uint64_t hi, uint64_t lo,
+                            int depth, double &cx, double &cy) {
+  cx = R.cx;
+  cy = R.cy;
+  double h = R.h0;
+  for (int d = 1; d <= depth; d++) {
+    const uint64_t q = d <= 32 ? (hi >> (64 - 2 * d)) & 3ull : (lo >> (128 - 2 * d)) & 3ull;
+    const double quarter = h / 2.0;
+    cx = (q & 1ull) ? cx + quarter : cx + (-quarter);
+    cy = (q & 2ull) ? cy + (-quarter) : cy + quarter;
+    h = quarter;
+  }
+}
+
+__device__ void put_far(const EM &a, uint32_t at, const GraphRoot &R,
+                        uint32_t keyBucket, int depth, double h, double4 q,
+                        double M, double SX, double SY, uint32_t s0,
+                        uint32_t s1) {
+  if (!a.cells || at >= a.maxNodes) return;
+  double comx = 0.0, comy = 0.0;
+  if (M > 1e-9 || M < -1e-9) {
+    comx = SX / M;
+    comy = SY / M;
+  }
+  double gx, gy;
+  cell_center(R, a.bHi[keyBucket], a.bLo[keyBucket], depth, gx, gy);
+  FarCell c;
+  c.qxx = (float)q.x;
+  c.qxy = (float)q.y;
+  c.qyy = (float)q.z;
+  c.h = (float)h;
+  c.ox = (float)(gx - comx);
+  c.oy = (float)(gy - comy);
+  c.s0 = s0;
+  c.s1 = s1;
+  a.cells[at] = c;
+}
 
 __device__ void put_cell(const EM &a, uint32_t at, double M, double SX,
                          double SY, double h, uint32_t next) {
@@ -584,6 +682,7 @@ __device__ void put_leaf(const EM &a, uint32_t at, uint32_t v) {
     atomicOr(a.status, GVIZ_ST_TREE);
     return;
   }
+  if (a.leafPre) a.leafPre[v] = at;
   double2 p = a.pos[v];
   if (a.f64) {
     NodeD n;
@@ -650,6 +749,11 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
     const int q = (a.nDelta[p] - 32) >> 1;
     put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], ldexp(R.h0, -q),
              pre + a.nT[p]);
+    if (a.cells) {
+      const uint32_t lb = a.nLast[p];
+      put_far(a, pre, R, fb, q, ldexp(R.h0, -q), a.nQ[p], a.nM[p], a.nSX[p],
+              a.nSY[p], a.bStart[fb], (lb + 1 < U) ? a.bStart[lb + 1] : a.V);
+    }
     return;
   }
   const uint32_t b = t - nInt;
@@ -671,6 +775,9 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
   const bool testable = c > a.k && qp < R.D - 1;
   const double h = testable ? ldexp(R.h0, -(R.D - 1)) : (double)INFINITY;
   put_cell(a, pre, a.bM[b], a.bSX[b], a.bSY[b], h, pre + 1 + c);
+  if (a.cells && testable)
+    put_far(a, pre, R, b, R.D - 1, h, a.bQ[b], a.bM[b], a.bSX[b], a.bSY[b], s0,
+            s0 + c);
   for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, a.idx[s0 + j]);
 }
 
@@ -737,6 +844,12 @@ EM make_em(gvizCudaForce *h) {
   a.V = (uint32_t)h->V;
   a.k = h->params.nodesPerCell;
   a.f64 = h->params.precision == GVIZ_CUDA_FP64;
+  a.bQ = h->farSide ? h->d_bQ : nullptr;
+  a.nQ = h->farSide ? h->d_nQ : nullptr;
+  a.bHi = h->d_bHi;
+  a.bLo = h->d_bLo;
+  a.cells = h->farSide ? h->d_cells : nullptr;
+  a.leafPre = h->farSide ? h->d_leafPre : nullptr;
   return a;
 }
 
@@ -817,6 +930,8 @@ void enqueue_tree_build(gvizCudaForce *h) {
   bu.status = h->d_status;
   bu.V = V;
   bu.k = h->params.nodesPerCell;
+  bu.bQ = h->farSide ? h->d_bQ : nullptr;
+  bu.nQ = h->farSide ? h->d_nQ : nullptr;
   k_bottom_up<<<blocks_for(V), kThreads, 0, st>>>(bu);
   scan_exclusive(h, h->d_rootT, h->d_graphBase, h->G, h->d_counts + 3);
   EM em = make_em(h);

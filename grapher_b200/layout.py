@@ -287,6 +287,14 @@ class ForceLayout:
                 "gvizCudaForceCountInteractions")
         return a.value, b.value
 
+    def count_far_rows(self):
+        """(shared rows, per-target rows) of MLP evaluations in one force
+        evaluation with the learned correction on."""
+        a, b = C.c_uint64(), C.c_uint64()
+        N.check(self.L.gvizCudaForceCountFarRows(self.h, C.byref(a), C.byref(b)),
+                "gvizCudaForceCountFarRows")
+        return a.value, b.value
+
     def profile_step(self):
         names = (C.c_char_p * 64)()
         ms = np.zeros(64)

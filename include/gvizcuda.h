@@ -90,6 +90,11 @@ typedef struct gvizCudaForceParams {
                                order like the reference's serial loops */
   int32_t farField;         /* 0: monopole; 1: learned correction (needs
                                gvizCudaForceSetFarFieldModel) */
+  double farGroupSpread;    /* learned correction: when the targets of one
+                               warp that accept a cell lie within this
+                               fraction of their mean distance to it from
+                               their centroid, one model evaluation at the
+                               centroid serves them all; 0: one per target */
 } gvizCudaForceParams;
 
 /* One step's entries of the five stat series the embedder appends
@@ -201,6 +206,12 @@ int gvizCudaForceRepulsion(gvizCudaForce *h, double *out);
 int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
                                    uint64_t *warpNodeVisits);
 
+/* With the learned correction on: the MLP rows one force evaluation runs,
+ * shared rows (one per warp and cell, evaluated at the centroid of the
+ * warp's accepting targets) and per-target rows. Zeros when it is off. */
+int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows,
+                              uint64_t *laneRows);
+
 /* Per-kernel device time of the last profiled step (CUDA events on the
  * handle's stream). names: up to cap C strings; ms: up to cap values. */
 int gvizCudaForceProfileStep(gvizCudaForce *h, size_t cap, const char **names,
@@ -219,6 +230,55 @@ const char *gvizCudaErrorString(int code);
 
 /* Lets a caller supply the CUDA stream (a cudaStream_t) the handle uses. */
 int gvizCudaForceSetStream(gvizCudaForce *h, void *stream);
+
+/* ---- learned far-field correction ------------------------------------- */
+
+/* No counterpart in the reference: a 10 -> 64 -> 64 -> 2 MLP (ReLU, BF16
+ * weights, FP32 accumulate on tensor cores) that predicts the relative
+ * correction of a Barnes-Hut pseudo-body force from the cell's offset,
+ * extent, mass and second moments, so a large opening threshold keeps the
+ * accuracy of a small one. Weights are MLP_PAD floats in the layout
+ * w1t[64][16] (input columns >= 10 unused), b1[64], w2t[64][64], b2[64],
+ * w3t[8][64] (rows >= 2 unused), b3[8] (entries >= 2 unused). */
+typedef struct gvizCudaMlp gvizCudaMlp;
+
+int gvizCudaMlpCreate(gvizCudaMlp **out, int device, uint64_t seed);
+void gvizCudaMlpDestroy(gvizCudaMlp *m);
+int gvizCudaMlpParamCount(void);
+int gvizCudaMlpSetWeights(gvizCudaMlp *m, const float *w);
+int gvizCudaMlpGetWeights(gvizCudaMlp *m, float *w);
+
+/* Gradient (master layout) and value of the weighted mean squared error
+ * sum_i W_i |MLP(X_i) - T_i|^2 / sum_i W_i over n samples (X n*10, T n*2,
+ * W n or NULL), from the BF16 tensor-core forward/backward kernels. */
+int gvizCudaMlpGradient(gvizCudaMlp *m, const float *X, const float *T,
+                        const float *W, size_t n, float *grad, float *loss);
+
+/* Adam on the same loss: `epochs` passes in mini-batches of `batch`,
+ * shuffled per epoch from `seed`; lossOut[epochs] may be NULL. */
+int gvizCudaMlpTrain(gvizCudaMlp *m, const float *X, const float *T,
+                     const float *W, size_t n, uint32_t epochs, uint32_t batch,
+                     float lr, uint64_t seed, float *lossOut);
+
+/* Batch inference: Y (n*2) from X (n*10). */
+int gvizCudaMlpInfer(gvizCudaMlp *m, const float *X, size_t n, float *Y);
+
+/* Uses (m != NULL) or stops using (m == NULL) a trained model in this
+ * layout's walk when params.farField is set: a cell is accepted when
+ * 2h/|c - v| < theta and it does not contain v, and its monopole force gets
+ * the model's correction. */
+int gvizCudaForceSetFarFieldModel(gvizCudaForce *h, gvizCudaMlp *m);
+
+/* Training pairs on the current positions at opening threshold theta: for
+ * each target vertex and each cell the learned walk accepts, the features
+ * (10), the exact relative correction (2, from the cell's points in FP64),
+ * the monopole magnitude and the target. Returns the number of pairs found;
+ * at most cap are written. */
+int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
+                                     size_t nTargets, double theta,
+                                     float *features, float *target,
+                                     float *fmono, uint32_t *vertex,
+                                     size_t cap);
 
 /* ---- allocation-free speed update ------------------------------------- */
 

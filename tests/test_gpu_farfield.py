@@ -1,0 +1,220 @@
+"""The learned far-field correction: the BF16 tensor-core training and
+inference kernels against the FP64 NumPy oracle (oracle/mlp_oracle.py, with
+BF16 rounding emulated where the kernels store BF16), the harvested training
+targets against the analytic quadrupole term, and what the trained network
+gains over the same walk without it, judged against exact FP64 all-pairs
+repulsion."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _model(seed=3):
+    from grapher_b200.farfield import FarFieldModel
+    return FarFieldModel(seed=seed)
+
+
+def _batch(n=1000, seed=0):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(0.0, 0.5, (n, 10)).astype(np.float32)
+    T = rng.normal(0.0, 0.2, (n, 2)).astype(np.float32)
+    W = rng.uniform(0.5, 2.0, n).astype(np.float32)
+    return X, T, W
+
+
+@pytest.mark.parametrize("n", [1, 17, 1000, 5000])
+def test_gradient_matches_oracle(n):
+    from oracle import mlp_oracle as MO
+    m = _model()
+    w = m.weights().astype(np.float64)
+    X, T, W = _batch(n)
+    loss, g = m.gradient(X, T, W)
+    lo, go = MO.loss_and_grad(w, X.astype(np.float64), T.astype(np.float64),
+                              W.astype(np.float64), bf=True)
+    # FP32 accumulation in a different order is the only difference left
+    assert abs(loss - lo) <= 1e-5 * abs(lo)
+    cos = float(np.dot(g, go) / (np.linalg.norm(g) * np.linalg.norm(go)))
+    assert cos > 0.99999
+    assert np.linalg.norm(g - go) <= 2e-3 * np.linalg.norm(go)
+    # padding entries of the master layout never receive gradient
+    assert np.all(g[go == 0.0] == 0.0)
+
+
+def test_gradient_unweighted_equals_unit_weights():
+    m = _model()
+    X, T, _ = _batch(300, 1)
+    l1, g1 = m.gradient(X, T, None)
+    l2, g2 = m.gradient(X, T, np.ones(300, np.float32))
+    assert l1 == l2 and np.array_equal(g1, g2)
+
+
+def test_inference_matches_oracle():
+    from oracle import mlp_oracle as MO
+    m = _model(5)
+    X, _, _ = _batch(4099, 2)   # not a multiple of the 32-row tiles
+    Y = m.infer(X)
+    Yo, _ = MO.forward(m.weights().astype(np.float64), X.astype(np.float64), bf=True)
+    assert np.max(np.abs(Y - Yo)) <= 1e-5 + 1e-4 * np.max(np.abs(Yo))
+
+
+def test_weights_round_trip_and_validation():
+    from grapher_b200._native import GvizCudaError
+    m = _model()
+    w = np.random.default_rng(4).normal(0, 0.1, m.nparams).astype(np.float32)
+    m.set_weights(w)
+    assert np.array_equal(m.weights(), w)
+    with pytest.raises(GvizCudaError):
+        m.gradient(np.zeros((0, 10), np.float32), np.zeros((0, 2), np.float32))
+
+
+def test_training_fits_quadrupole_law():
+    """Adam over the tensor-core gradient learns the leading 1/r correction
+    t = (f1, -f2) from random features."""
+    m = _model(7)
+    rng = np.random.default_rng(8)
+    X = rng.uniform(-0.3, 0.3, (20000, 10)).astype(np.float32)
+    T = np.stack([X[:, 1], -X[:, 2]], 1).astype(np.float32)
+    losses = m.train(X, T, None, epochs=30, batch=2048, lr=3e-3, seed=1)
+    assert np.all(np.isfinite(losses))
+    assert losses[-1] < 0.05 * losses[0]
+    assert m.gradient(X, T)[0] < 1e-2 * float(np.mean(np.sum(T * T, 1)))
+
+
+# ----------------------------------------------------------------- layouts
+def _ba_layout(V=1 << 15, steps=20, theta=0.5):
+    from grapher_b200 import ForceLayout, graphs
+    a, b = graphs.barabasi_albert(V, 4, 7)
+    row, col = graphs.to_csr(V, a, b)
+    lay = ForceLayout(row, col, model=1)
+    lay.set_params(theta=theta, gravityK=1.0, preventOverlap=0)
+    lay.begin(0, positions=graphs.randomize_positions(V, 1000.0, 7))
+    for _ in range(steps):
+        lay.step()
+    return lay
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """A 32K-vertex BA layout (LinLog + gravity) and a model trained on its
+    own harvested pairs at theta = 1.2 from two snapshots."""
+    from grapher_b200.farfield import harvest_training_set
+    lay = _ba_layout()
+    rng = np.random.default_rng(0)
+    Xs, Ts, Ws = [], [], []
+    for _ in range(2):
+        for _ in range(5):
+            lay.step()
+        t = np.sort(rng.choice(lay.V, 4096, replace=False)).astype(np.uint32)
+        X, T, W = harvest_training_set(lay, 1.2, t)
+        Xs.append(X), Ts.append(T), Ws.append(W)
+    m = _model(3)
+    m.train(np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws), epochs=40,
+            batch=4096, lr=2e-3, seed=2)
+    for _ in range(5):
+        lay.step()
+    targets = np.sort(rng.choice(lay.V, 2048, replace=False)).astype(np.uint32)
+    return lay, m, targets, lay.exact_repulsion(targets)
+
+
+def _nrms(lay, targets, exact):
+    rep = lay.repulsion()[targets]
+    return float(np.sqrt(np.sum((rep - exact) ** 2) / np.sum(exact ** 2)))
+
+
+def test_harvest_targets_follow_quadrupole(trained):
+    """For cells far away compared with their size the exact relative
+    correction is the quadrupole term (f1, -f2) up to O((h/d)^3)."""
+    from grapher_b200.farfield import harvest
+    lay, _, targets, _ = trained
+    X, T, M, Vx = harvest(lay, targets[:512], 1.2)
+    assert len(X) > 512 and np.all(np.isfinite(X)) and np.all(np.isfinite(T))
+    assert set(np.unique(Vx)) <= set(targets[:512].tolist())
+    far = X[:, 0] < 0.25
+    quad = np.stack([X[:, 1], -X[:, 2]], 1)
+    res = np.sqrt(np.mean(np.sum((T[far] - quad[far]) ** 2, 1)))
+    tr = np.sqrt(np.mean(np.sum(T[far] ** 2, 1)))
+    assert res < 0.35 * tr
+    assert np.all(M > 0)
+
+
+def test_zero_model_is_the_plain_walk(trained):
+    """With all weights zero the learned walk adds nothing; below
+    theta = 1/sqrt(2) no cell can contain its target, so it visits the same
+    cells as the plain walk and the forces agree bit for bit."""
+    lay, _, targets, _ = trained
+    z = _model(1)
+    z.set_weights(np.zeros(z.nparams, np.float32))
+    lay.set_params(theta=0.6, farField=0)
+    plain = lay.repulsion()
+    z.attach(lay)
+    for spread in (0.0, 0.25):
+        lay.set_params(theta=0.6, farField=1, farGroupSpread=spread)
+        assert np.array_equal(lay.repulsion(), plain)
+    lay.set_params(farField=0)
+
+
+@pytest.mark.parametrize("spread", [0.0, 0.25])
+def test_learned_correction_beats_monopole(trained, spread):
+    """The gain of the trained network: at theta = 1.2 its force error
+    against exact FP64 repulsion is well below that of the same walk with
+    the monopole alone."""
+    lay, m, targets, exact = trained
+    z = _model(1)
+    z.set_weights(np.zeros(z.nparams, np.float32))
+    z.attach(lay)
+    lay.set_params(theta=1.2, farField=1, farGroupSpread=spread)
+    e_mono = _nrms(lay, targets, exact)
+    m.attach(lay)
+    e_mlp = _nrms(lay, targets, exact)
+    lay.set_params(farField=0)
+    e_plain = _nrms(lay, targets, exact)
+    assert e_mlp < 0.5 * e_mono, (e_mlp, e_mono)
+    assert e_mlp < 0.5 * e_plain, (e_mlp, e_plain)
+
+
+def test_group_rows_cut_evaluations(trained):
+    lay, m, targets, exact = trained
+    m.attach(lay)
+    lay.set_params(theta=1.2, farField=1, farGroupSpread=0.0)
+    g0, l0 = lay.count_far_rows()
+    e0 = _nrms(lay, targets, exact)
+    lay.set_params(farGroupSpread=0.25)
+    g1, l1 = lay.count_far_rows()
+    e1 = _nrms(lay, targets, exact)
+    lay.set_params(farField=0)
+    assert g0 == 0 and l0 > 0
+    assert g1 > 0 and g1 + l1 < 0.75 * l0
+    assert e1 < 1.5 * e0
+
+
+def test_learned_steps_and_graph_replay(trained):
+    """Steps with the correction on run inside the captured step graph and
+    are deterministic: two layouts from the same state agree exactly."""
+    from grapher_b200 import graphs
+    _, m, _, _ = trained
+    outs = []
+    for _ in range(2):
+        lay = _ba_layout(V=4096, steps=3)
+        m.attach(lay)
+        lay.set_params(theta=1.2, farField=1)
+        for _ in range(5):
+            lay.step()
+        outs.append(lay.positions())
+    assert np.all(np.isfinite(outs[0]))
+    assert np.array_equal(outs[0], outs[1])
+
+
+def test_far_field_argument_checks(trained):
+    from grapher_b200._native import GvizCudaError
+    lay = _ba_layout(V=512, steps=1)
+    with pytest.raises(GvizCudaError):      # no model attached
+        lay.set_params(farField=1)
+    lay.set_params(farField=0)
+    _, m, _, _ = trained
+    m.attach(lay)
+    with pytest.raises(GvizCudaError):      # the correction is FP32 only
+        lay.set_params(farField=1, precision=1)
+    lay.set_params(farField=0, precision=0)
+    with pytest.raises(GvizCudaError):
+        lay.set_params(farField=1, farGroupSpread=-1.0)
