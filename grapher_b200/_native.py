@@ -110,7 +110,7 @@ _SIGS = {
     "gvizCudaForceExactRepulsion": (C.c_int, [P, U32P, SZ, DP]),
     "gvizCudaForceRepulsion": (C.c_int, [P, DP]),
     "gvizCudaForceCountInteractions": (C.c_int, [P, U64P, U64P]),
-    "gvizCudaForceCountFarRows": (C.c_int, [P, U64P, U64P]),
+    "gvizCudaForceCountFarRows": (C.c_int, [P, U64P, U64P, U64P]),
     "gvizCudaForceProfileStep": (C.c_int, [P, SZ, C.POINTER(C.c_char_p), DP]),
     "gvizCudaForceTimeSteps": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_float)]),
     "gvizCudaForceStepKernelCount": (C.c_int, [P]),

@@ -545,7 +545,7 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_graphBase, G);
   rc |= dalloc(h, &h->d_nodes, h->maxNodes * sizeof(NodeD));
   rc |= dalloc(h, &h->d_leafDepth, Vs);
-  rc |= dalloc(h, &h->d_counters, 4);
+  rc |= dalloc(h, &h->d_counters, 8);
   if (rc) {
     gvizCudaForceDestroy(h);
     return GVIZ_CUDA_ERR_ALLOC;
@@ -571,7 +571,7 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   up(h->d_attrHeavy, heavy.data(), heavy.size() * 4);
   ok = ok && cudaMemset(h->d_nCounter, 0, Vs * 4) == cudaSuccess;
   ok = ok && cudaMemset(h->d_pos, 0, Vs * 16) == cudaSuccess;
-  ok = ok && cudaMemset(h->d_counters, 0, 32) == cudaSuccess;
+  ok = ok && cudaMemset(h->d_counters, 0, 64) == cudaSuccess;
   if (!ok || upload_dir_table(h) || upload_radius(h)) {
     gvizCudaForceDestroy(h);
     return GVIZ_CUDA_ERR_CUDA;
@@ -978,12 +978,14 @@ int gvizCudaForceRepulsion(gvizCudaForce *h, double *out) {
 }
 
 // One instrumented force evaluation: c = {pair interactions, warp node
-// visits, learned-correction group rows, lane rows}.
-static int count_walk(gvizCudaForce *h, uint64_t c[4]) {
+// visits, learned-correction shared rows, lane rows, lane rows by cause:
+// too few accepting targets, spread too wide, centroid fails the opening
+// test, warp iterations that accepted a cell}.
+static int count_walk(gvizCudaForce *h, uint64_t c[8]) {
   const gvizCudaForceParams saved = h->params;
   h->params.precision = GVIZ_CUDA_FP32;
   h->forceOnly = true;
-  cudaMemsetAsync(h->d_counters, 0, 32, h->stream);
+  cudaMemsetAsync(h->d_counters, 0, 64, h->stream);
   cudaMemsetAsync(h->d_status, 0, 4, h->stream);
   enqueue_tree_build(h);
   enqueue_attraction_f32(h);
@@ -991,7 +993,7 @@ static int count_walk(gvizCudaForce *h, uint64_t c[4]) {
   h->forceOnly = false;
   h->params = saved;
   int rc = sync_and_check(h);
-  if (cudaMemcpy(c, h->d_counters, 32, cudaMemcpyDeviceToHost) != cudaSuccess && !rc)
+  if (cudaMemcpy(c, h->d_counters, 64, cudaMemcpyDeviceToHost) != cudaSuccess && !rc)
     rc = set_err(h, GVIZ_CUDA_ERR_CUDA);
   return rc;
 }
@@ -1006,21 +1008,23 @@ int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
     if (warpNodeVisits) *warpNodeVisits = 0;
     return GVIZ_CUDA_OK;
   }
-  uint64_t c[4] = {0, 0, 0, 0};
+  uint64_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   const int rc = count_walk(h, c);
   if (interactions) *interactions = c[0];
   if (warpNodeVisits) *warpNodeVisits = c[1];
   return rc;
 }
 
-int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows, uint64_t *laneRows) {
+int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows, uint64_t *laneRows,
+                              uint64_t *laneRowCause) {
   if (!h) return GVIZ_CUDA_ERR_ARG;
   DeviceGuard guard(h->device);
-  uint64_t c[4] = {0, 0, 0, 0};
+  uint64_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int rc = GVIZ_CUDA_OK;
   if (h->V > 0 && h->params.barnesHutEnabled && h->params.farField) rc = count_walk(h, c);
   if (groupRows) *groupRows = c[2];
   if (laneRows) *laneRows = c[3];
+  if (laneRowCause) memcpy(laneRowCause, c + 4, 3 * sizeof(uint64_t));
   return rc;
 }
 

@@ -233,20 +233,22 @@ __global__ __launch_bounds__(kWalkThreads) void k_walk_f32(WalkArgs a) {
 // never accepted, and every accepted cell's monopole force F gets the MLP's
 // correction p1 F + p2 rot90(F) (p is the relative correction in the frame
 // of F). The MLP runs on the tensor cores over 16-row tiles queued per warp
-// in shared memory, in two queues:
-//   group rows - the lanes that accept the current cell lie close together
-//     compared with their distance to it (spread <= farGroupSpread times the
-//     mean distance, and the cell passes the opening test from their
-//     centroid): one row with the features seen from the centroid serves
-//     all of them; each lane keeps its own F for that row;
-//   lane rows - otherwise one row per accepting lane.
-// Rows are applied in queue order, so the sums are deterministic.
+// in shared memory. The accepting lanes of a cell share a row where their
+// targets are close together compared with their distance to it:
+//   shared row - lanes within farGroupSpread * |c - g| of the warp's target
+//                centroid g (the cell must pass the opening test from g)
+//                share one row with the features seen from g; each keeps
+//                its own F for it;
+//   lane row   - one row per remaining accepting lane.
+// One feature pass serves both kinds. Rows are applied in queue order, so
+// the sums are deterministic. (Nearly every warp iteration accepts some
+// cell, so the per-iteration bookkeeping, not the tensor-core work, sets
+// the cost; finer groups, e.g. per quarter-warp, cut rows but cost more.)
 // ---------------------------------------------------------------------------
 
 constexpr int kFarThreads = 128;
 constexpr int kFarTile = 16;
 constexpr int kFarLaneCap = 48;  // a tile plus one warp's worth of overflow
-constexpr int kFarGroupMin = 3;  // fewer accepting lanes: lane rows
 
 struct FarArgs {
   WalkArgs w;
@@ -257,9 +259,9 @@ struct FarArgs {
 };
 
 struct __align__(16) FarWarpSmem {
-  __nv_bfloat16 gx[kFarTile * MLP_XS];     // group rows
+  __nv_bfloat16 gx[kFarTile * MLP_XS];     // shared rows
   __nv_bfloat16 lx[kFarLaneCap * MLP_XS];  // lane rows
-  float2 gF[kFarTile][32];                 // each lane's F in each group row
+  float2 gF[kFarTile][32];                 // each lane's F in each shared row
   float2 lF[kFarLaneCap];                  // the owner's F of each lane row
   float2 out[kFarTile];
 };
@@ -281,16 +283,34 @@ __device__ __forceinline__ void far_apply(float2 p, float2 F, float &cx, float &
   cy += p.x * F.y + p.y * F.x;
 }
 
-__device__ __forceinline__ float warp_sum(float x) {
+// sum over the aligned group of `width` lanes (16, 8, ...: xor offsets below
+// width); the same bits in every lane of the group
+template <int WIDTH>
+__device__ __forceinline__ double group_sum_d(double x) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-  return x;  // the same bits in every lane: each step adds a commuted pair
+  for (int o = WIDTH / 2; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
 }
 
-__device__ __forceinline__ float warp_max(float x) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
-  return x;
+// centroid (double-single) of the active lanes of an aligned lane group and
+// this lane's squared distance to it (INFINITY when inactive)
+template <int WIDTH, bool RADIUS>
+__device__ __forceinline__ void group_centroid(bool act, double2 p, float vxh, float vxl,
+                                               float vyh, float vyl, float rv, float &gxh,
+                                               float &gxl, float &gyh, float &gyl,
+                                               float &r2, float &grv) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t grp = WIDTH == 32 ? 0xffffffffu : (((1u << WIDTH) - 1u) << (lane & ~(WIDTH - 1u)));
+  const int na = __popc(__ballot_sync(0xffffffffu, act) & grp);
+  const double inv = na > 0 ? 1.0 / (double)na : 0.0;
+  ds_split(group_sum_d<WIDTH>(act ? p.x : 0.0) * inv, gxh, gxl);
+  ds_split(group_sum_d<WIDTH>(act ? p.y : 0.0) * inv, gyh, gyl);
+  grv = RADIUS ? (float)(group_sum_d<WIDTH>(act ? (double)rv : 0.0) * inv) : 0.f;
+  r2 = INFINITY;
+  if (act) {
+    const float ex = (vxh - gxh) + (vxl - gxl), ey = (vyh - gyh) + (vyl - gyl);
+    r2 = ex * ex + ey * ey;
+  }
 }
 
 template <int MODEL, bool OVERLAP, bool COUNT>
@@ -309,26 +329,36 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
   const bool act = valid && (a.active == nullptr || a.active[g] != 0u);
   uint32_t resume = 0, myEnd = 0, myLeaf = 0;
   float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
+  double2 pv = make_double2(0.0, 0.0);
   if (act) {
     resume = a.graphBase[g];
     myEnd = min(resume + a.rootT[g], a.maxNodes);
     myLeaf = fa.leafPre[v];
-    const double2 p = a.pos[v];
-    ds_split(p.x, vxh, vxl);
-    ds_split(p.y, vyh, vyl);
+    pv = a.pos[v];
+    ds_split(pv.x, vxh, vxl);
+    ds_split(pv.y, vyh, vyl);
     mv = a.massF[v];
     if (OVERLAP) rv = a.radiusF[v];
   }
+  // the warp's target centroid
+  float wxh, wxl, wyh, wyl, wr2, wrv;
+  group_centroid<32, OVERLAP>(act, pv, vxh, vxl, vyh, vyl, rv, wxh, wxl, wyh, wyl, wr2, wrv);
+  const float spread2 = fa.spread2;
+  const bool grouping = spread2 > 0.0f;
   Kahan kx, ky;
   float corrx = 0.f, corry = 0.f;
   int qg = 0, ql = 0;  // warp-uniform queue lengths
   uint64_t mine = 0;   // this lane's slots in the lane queue
-  unsigned long long nInter = 0, nVisit = 0, nGroup = 0, nLane = 0;
+  unsigned long long nInter = 0, nVisit = 0, nGroup = 0, nLane = 0, nEvent = 0;
+  unsigned long long nWhy[3] = {0, 0, 0};
   uint32_t nxt = resume < myEnd ? resume : kInf;
   uint32_t cur = __reduce_min_sync(0xffffffffu, nxt);
   while (cur != kInf) {
     const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
     const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+    // the cell's side record, fetched alongside (unused for leaves)
+    const float4 c0 = __ldg(reinterpret_cast<const float4 *>(fa.cells + cur));
+    const uint4 c1 = __ldg(reinterpret_cast<const uint4 *>(fa.cells + cur) + 1);
     const float nmass = n1.x, nsize = n1.y;
     const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
     const bool active = cur >= resume && cur < myEnd;
@@ -355,67 +385,83 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
     const bool wantMlp = doForce && !isLeaf;
     const uint32_t ball = __ballot_sync(0xffffffffu, wantMlp);
     if (ball) {
-      const FarCell c = fa.cells[cur];
-      const int k = __popc(ball);
-      bool grouped = false;
-      float gdx = 0.f, gdy = 0.f, gd2 = 0.f, grv = 0.f;
-      if (k >= kFarGroupMin && fa.spread2 > 0.0f) {
-        const float inv = 1.0f / (float)k;
-        gdx = warp_sum(wantMlp ? dx : 0.f) * inv;
-        gdy = warp_sum(wantMlp ? dy : 0.f) * inv;
-        if (OVERLAP) grv = warp_sum(wantMlp ? rv : 0.f) * inv;
-        gd2 = gdx * gdx + gdy * gdy;
-        const float ex = dx - gdx, ey = dy - gdy;
-        const float spread = warp_max(wantMlp ? ex * ex + ey * ey : 0.f);
-        grouped = spread <= fa.spread2 * gd2 && nsize < gd2;
-      }
-      if (grouped) {
-        float f[MLP_IN], e1x, e1y;
-        far_features(gdx, gdy, gd2, c, nmass, grv, f, e1x, e1y);
-        if (lane == 0) far_put_row(q.gx + qg * MLP_XS, f);
-        q.gF[qg][lane] = wantMlp ? make_float2(fx, fy) : make_float2(0.f, 0.f);
-        if (COUNT && lane == 0) nGroup++;
-        if (++qg == kFarTile) {
-          __syncwarp();
-          mlp_forward_tile(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
-          __syncwarp();
+      FarCell c;
+      c.qa = c0.x;
+      c.qb = c0.y;
+      c.tr = c0.z;
+      c.h = c0.w;
+      c.ox = __uint_as_float(c1.x);
+      c.oy = __uint_as_float(c1.y);
+      c.s0 = c1.z;
+      c.s1 = c1.w;
+      // the cell seen from the warp centroid (the same bits in every lane)
+      const float wdx = (n0.x - wxh) + (n0.z - wxl);
+      const float wdy = (n0.y - wyh) + (n0.w - wyl);
+      const float wd2 = wdx * wdx + wdy * wdy;
+      const bool seenW = nsize < wd2, closeW = wr2 <= spread2 * wd2;
+      uint32_t wball = __ballot_sync(0xffffffffu, wantMlp && grouping && seenW && closeW);
+      if (__popc(wball) < 2) wball = 0u;
+      const bool inW = (wball >> lane) & 1u;
+      const bool inL = wantMlp && !inW;
+      const uint32_t lball = ball & ~wball;
+      const int nG = wball ? 1 : 0;
+      if (nG > 0 && qg == kFarTile) {
+        __syncwarp();
+        mlp_forward_tile(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
+        __syncwarp();
 #pragma unroll 4
-          for (int r = 0; r < kFarTile; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
-          __syncwarp();
-          qg = 0;
-        }
-      } else {
-        if (wantMlp) {
-          float f[MLP_IN], e1x, e1y;
-          far_features(dx, dy, d2, c, nmass, rv, f, e1x, e1y);
-          const int slot = ql + __popc(ball & ((1u << lane) - 1u));
+        for (int r = 0; r < kFarTile; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
+        __syncwarp();
+        qg = 0;
+      }
+      // one feature pass: each lane for its own row
+      if (inW || inL) {
+        const float sdx = inW ? wdx : dx, sdy = inW ? wdy : dy, sd2 = inW ? wd2 : d2;
+        const float srv = OVERLAP ? (inW ? wrv : rv) : 0.f;
+        float f[MLP_IN], e1x, e1y;
+        far_features(sdx, sdy, sd2, c, srv, f, e1x, e1y);
+        if (inL) {
+          const int slot = ql + __popc(lball & ((1u << lane) - 1u));
           far_put_row(q.lx + slot * MLP_XS, f);
           q.lF[slot] = make_float2(fx, fy);
           mine |= 1ull << slot;
-          if (COUNT) nLane++;
+        } else if ((uint32_t)(__ffs(wball) - 1) == lane) {
+          far_put_row(q.gx + qg * MLP_XS, f);
         }
-        ql += k;
-        while (ql >= kFarTile) {
-          __syncwarp();
-          mlp_forward_tile(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
-          __syncwarp();
-          for (uint32_t m = (uint32_t)(mine & 0xffffu); m; m &= m - 1u) {
-            const int e = __ffs(m) - 1;
-            far_apply(q.out[e], q.lF[e], corrx, corry);
-          }
-          __syncwarp();
-          // move the rows past the tile (at most 31) to the front
-          for (int e = kFarTile + (int)lane; e < ql; e += 32) {
-            const uint4 *src = reinterpret_cast<const uint4 *>(q.lx + e * MLP_XS);
-            uint4 *dst = reinterpret_cast<uint4 *>(q.lx + (e - kFarTile) * MLP_XS);
-            dst[0] = src[0];
-            dst[1] = src[1];
-            q.lF[e - kFarTile] = q.lF[e];
-          }
-          mine >>= kFarTile;
-          ql -= kFarTile;
-          __syncwarp();
+      }
+      if (nG) q.gF[qg][lane] = inW ? make_float2(fx, fy) : make_float2(0.f, 0.f);
+      if (COUNT) {
+        if (lane == 0) {
+          nGroup += nG;
+          nEvent++;
         }
+        if (inL) {
+          nLane++;
+          nWhy[!seenW ? 2 : (!closeW ? 1 : 0)]++;  // few members / spread / test
+        }
+      }
+      qg += nG;
+      ql += __popc(lball);
+      while (ql >= kFarTile) {
+        __syncwarp();
+        mlp_forward_tile(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
+        __syncwarp();
+        for (uint32_t m = (uint32_t)(mine & 0xffffu); m; m &= m - 1u) {
+          const int e = __ffs(m) - 1;
+          far_apply(q.out[e], q.lF[e], corrx, corry);
+        }
+        __syncwarp();
+        // move the rows past the tile (at most 31) to the front
+        for (int e = kFarTile + (int)lane; e < ql; e += 32) {
+          const uint4 *src = reinterpret_cast<const uint4 *>(q.lx + e * MLP_XS);
+          uint4 *dst = reinterpret_cast<uint4 *>(q.lx + (e - kFarTile) * MLP_XS);
+          dst[0] = src[0];
+          dst[1] = src[1];
+          q.lF[e - kFarTile] = q.lF[e];
+        }
+        mine >>= kFarTile;
+        ql -= kFarTile;
+        __syncwarp();
       }
     }
     if (active) resume = open ? cur + 1u : skip;
@@ -441,9 +487,13 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
   if (COUNT) {
     atomicAdd(a.counters, nInter);
     atomicAdd(a.counters + 3, nLane);
+    atomicAdd(a.counters + 4, nWhy[0]);
+    atomicAdd(a.counters + 5, nWhy[1]);
+    atomicAdd(a.counters + 6, nWhy[2]);
     if (lane == 0) {
       atomicAdd(a.counters + 1, nVisit);
       atomicAdd(a.counters + 2, nGroup);
+      atomicAdd(a.counters + 7, nEvent);
     }
   }
   if (!act) return;
@@ -580,6 +630,26 @@ static void launch_far(gvizCudaForce *h, const FarArgs &fa, bool count) {
   else k_walk_f32_far<MODEL, OVERLAP, false><<<grid, kFarThreads, 0, h->stream>>>(fa);
 }
 
+// The learned walk (see k_walk_f32_far).
+static void enqueue_far(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters) {
+  FarArgs fa;
+  fa.w = a;
+  fa.cells = h->d_cells;
+  fa.leafPre = h->d_leafPre;
+  fa.mlp = reinterpret_cast<const MlpDev *>(h->d_mlp);
+  fa.spread2 = (float)(h->params.farGroupSpread * h->params.farGroupSpread);
+  const bool ov = h->params.preventOverlap != 0;
+  const bool count = counters != nullptr;
+  if (h->model == GVIZ_CUDA_MODEL_FR) {
+    if (ov) launch_far<GVIZ_CUDA_MODEL_FR, true>(h, fa, count);
+    else launch_far<GVIZ_CUDA_MODEL_FR, false>(h, fa, count);
+  } else {
+    if (ov) launch_far<GVIZ_CUDA_MODEL_LINLOG, true>(h, fa, count);
+    else launch_far<GVIZ_CUDA_MODEL_LINLOG, false>(h, fa, count);
+  }
+  prof_mark(h, "bh_walk_f32_learned");
+}
+
 void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   WalkArgs a;
   a.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
@@ -601,20 +671,7 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   const bool ov = h->params.preventOverlap != 0;
   const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
   if (h->params.farField && h->d_mlp) {
-    FarArgs fa;
-    fa.w = a;
-    fa.cells = h->d_cells;
-    fa.leafPre = h->d_leafPre;
-    fa.mlp = reinterpret_cast<const MlpDev *>(h->d_mlp);
-    fa.spread2 = (float)(h->params.farGroupSpread * h->params.farGroupSpread);
-    if (fr) {
-      if (ov) launch_far<GVIZ_CUDA_MODEL_FR, true>(h, fa, counters != nullptr);
-      else launch_far<GVIZ_CUDA_MODEL_FR, false>(h, fa, counters != nullptr);
-    } else {
-      if (ov) launch_far<GVIZ_CUDA_MODEL_LINLOG, true>(h, fa, counters != nullptr);
-      else launch_far<GVIZ_CUDA_MODEL_LINLOG, false>(h, fa, counters != nullptr);
-    }
-    prof_mark(h, "bh_walk_f32_learned");
+    enqueue_far(h, a, counters);
     return;
   }
   if (counters) {

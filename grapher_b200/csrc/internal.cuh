@@ -24,6 +24,7 @@
 #define GVIZ_ST_DEEP_RUN 2u
 #define GVIZ_ST_DEPTH_CAP 4u
 #define GVIZ_ST_TREE 8u  // tree invariant broken (guarded, never expected)
+
 #define GVIZ_MAX_CLIMB 256  // binary radix tree depth <= 161 (key bits + 1)
 
 // Per-graph quadtree root: the reference's square root box
@@ -56,11 +57,13 @@ struct __align__(16) NodeD {
 };
 
 // Side record of a cell (same preorder index as its node record) for the
-// learned far-field correction and its training: the cell's second central
-// moments, the halfSize its opening test uses, the geometric centre relative
-// to the centre of mass, and its points' range in path-sorted order.
+// learned far-field correction and its training, in the form the features
+// use: the second central moments per unit mass (Qxx - Qyy, 2 Qxy,
+// Qxx + Qyy, all / M), the halfSize h its opening test uses, the geometric
+// centre relative to the centre of mass in units of h, and its points'
+// range in path-sorted order.
 struct __align__(16) FarCell {
-  float qxx, qxy, qyy;
+  float qa, qb, tr;
   float h;
   float ox, oy;
   uint32_t s0, s1;
@@ -243,7 +246,8 @@ size_t scan_scratch_entries(size_t n);
 void enqueue_tree_build(gvizCudaForce *h);
 void enqueue_tree_export(gvizCudaForce *h, int32_t *leafDepth);
 
-void mlp_free(gvizCudaForce *h);  // mlp.cu
+// mlp.cu
+void mlp_free(gvizCudaForce *h);
 int far_side_alloc(gvizCudaForce *h);
 void far_side_free(gvizCudaForce *h);
 int dir_table_upload_forces(const double *t);

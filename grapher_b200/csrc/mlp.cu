@@ -370,6 +370,7 @@ __global__ __launch_bounds__(128) void k_mlp_infer(const MlpDev *__restrict__ Wg
   }
 }
 
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -459,7 +460,7 @@ __global__ __launch_bounds__(128) void k_far_harvest(HarvestArgs a) {
       pair64(a, p.x, p.y, comx, comy, mv, (double)n.mass, rv, mx, my);
       const double fm = sqrt(mx * mx + my * my);
       float f[MLP_IN], e1x, e1y;
-      far_features(dx, dy, d2, c, n.mass, (float)rv, f, e1x, e1y);
+      far_features(dx, dy, d2, c, (float)rv, f, e1x, e1y);
       const uint32_t slot = atomicAdd(a.count, 1u);
       if (slot < a.cap && fm > 0.0) {
         for (int k = 0; k < MLP_IN; k++) a.feat[(size_t)slot * MLP_IN + k] = f[k];

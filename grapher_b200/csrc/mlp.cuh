@@ -80,37 +80,29 @@ __device__ __forceinline__ void mlp_stage(MlpSmem &S, const MlpDev *__restrict__
 // ---------------------------------------------------------------------------
 
 // (dx, dy) = c - v, d2 = |c - v|^2 (FP32), FarCell of the accepted cell,
-// cell mass M and point count, target radius rv (0 without overlap).
-// Writes the 10 features and the frame (e1 = -(c-v)/|c-v|).
+// target radius rv (0 without overlap). Writes the 10 features and the
+// frame (e1 = -(c-v)/|c-v|).
 __device__ __forceinline__ void far_features(float dx, float dy, float d2,
-                                             const FarCell &c, float M,
-                                             float rv, float *f, float &e1x,
-                                             float &e1y) {
+                                             const FarCell &c, float rv, float *f,
+                                             float &e1x, float &e1y) {
   const float inv = rsqrtf(d2);
-  const float d = d2 * inv;
+  const float inv2 = inv * inv;
   const float wx = dx * inv, wy = dy * inv;  // unit vector v -> c
   e1x = -wx;
   e1y = -wy;
   // quadrupole (Qxx - Qyy) + 2i Qxy rotated by conj(w)^2 into the pair frame
-  const float qa = c.qxx - c.qyy, qb = 2.0f * c.qxy;
   const float ca = wx * wx - wy * wy, cb = -2.0f * wx * wy;
-  const float qr = qa * ca - qb * cb;
-  const float qi = qa * cb + qb * ca;
-  const float nrm = 1.0f / fmaxf(M * d2, 1e-30f);
   const float s = c.h * inv;  // h / d
-  const float hinv = 1.0f / fmaxf(c.h, 1e-30f);
-  const float cnt = (float)(c.s1 - c.s0);
   f[0] = s;
-  f[1] = qr * nrm;
-  f[2] = qi * nrm;
-  f[3] = (c.qxx + c.qyy) * nrm;
+  f[1] = (c.qa * ca - c.qb * cb) * inv2;
+  f[2] = (c.qa * cb + c.qb * ca) * inv2;
+  f[3] = c.tr * inv2;
   f[4] = rv * inv;
-  f[5] = (c.ox * wx + c.oy * wy) * hinv;
-  f[6] = (-c.ox * wy + c.oy * wx) * hinv;
-  f[7] = __log2f(fmaxf(cnt, 1.0f)) * (1.0f / 16.0f);
+  f[5] = c.ox * wx + c.oy * wy;
+  f[6] = c.oy * wx - c.ox * wy;
+  f[7] = __log2f((float)max(c.s1 - c.s0, 1u)) * (1.0f / 16.0f);
   f[8] = s * s;
   f[9] = s * s * s;
-  (void)d;
 }
 
 // ---------------------------------------------------------------------------

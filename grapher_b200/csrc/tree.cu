@@ -627,13 +627,15 @@ __device__ void put_far(const EM &a, uint32_t at, const GraphRoot &R,
   }
   double gx, gy;
   cell_center(R, a.bHi[keyBucket], a.bLo[keyBucket], depth, gx, gy);
+  const double im = (M > 1e-30 || M < -1e-30) ? 1.0 / M : 0.0;
+  const double ih = h > 0.0 ? 1.0 / h : 0.0;
   FarCell c;
-  c.qxx = (float)q.x;
-  c.qxy = (float)q.y;
-  c.qyy = (float)q.z;
+  c.qa = (float)((q.x - q.z) * im);
+  c.qb = (float)(2.0 * q.y * im);
+  c.tr = (float)((q.x + q.z) * im);
   c.h = (float)h;
-  c.ox = (float)(gx - comx);
-  c.oy = (float)(gy - comy);
+  c.ox = (float)((gx - comx) * ih);
+  c.oy = (float)((gy - comy) * ih);
   c.s0 = s0;
   c.s1 = s1;
   a.cells[at] = c;

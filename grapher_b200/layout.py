@@ -287,12 +287,17 @@ class ForceLayout:
                 "gvizCudaForceCountInteractions")
         return a.value, b.value
 
-    def count_far_rows(self):
+    def count_far_rows(self, causes=False):
         """(shared rows, per-target rows) of MLP evaluations in one force
-        evaluation with the learned correction on."""
+        evaluation with the learned correction on; with causes=True also the
+        per-target rows by cause (too few targets, spread, centroid test)."""
         a, b = C.c_uint64(), C.c_uint64()
-        N.check(self.L.gvizCudaForceCountFarRows(self.h, C.byref(a), C.byref(b)),
+        why = np.zeros(3, np.uint64)
+        N.check(self.L.gvizCudaForceCountFarRows(self.h, C.byref(a), C.byref(b),
+                                                 N.ptr(why, C.c_uint64)),
                 "gvizCudaForceCountFarRows")
+        if causes:
+            return a.value, b.value, [int(x) for x in why]
         return a.value, b.value
 
     def profile_step(self):

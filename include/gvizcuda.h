@@ -208,9 +208,12 @@ int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
 
 /* With the learned correction on: the MLP rows one force evaluation runs,
  * shared rows (one per warp and cell, evaluated at the centroid of the
- * warp's accepting targets) and per-target rows. Zeros when it is off. */
+ * warp's accepting targets) and per-target rows, and (laneRowCause[3], may
+ * be NULL) why per-target rows were used: fewer than three targets accepted
+ * the cell, their spread was too wide, or the cell fails the opening test
+ * seen from their centroid. Zeros when the correction is off. */
 int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows,
-                              uint64_t *laneRows);
+                              uint64_t *laneRows, uint64_t *laneRowCause);
 
 /* Per-kernel device time of the last profiled step (CUDA events on the
  * handle's stream). names: up to cap C strings; ms: up to cap values. */
