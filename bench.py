@@ -1,12 +1,22 @@
 """Benchmark of the B200 force-layout step (libgvizcuda).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ba1m|batch4096|grid32|er65k_exact]
+                    [--workload ba1m_learned|ba1m|batch4096|grid32|er65k_exact]
 
-Default workload (the headline configuration): Barabasi-Albert graph,
-n = 1,048,576, m = 4 (4,194,294 edges, seeded), LinLog with gravity 1.0 and
-degree-sized prevent-overlap (r = 1.0 * (1 + 0.5 sqrt(deg))), Barnes-Hut
-theta = 0.8, start uniform in [-1000, 1000]^2 (rand_r, seed 7), FP32 walk.
+Default workload (the headline metric: learned vs plain Barnes-Hut at equal
+force error): Barabasi-Albert graph, n = 1,048,576, m = 4 (4,194,294 edges,
+seeded), LinLog with gravity 1.0, start uniform in [-1000, 1000]^2 (rand_r,
+seed 7). After the warm-up steps (plain, theta = 0.5) the far-field MLP is
+trained on the GPU from pairs harvested at theta = 1.2, 0.9 and 0.6 on three
+snapshots of this layout (untimed setup, reported as train_s). Force error is the
+normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
+65,536 sampled vertices, all configurations judged on the same positions.
+The plain walk runs at theta = 0.5; the learned walk at the largest theta of
+1.2, 1.1, ..., 0.6 whose error is not above the plain walk's. ``value`` is
+the learned path's iterations/s; the plain path's are in ``plain``. Both are
+timed from the same saved layout state.
+ba1m: the same graph with degree-sized prevent-overlap
+(r = 1.0 * (1 + 0.5 sqrt(deg))), plain theta = 0.8, FP32 walk.
 batch4096: 4096 independent graphs, sizes log-uniform in [32, 8192], each an
 Erdos-Renyi graph (mean degree U[3,6]), a random tree or a square grid,
 FR theta = 0.7, laid out together in one handle (one step = every graph steps).
@@ -38,8 +48,11 @@ sys.path.insert(0, ROOT)
 
 SEED = 7
 FLOP_PER_INTERACTION = 20  # pair or pseudo-body term (GPU Gems 3 ch. 31 convention)
+MLP_FLOP_PER_ROW = 2 * (10 * 64 + 64 * 64 + 64 * 2)  # one 10-64-64-2 evaluation
 
 SPECS = {
+    "ba1m_learned": dict(model=1, theta=0.5, gravity=1.0, radius_base=0.0,
+                         radius_per_degree=0.0, overlap=False, bh=True),
     "ba1m": dict(model=1, theta=0.8, gravity=1.0, radius_base=1.0, radius_per_degree=0.5,
                  overlap=True, bh=True),
     "batch4096": dict(model=0, theta=0.7, gravity=0.0, radius_base=0.0,
@@ -60,7 +73,7 @@ class Workload:
         self.name = name
         self.spec = SPECS[name]
         self.graphs = []  # (V, a, b, box, seed)
-        if name == "ba1m":
+        if name in ("ba1m", "ba1m_learned"):
             V = 1 << 20
             a, b = graphs.barabasi_albert(V, 4, SEED)
             self.graphs.append((V, a, b, 1000.0, SEED))
@@ -281,6 +294,72 @@ def run_reference_arm(args, w):
     return 0
 
 
+# ------------------------------------------------------------ learned setup
+LEARNED_THETAS = (1.2, 1.1, 1.0, 0.9, 0.8, 0.7, 0.6)
+LEARNED_SPREAD = 0.5
+JUDGE_VERTICES = 65536
+
+
+def force_error(lay, targets, exact):
+    """Normalised RMS error of the current repulsion on the sampled targets,
+    and the RMS of the per-vertex relative errors."""
+    rep = lay.repulsion()[targets]
+    d = np.linalg.norm(rep - exact, axis=1)
+    n = np.linalg.norm(exact, axis=1)
+    return (float(np.sqrt(np.sum(d * d) / np.sum(n * n))),
+            float(np.sqrt(np.mean((d / np.maximum(n, 1e-300)) ** 2))))
+
+
+def learned_setup(lay, w):
+    """Trains the far-field MLP on this layout's own harvested pairs, judges
+    plain theta = 0.5 and the learned walk against exact FP64 repulsion on
+    the same positions and picks the learned theta (see the module text)."""
+    from grapher_b200.farfield import FarFieldModel, harvest_training_set
+    rng = np.random.default_rng(SEED)
+    t0 = time.perf_counter()
+    Xs, Ts, Ws = [], [], []
+    for snap, th in enumerate((1.2, 0.9, 0.6)):  # cells of every angular size
+        if snap:
+            for _ in range(5):
+                lay.step()
+        t = np.sort(rng.choice(w.V, 16384, replace=False)).astype(np.uint32)
+        X, T, Wt = harvest_training_set(lay, th, t)
+        Xs.append(X), Ts.append(T), Ws.append(Wt)
+    model = FarFieldModel(seed=SEED)
+    losses = model.train(np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws),
+                         epochs=40, batch=4096, lr=2e-3, seed=SEED)
+    train_s = time.perf_counter() - t0
+    targets = np.sort(rng.choice(w.V, min(JUDGE_VERTICES, w.V), replace=False)).astype(np.uint32)
+    exact = lay.exact_repulsion(targets)
+    lay.set_params(theta=w.spec["theta"], farField=0)
+    e_plain, e_plain_pv = force_error(lay, targets, exact)
+    model.attach(lay)
+    table = {}
+    chosen = None
+    for th in LEARNED_THETAS:
+        lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD)
+        e, e_pv = force_error(lay, targets, exact)
+        table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
+        if chosen is None and e <= e_plain:
+            chosen = th
+    if chosen is None:
+        chosen = LEARNED_THETAS[-1]
+    lay.set_params(theta=w.spec["theta"], farField=0)
+    plain_table = {}
+    for th in (0.3, 0.4, 0.5, 0.6, 0.8, 1.0, 1.2):
+        lay.set_params(theta=th)
+        e, e_pv = force_error(lay, targets, exact)
+        plain_table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
+    lay.set_params(theta=w.spec["theta"])
+    info = {"train_s": train_s, "train_pairs": int(sum(len(x) for x in Xs)),
+            "train_loss_first_last": [float(losses[0]), float(losses[-1])],
+            "judge_vertices": int(len(targets)), "plain_rms_err": e_plain,
+            "plain_rms_rel_err_per_vertex": e_plain_pv, "learned_theta": chosen,
+            "learned_errors": table, "plain_errors": plain_table,
+            "group_spread": LEARNED_SPREAD}
+    return model, info
+
+
 # ---------------------------------------------------------------------- ours
 def main():
     ap = argparse.ArgumentParser()
@@ -288,11 +367,12 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ba1m", choices=sorted(SPECS))
+    ap.add_argument("--workload", default="ba1m_learned", choices=sorted(SPECS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     w = Workload(args.workload)
+    learned = args.workload == "ba1m_learned"
     if args.impl == "reference":
         return run_reference_arm(args, w)
 
@@ -327,6 +407,29 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    model, linfo, plain_line = None, None, None
+    if learned:
+        model, linfo = learned_setup(lay, w)
+        x_s, (sf_s, sp_s, ef_s) = lay.positions(), lay.fa2_state()
+        # plain theta = 0.5 from the saved state
+        lay.set_params(theta=w.spec["theta"], farField=0)
+        lay.time_steps(args.warmup)
+        lay.set_positions(x_s)
+        lay.set_fa2_state(sf_s, sp_s, ef_s)
+        barrier()
+        pms = max_over_ranks(lay.time_steps(args.steps))
+        pprof = lay.profile_step()
+        plain_line = {"theta": w.spec["theta"], "value": world * args.steps / (pms / 1e3),
+                      "ms_per_step": pms / args.steps, "rms_err": linfo["plain_rms_err"],
+                      "kernel_ms": {k: round(v, 4) for k, v in pprof}}
+        # then the learned walk from the same state
+        lay.set_positions(x_s)
+        lay.set_fa2_state(sf_s, sp_s, ef_s)
+        lay.set_params(theta=linfo["learned_theta"], farField=1, farGroupSpread=LEARNED_SPREAD)
+        lay.time_steps(args.warmup)
+        lay.set_positions(x_s)
+        lay.set_fa2_state(sf_s, sp_s, ef_s)
+
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
@@ -359,7 +462,7 @@ def main():
     inter, visits = lay.count_interactions()
     peaks, peak_src = load_peaks()
     pd = dict(prof)
-    kname = "bh_walk_f32" if w.spec["bh"] else "exact_f32"
+    kname = ("bh_walk_f32_learned" if learned else "bh_walk_f32") if w.spec["bh"] else "exact_f32"
     walk_ms = pd.get(kname)
     step_ms = sum(t for _, t in prof)
     flops = FLOP_PER_INTERACTION * inter
@@ -371,6 +474,22 @@ def main():
                                "MEASURED_PEAKS.json max SM clock (no measured FP32 figure)",
                 "algorithmic": f"{FLOP_PER_INTERACTION} FLOP x {inter} interactions per launch",
                 "share_of_step": walk_ms / step_ms, "warp_node_visits": visits}
+    if learned:
+        g_rows, l_rows = lay.count_far_rows()
+        rows = g_rows + l_rows
+        mlp_flop = MLP_FLOP_PER_ROW * rows
+        tc = mlp_flop / (walk_ms * 1e-3) / 1e12
+        roofline = {"kernel": kname, "bound": "tensor", "achieved": tc,
+                    "peak": peaks.get("bf16_tflops", 1590.0), "unit": "TFLOP/s",
+                    "frac": tc / peaks.get("bf16_tflops", 1590.0), "traffic": None,
+                    "peak_source": f"bf16_tflops ({peak_src})",
+                    "algorithmic": (f"{MLP_FLOP_PER_ROW} FLOP (10-64-64-2 MLP) x {rows} rows "
+                                    f"({g_rows} shared, {l_rows} per target) per launch"),
+                    "share_of_step": walk_ms / step_ms, "warp_node_visits": visits,
+                    "fp32_view": {"achieved": achieved, "peak": fp32_peak,
+                                  "frac": achieved / fp32_peak,
+                                  "algorithmic": f"{FLOP_PER_INTERACTION} FLOP x {inter} "
+                                                 "monopole/pair interactions per launch"}}
 
     line = {
         "metric": "layout iters/sec", "value": value, "unit": "iters/s", "n_gpus": world,
@@ -381,6 +500,13 @@ def main():
         "vertex_updates_per_s": value * V, "roofline": roofline,
         "kernel_ms": {k: round(v, 4) for k, v in prof}, "peaks": peak_src,
     }
+    if learned:
+        line["metric"] = ("layout iters/sec, 1M-vertex BA graph: learned vs plain BH at "
+                          "equal force error")
+        line["learned"] = dict(linfo, value=value, theta=linfo["learned_theta"],
+                               rms_err=linfo["learned_errors"][str(linfo["learned_theta"])]["rms_err"])
+        line["plain"] = plain_line
+        line["config"]["theta"] = {"plain": w.spec["theta"], "learned": linfo["learned_theta"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

@@ -231,8 +231,8 @@ __global__ __launch_bounds__(kWalkThreads) void k_walk_f32(WalkArgs a) {
 // The learned walk: as k_walk_f32, with two changes that define the learned
 // method (it has no reference counterpart): a cell containing the target is
 // never accepted, and every accepted cell's monopole force F gets the MLP's
-// correction p1 F + p2 rot90(F) (p is the relative correction in the frame
-// of F). The MLP runs on the tensor cores over 16-row tiles queued per warp
+// correction p1 F + p2 rot90(F) (p = s^2 MLP(features), s = h/d, is the
+// relative correction in the frame of F). The MLP runs on the tensor cores over 16-row tiles queued per warp
 // in shared memory. The accepting lanes of a cell share a row where their
 // targets are close together compared with their distance to it:
 //   shared row - lanes within farGroupSpread * |c - g| of the warp's target
@@ -407,7 +407,7 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
       const int nG = wball ? 1 : 0;
       if (nG > 0 && qg == kFarTile) {
         __syncwarp();
-        mlp_forward_tile(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
+        mlp_forward_tile<true>(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
         __syncwarp();
 #pragma unroll 4
         for (int r = 0; r < kFarTile; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
@@ -444,7 +444,7 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
       ql += __popc(lball);
       while (ql >= kFarTile) {
         __syncwarp();
-        mlp_forward_tile(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
+        mlp_forward_tile<true>(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
         __syncwarp();
         for (uint32_t m = (uint32_t)(mine & 0xffffu); m; m &= m - 1u) {
           const int e = __ffs(m) - 1;
@@ -471,13 +471,13 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
   }
   if (qg > 0) {
     __syncwarp();
-    mlp_forward_tile(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
+    mlp_forward_tile<true>(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
     __syncwarp();
     for (int r = 0; r < qg; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
   }
   if (ql > 0) {
     __syncwarp();
-    mlp_forward_tile(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
+    mlp_forward_tile<true>(W, q.lx, MLP_XS, reinterpret_cast<float *>(q.out));
     __syncwarp();
     for (uint32_t m = (uint32_t)(mine & 0xffffu); m; m &= m - 1u) {
       const int e = __ffs(m) - 1;

@@ -361,8 +361,8 @@ __global__ __launch_bounds__(128) void k_mlp_infer(const MlpDev *__restrict__ Wg
   for (int f = 0; f < MLP_INP; f++)
     xs[w][l * MLP_XS + f] = __float2bfloat16_rn(row < n && f < MLP_IN ? X[(size_t)row * MLP_IN + f] : 0.f);
   __syncwarp();
-  mlp_forward_tile(W, xs[w], MLP_XS, ys[w]);
-  mlp_forward_tile(W, xs[w] + 16 * MLP_XS, MLP_XS, ys[w] + 32);
+  mlp_forward_tile<false>(W, xs[w], MLP_XS, ys[w]);
+  mlp_forward_tile<false>(W, xs[w] + 16 * MLP_XS, MLP_XS, ys[w] + 32);
   __syncwarp();
   if (row < n) {
     Y[(size_t)row * 2] = ys[w][l * 2];

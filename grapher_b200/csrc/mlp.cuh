@@ -7,10 +7,10 @@
 // the leading correction is the cell's quadrupole over |c - v|^2, then
 // higher multipoles. The MLP predicts the relative correction in the local
 // frame of the pair (e1 = direction of the monopole force, e2 = e1 rotated
-// by +90 degrees):
-//     F = F_mono + |F_mono| (p1 e1 + p2 e2)
+// by +90 degrees) in units of its leading order s^2 = (h/d)^2:
+//     F = F_mono + |F_mono| s^2 (m1 e1 + m2 e2),   m = MLP(features)
 // from rotation-invariant features (the quadrupole is rotated into the same
-// frame), so one small network serves every direction.
+// frame), so one small network serves every direction and every distance.
 #pragma once
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -205,6 +205,10 @@ __device__ __forceinline__ void load_b2_nk(uint32_t *b, const __nv_bfloat16 *m,
 // memory, row stride ldx) -> out[16][2] FP32 in shared memory. W holds the
 // weights staged by mlp_stage. Hidden layers stay in registers: the
 // accumulator layout of two adjacent n-tiles is the A layout of one k-tile.
+// With SCALE_S2 the outputs are multiplied by the row's feature 8, s^2: the
+// network predicts the relative correction in units of (h/d)^2, its leading
+// order, so the correction vanishes with the cell's angular size.
+template <bool SCALE_S2>
 __device__ __forceinline__ void mlp_forward_tile(const MlpSmem &W,
                                                  const __nv_bfloat16 *X, int ldx,
                                                  float *out) {
@@ -254,9 +258,11 @@ __device__ __forceinline__ void mlp_forward_tile(const MlpSmem &W,
   }
   // outputs 0 and 1 sit in threads with t == 0: rows g and g + 8
   if (t == 0) {
-    out[g * 2 + 0] = y[0] + W.b3[0];
-    out[g * 2 + 1] = y[1] + W.b3[1];
-    out[(g + 8) * 2 + 0] = y[2] + W.b3[0];
-    out[(g + 8) * 2 + 1] = y[3] + W.b3[1];
+    const float s0 = SCALE_S2 ? __bfloat162float(X[g * ldx + 8]) : 1.f;
+    const float s1 = SCALE_S2 ? __bfloat162float(X[(g + 8) * ldx + 8]) : 1.f;
+    out[g * 2 + 0] = (y[0] + W.b3[0]) * s0;
+    out[g * 2 + 1] = (y[1] + W.b3[1]) * s0;
+    out[(g + 8) * 2 + 0] = (y[2] + W.b3[0]) * s1;
+    out[(g + 8) * 2 + 1] = (y[3] + W.b3[1]) * s1;
   }
 }

@@ -9,8 +9,10 @@
 
 Training pairs are harvested from the layout's own tree (gvizCudaForce-
 HarvestFarField): exact FP64 force of every accepted cell's points against
-its monopole. Sample weights (|F_mono| / |F_v|)^2 make the loss the sum of
-squared per-cell contributions to each target's relative force error.
+its monopole. The network predicts that relative correction in units of
+s^2 = (h/d)^2, its leading order, and the walk multiplies its output by s^2.
+Sample weights (|F_mono| / |F_v|)^2 s^4 make the loss the sum of squared
+per-cell contributions to each target's relative force error.
 """
 from __future__ import annotations
 
@@ -109,14 +111,19 @@ def harvest(layout, targets, theta, cap=None):
 
 
 def harvest_training_set(layout, theta, targets):
-    """Features, targets and per-sample weights (|F_mono| / |F_v|)^2 with
-    F_v the exact FP64 repulsion of the sample's target vertex."""
+    """Training set for the network of the learned walk, which predicts the
+    relative correction in units of s^2 = (h/d)^2 (feature 8) and has its
+    output multiplied by s^2 in the walk: features, targets T / s^2 and
+    weights W s^4 with W = (|F_mono| / |F_v|)^2 and F_v the exact FP64
+    repulsion of the sample's target vertex, so that the loss is the sum of
+    squared per-cell contributions to each target's relative force error."""
     X, T, M, V = harvest(layout, targets, theta)
     exact = layout.exact_repulsion(targets)
     fv = dict(zip(np.asarray(targets, np.uint32).tolist(), np.linalg.norm(exact, axis=1)))
     den = np.array([fv[int(v)] for v in V])
     W = (M / np.maximum(den, 1e-30)) ** 2
-    return X, T, W.astype(np.float32)
+    s2 = np.maximum(X[:, 8].astype(np.float64), 1e-12)
+    return X, (T / s2[:, None]).astype(np.float32), (W * s2 * s2).astype(np.float32)
 
 
 def force_error(layout, targets, exact=None):
