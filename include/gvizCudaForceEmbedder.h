@@ -63,6 +63,21 @@ void gvizCudaForceDetach(gvizForceEmbedderState *state);
  * handler cannot return one. */
 int gvizCudaForceEmbedderLastError(const gvizForceEmbedderState *state);
 
+/* gvizForceEmbedderRun (src/embedders/gvizForceEmbedder.c:497-510) for n
+ * independent begun embedders at once, all laid out by one GPU handle (one
+ * quadtree per graph in one forest, per-graph FA2 speed, per-graph
+ * convergence), then written back to each state like n separate Runs:
+ * positions, iteration, lastMaxDisplacement, globalSpeed, speedEfficiency,
+ * the five stat series (each graph's latest 4096 rows) and, with
+ * options->syncScratch, the per-vertex arrays. The embedders need not be
+ * attached. They must share the force model and configuration (theta,
+ * edgeLength, ...); otherwise GVIZ_CUDA_ERR_ARG. rounds[n] (may be NULL)
+ * receives each graph's round count. Returns 0, -1 if one has not begun, or
+ * a negative GVIZ_CUDA_ERR_* code. */
+int gvizCudaForceEmbedderRunBatch(gvizForceEmbedderState **states, size_t n,
+                                  size_t maxIters, double epsilon,
+                                  const gvizCudaOptions *options, uint64_t *rounds);
+
 #ifdef __cplusplus
 }
 #endif
