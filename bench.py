@@ -294,6 +294,22 @@ def run_reference_arm(args, w):
     return 0
 
 
+class nvtx_range:
+    """NVTX range around a timed region, so that a profiler can be limited
+    to it (ncu --nvtx --nvtx-include <name>/)."""
+
+    def __init__(self, name):
+        self.name = name
+
+    def __enter__(self):
+        import torch
+        torch.cuda.nvtx.range_push(self.name)
+
+    def __exit__(self, *exc):
+        import torch
+        torch.cuda.nvtx.range_pop()
+
+
 # ------------------------------------------------------------ learned setup
 LEARNED_THETAS = (1.2, 1.1, 1.0, 0.9, 0.8, 0.7, 0.6)
 LEARNED_SPREAD = 0.5
@@ -417,7 +433,8 @@ def main():
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
         barrier()
-        pms = max_over_ranks(lay.time_steps(args.steps))
+        with nvtx_range("plain_steps"):
+            pms = max_over_ranks(lay.time_steps(args.steps))
         pprof = lay.profile_step()
         plain_line = {"theta": w.spec["theta"], "value": world * args.steps / (pms / 1e3),
                       "ms_per_step": pms / args.steps, "rms_err": linfo["plain_rms_err"],
@@ -433,7 +450,8 @@ def main():
     sampler = ClockSampler(local)
     sampler.start()
     barrier()
-    ms = lay.time_steps(args.steps)
+    with nvtx_range("learned_steps" if learned else "timed_steps"):
+        ms = lay.time_steps(args.steps)
     barrier()
     clocks = sampler.stop()
     ms = max_over_ranks(ms)
