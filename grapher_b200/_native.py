@@ -67,6 +67,17 @@ class GraphDesc(C.Structure):
     ]
 
 
+class Csr(C.Structure):
+    _fields_ = [
+        ("vertexCount", C.c_size_t),
+        ("entryCount", C.c_size_t),
+        ("rowOffsets", C.POINTER(C.c_uint64)),
+        ("neighbors", C.POINTER(C.c_uint32)),
+        ("externalIds", C.POINTER(C.c_int64)),
+        ("directed", C.c_int32),
+    ]
+
+
 class StepStats(C.Structure):
     _fields_ = [
         ("maxDisp", C.c_double),
@@ -140,6 +151,9 @@ _SIGS = {
     "gvizCudaGenErdosRenyi": (SZ, [SZ, SZ, C.c_uint64, U32P, U32P]),
     "gvizCudaGenRmat": (SZ, [C.c_uint32, SZ, D, D, D, C.c_uint64, U32P, U32P]),
     "gvizCudaEdgesToCsr": (C.c_int, [SZ, U32P, U32P, SZ, U64P, U32P]),
+    "gvizCudaLoadEdgesFile": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(Csr)]),
+    "gvizCudaLoadObjFile": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "gvizCudaCsrFree": (None, [C.POINTER(Csr)]),
     "gvizCudaRandomizePositions": (None, [DP, SZ, D, C.c_uint]),
 }
 

@@ -35,6 +35,7 @@ SOURCES = {
     "mlp.cu": [],
     "api.cu": [],
     "host_graphs.cpp": [],
+    "loaders.cpp": [],
 }
 
 

@@ -82,3 +82,37 @@ def batch(graphs):
     b = np.concatenate(bb) if bb else np.zeros(0, np.uint32)
     row, col = to_csr(offs[-1], a, b)
     return row, col, np.asarray(offs, np.uint64)
+
+
+def _take_csr(rc, csr, what):
+    """Copies a library-owned gvizCudaCsr into numpy arrays and frees it."""
+    L = N.lib()
+    if rc != 0:
+        raise OSError(f"{what}: gviz loader rules rejected the file or it could not be read")
+    try:
+        V, nnz = int(csr.vertexCount), int(csr.entryCount)
+        row = np.ctypeslib.as_array(csr.rowOffsets, shape=(V + 1,)).copy()
+        col = (np.ctypeslib.as_array(csr.neighbors, shape=(nnz,)).copy() if nnz
+               else np.zeros(0, np.uint32))
+        ext = (np.ctypeslib.as_array(csr.externalIds, shape=(V,)).copy()
+               if bool(csr.externalIds) else None)
+    finally:
+        L.gvizCudaCsrFree(C.byref(csr))
+    return row, col, ext
+
+
+def load_edges_file(path, directed=False, skip_header=False):
+    """gvizGraphLoadFromEdgesFile straight to CSR: (row_offsets, neighbors,
+    external_ids) with gviz's vertex numbering and neighbour order."""
+    csr = N.Csr()
+    rc = N.lib().gvizCudaLoadEdgesFile(str(path).encode(), int(directed), int(skip_header),
+                                        C.byref(csr))
+    return _take_csr(rc, csr, f"load_edges_file({path})")
+
+
+def load_obj_file(path):
+    """gvizGraphLoadFromObjFile straight to CSR: (row_offsets, neighbors)."""
+    csr = N.Csr()
+    rc = N.lib().gvizCudaLoadObjFile(str(path).encode(), C.byref(csr))
+    row, col, _ = _take_csr(rc, csr, f"load_obj_file({path})")
+    return row, col

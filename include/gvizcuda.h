@@ -309,6 +309,39 @@ int gvizCudaFa2SpeedUpdateNoAlloc(const double *d_structForce,
                                   double jitterTolerance, double *d_swing,
                                   double *d_speedState, void *stream);
 
+/* ---- graph files straight to CSR ------------------------------------- */
+
+/* A graph loaded from a file, in the layout's CSR form (library-owned
+ * arrays; release with gvizCudaCsrFree). Vertex numbering and neighbour
+ * order are those of gviz's loader followed by its subgraph neighbour
+ * iterator, so the same file gives the same graph here and in gviz. */
+typedef struct gvizCudaCsr {
+  size_t vertexCount;
+  size_t entryCount;     /* rowOffsets[vertexCount] */
+  uint64_t *rowOffsets;  /* vertexCount + 1 */
+  uint32_t *neighbors;   /* entryCount */
+  int64_t *externalIds;  /* .edges files: each vertex's id in the file */
+  int32_t directed;      /* 1: rows hold out-neighbours only */
+} gvizCudaCsr;
+
+/* gvizGraphLoadFromEdgesFile (include/utils/graphLoader.h:33-35, Network
+ * Repository .edges: "u v [weight]" per line, '%' comments, ids of any
+ * base compacted in order of first appearance; skipHeader drops the first
+ * data line) without the adjacency-list graph. Unlike gviz's loader, whose
+ * id map spans max_id - min_id + 1 entries, sparse huge ids cost nothing
+ * extra. Returns 0, or -1 on I/O, parse or allocation failure (out
+ * zeroed), or when the graph needs indices beyond 32 bits. */
+int gvizCudaLoadEdgesFile(const char *path, int directed, int skipHeader,
+                          gvizCudaCsr *out);
+
+/* gvizGraphLoadFromObjFile (include/utils/graphLoader.h:76-89): one vertex
+ * per "v" line, edges along each "f" loop (consecutive corners and the
+ * closing edge, 1-based or negative relative indices, texture/normal parts
+ * ignored, no repeats, no self-loops). Returns 0 or -1 like gviz. */
+int gvizCudaLoadObjFile(const char *path, gvizCudaCsr *out);
+
+void gvizCudaCsrFree(gvizCudaCsr *csr);
+
 /* ---- host helpers: workloads and initial placement ------------------- */
 
 /* Ordered undirected edge lists. Each returns the edge count; pass NULL

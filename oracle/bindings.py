@@ -243,6 +243,28 @@ class Reference:
                                       C.c_size_t(ea.shape[0]), C.c_int(model))
         return RefLayout(self, h)
 
+    # ---- the reference's graph loaders, exported as CSR ----
+    def _load_csr(self, fn, *args):
+        fn.restype = C.c_longlong
+        n = C.c_size_t()
+        V = fn(*args, None, None, C.byref(n))
+        if V < 0:
+            return None
+        row = np.zeros(V + 1, np.uint64)
+        col = np.zeros(max(1, n.value), np.uint32)
+        fn(*args, _ptr(row, C.c_uint64), _ptr(col, U32), C.byref(n))
+        return row, col[:n.value]
+
+    def load_edges_csr(self, path, directed=False, skip_header=False):
+        """gvizGraphLoadFromEdgesFile, then the graph's adjacency as CSR;
+        None when the loader fails."""
+        return self._load_csr(self.lib.ref_load_edges_csr, str(path).encode(),
+                              C.c_int(int(directed)), C.c_int(int(skip_header)))
+
+    def load_obj_csr(self, path):
+        """gvizGraphLoadFromObjFile, then the adjacency as CSR (or None)."""
+        return self._load_csr(self.lib.ref_load_obj_csr, str(path).encode())
+
     def create_builtin(self, kind, a, b=0, density=0.0, seed=0, model=MODEL_FR):
         h = self.lib.ref_create_builtin(C.c_int(kind), C.c_size_t(a), C.c_size_t(b),
                                         D(density), C.c_uint(seed), C.c_int(model))

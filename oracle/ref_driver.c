@@ -14,6 +14,7 @@
 #include "ds/gvizSubgraph.h"
 #include "embedders/gvizEmbeddedGraph.h"
 #include "embedders/gvizForceEmbedder.h"
+#include "utils/graphLoader.h"
 #include "utils/graphs.h"
 
 #include <stdlib.h>
@@ -397,3 +398,49 @@ void ref_time_steps(refLayout *r, int steps, double *secondsOut) {
 
 /* Worker count gvizThreadPoolCreate(0) uses (src/core/gvizThreadPool.c:75-78). */
 long ref_pool_threads(void) { return sysconf(_SC_NPROCESSORS_ONLN); }
+
+/* The reference's own loaders (src/utils/graphLoader.c), exported as CSR
+ * from the loaded graph's adjacency lists (neighbour order as the subgraph
+ * neighbour iterator yields it). Returns the vertex count and *entries, or
+ * -1 when the loader fails. With row == NULL only the sizes are returned. */
+static long long csr_of_graph(gvizGraph *g, uint64_t *row, uint32_t *col, size_t *entries) {
+  const size_t V = gvizGraphSize(g);
+  size_t off = 0;
+  for (size_t i = 0; i < V; i++) {
+    gvizArray *nb = gvizGraphGetVertexNeighbors(g, i);
+    if (row)
+      row[i] = off;
+    for (size_t k = 0; k < nb->count; k++) {
+      if (col)
+        col[off] = (uint32_t)*(size_t *)gvizArrayAtIndex(nb, k);
+      off++;
+    }
+  }
+  if (row)
+    row[V] = off;
+  *entries = off;
+  return (long long)V;
+}
+
+long long ref_load_edges_csr(const char *path, int directed, int skipHeader,
+                             uint64_t *row, uint32_t *col, size_t *entries) {
+  gvizEdgesFileOptions o;
+  gvizEdgesFileOptionsInit(&o);
+  o.directed = directed;
+  o.skip_header = skipHeader;
+  gvizGraph g;
+  if (gvizGraphLoadFromEdgesFile(path, &o, &g) < 0)
+    return -1;
+  long long V = csr_of_graph(&g, row, col, entries);
+  gvizGraphRelease(&g);
+  return V;
+}
+
+long long ref_load_obj_csr(const char *path, uint64_t *row, uint32_t *col, size_t *entries) {
+  gvizGraph g;
+  if (gvizGraphLoadFromObjFile(path, &g) < 0)
+    return -1;
+  long long V = csr_of_graph(&g, row, col, entries);
+  gvizGraphRelease(&g);
+  return V;
+}
