@@ -151,6 +151,9 @@ _SIGS = {
     "gvizCudaGenErdosRenyi": (SZ, [SZ, SZ, C.c_uint64, U32P, U32P]),
     "gvizCudaGenRmat": (SZ, [C.c_uint32, SZ, D, D, D, C.c_uint64, U32P, U32P]),
     "gvizCudaEdgesToCsr": (C.c_int, [SZ, U32P, U32P, SZ, U64P, U32P]),
+    "gvizCudaForceSaveCheckpoint": (C.c_int, [P, C.c_char_p, C.c_char_p]),
+    "gvizCudaForceLoadCheckpoint": (C.c_int, [P, C.c_char_p, C.c_int, C.c_char_p, SZ]),
+    "gvizCudaForceSaveEmbeddingText": (C.c_int, [P, C.c_char_p, C.c_char_p]),
     "gvizCudaLoadEdgesFile": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(Csr)]),
     "gvizCudaLoadObjFile": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
     "gvizCudaCsrFree": (None, [C.POINTER(Csr)]),

@@ -14,6 +14,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
+#include <string>
 #include <vector>
 
 #include "epilogue.cuh"
@@ -1108,6 +1110,222 @@ int gvizCudaForceSetStream(gvizCudaForce *h, void *stream) {
   h->ownStream = false;
   h->graphDirty = true;
   return GVIZ_CUDA_OK;
+}
+
+
+// ---- lossless checkpoint ---------------------------------------------------
+//
+// gviz saves an embedding as text with six decimals and no FA2 speed state
+// (src/embedders/gvizEmbeddedGraph.c:428-448), so a run cannot be resumed
+// exactly. The binary checkpoint below holds everything a step reads from
+// the previous one: positions, structForce (the next step's old force),
+// global speed and efficiency, per-graph iteration counters and the stat
+// history ring, all as raw little-endian bytes, closed by an FNV-1a 64
+// checksum of everything before it. Layout (version 1):
+//   "GVZCKPT1" | u32 version | u32 name bytes | u64 V | u64 G | i32 model |
+//   i32 dim (2) | u32 params bytes | u32 begun | name | params |
+//   u64 graphOffsets[G+1] | f64 positions[2V] | f64 structForce[2V] |
+//   f64 speed[G] | f64 efficiency[G] | u64 iteration[G] | u64 host iteration |
+//   u64 ring rows R | f64 stats[R][G][5] | f64 lastStats[G][5] | u64 checksum
+
+namespace {
+
+constexpr char kCkptMagic[8] = {'G', 'V', 'Z', 'C', 'K', 'P', 'T', '1'};
+constexpr uint32_t kCkptVersion = 1;
+
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, nameBytes;
+  uint64_t V, G;
+  int32_t model, dim;
+  uint32_t paramsBytes, begun;
+};
+
+struct Fnv {
+  uint64_t h = 1469598103934665603ull;
+  void add(const void *p, size_t n) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < n; i++) {
+      h ^= b[i];
+      h *= 1099511628211ull;
+    }
+  }
+};
+
+struct CkptWriter {
+  FILE *f;
+  Fnv sum;
+  bool ok = true;
+  void put(const void *p, size_t n) {
+    if (!ok || n == 0) return;
+    sum.add(p, n);
+    ok = fwrite(p, 1, n, f) == n;
+  }
+};
+
+struct CkptReader {
+  FILE *f;
+  Fnv sum;
+  bool ok = true;
+  void get(void *p, size_t n) {
+    if (!ok || n == 0) return;
+    ok = fread(p, 1, n, f) == n;
+    if (ok) sum.add(p, n);
+  }
+};
+
+}  // namespace
+
+int gvizCudaForceSaveCheckpoint(gvizCudaForce *h, const char *name, const char *filename) {
+  if (!h || !filename) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  const size_t V = h->V, G = h->G;
+  std::vector<double> pos(2 * V), sf(2 * V), speed(G), eff(G), last(5 * G);
+  std::vector<uint64_t> iter(G);
+  bool ok = true;
+  if (V) {
+    ok = cudaMemcpy(pos.data(), h->d_pos, V * 16, cudaMemcpyDeviceToHost) == cudaSuccess;
+    ok = ok && cudaMemcpy(sf.data(), h->d_sf, V * 16, cudaMemcpyDeviceToHost) == cudaSuccess;
+  }
+  ok = ok && cudaMemcpy(speed.data(), h->d_speed, G * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(eff.data(), h->d_eff, G * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(iter.data(), h->d_iter, G * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+  ok = ok && cudaMemcpy(last.data(), h->d_lastStats, G * 40, cudaMemcpyDeviceToHost) == cudaSuccess;
+  uint64_t maxIt = 0;
+  for (uint64_t it : iter) maxIt = std::max(maxIt, it);
+  const uint64_t rows = std::min<uint64_t>(maxIt, GVIZ_STATS_CAP);
+  std::vector<double> ring(rows * G * 5);
+  if (rows)
+    ok = ok && cudaMemcpy(ring.data(), h->d_stats, ring.size() * 8, cudaMemcpyDeviceToHost) ==
+                   cudaSuccess;
+  if (!ok) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  FILE *f = fopen(filename, "wb");
+  if (!f) return set_err(h, GVIZ_CUDA_ERR_ARG);
+  CkptWriter w{f};
+  CkptHeader hd;
+  memcpy(hd.magic, kCkptMagic, 8);
+  hd.version = kCkptVersion;
+  hd.nameBytes = name ? (uint32_t)strlen(name) : 0u;
+  hd.V = V;
+  hd.G = G;
+  hd.model = h->model;
+  hd.dim = 2;
+  hd.paramsBytes = sizeof(gvizCudaForceParams);
+  hd.begun = h->begun ? 1u : 0u;
+  w.put(&hd, sizeof(hd));
+  w.put(name, hd.nameBytes);
+  w.put(&h->params, sizeof(gvizCudaForceParams));
+  w.put(h->h_graphOff, (G + 1) * 8);
+  w.put(pos.data(), pos.size() * 8);
+  w.put(sf.data(), sf.size() * 8);
+  w.put(speed.data(), G * 8);
+  w.put(eff.data(), G * 8);
+  w.put(iter.data(), G * 8);
+  w.put(&h->hostIteration, 8);
+  w.put(&rows, 8);
+  w.put(ring.data(), ring.size() * 8);
+  w.put(last.data(), last.size() * 8);
+  const uint64_t sum = w.sum.h;
+  ok = w.ok && fwrite(&sum, 8, 1, f) == 1;
+  ok = (fclose(f) == 0) && ok;
+  return ok ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_ARG);
+}
+
+int gvizCudaForceLoadCheckpoint(gvizCudaForce *h, const char *filename, int restoreParams,
+                                char *nameOut, size_t nameCap) {
+  if (!h || !filename) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  FILE *f = fopen(filename, "rb");
+  if (!f) return set_err(h, GVIZ_CUDA_ERR_ARG);
+  CkptReader r{f};
+  CkptHeader hd;
+  r.get(&hd, sizeof(hd));
+  // the file must be a version-1 checkpoint of this very graph (or forest)
+  bool ok = r.ok && memcmp(hd.magic, kCkptMagic, 8) == 0 && hd.version == kCkptVersion &&
+            hd.V == h->V && hd.G == h->G && hd.model == h->model && hd.dim == 2 &&
+            hd.paramsBytes == sizeof(gvizCudaForceParams) && hd.nameBytes < (1u << 20);
+  const size_t V = h->V, G = h->G;
+  std::string name(ok ? hd.nameBytes : 0, '\0');
+  gvizCudaForceParams params;
+  std::vector<uint64_t> goff(G + 1), iter(G);
+  std::vector<double> pos(2 * V), sf(2 * V), speed(G), eff(G), last(5 * G);
+  uint64_t hostIt = 0, rows = 0;
+  if (ok) {
+    r.get(&name[0], hd.nameBytes);
+    r.get(&params, sizeof(params));
+    r.get(goff.data(), (G + 1) * 8);
+    ok = r.ok && memcmp(goff.data(), h->h_graphOff, (G + 1) * 8) == 0;
+  }
+  if (ok) {
+    r.get(pos.data(), pos.size() * 8);
+    r.get(sf.data(), sf.size() * 8);
+    r.get(speed.data(), G * 8);
+    r.get(eff.data(), G * 8);
+    r.get(iter.data(), G * 8);
+    r.get(&hostIt, 8);
+    r.get(&rows, 8);
+    ok = r.ok && rows <= GVIZ_STATS_CAP;
+  }
+  std::vector<double> ring(ok ? rows * G * 5 : 0);
+  uint64_t stored = 0;
+  if (ok) {
+    r.get(ring.data(), ring.size() * 8);
+    r.get(last.data(), last.size() * 8);
+    const uint64_t sum = r.sum.h;
+    ok = r.ok && fread(&stored, 8, 1, f) == 1 && stored == sum && fgetc(f) == EOF;
+  }
+  fclose(f);
+  if (!ok) return set_err(h, GVIZ_CUDA_ERR_ARG);  // not this graph's, or damaged
+  for (size_t i = 0; i < 2 * V; i++)
+    if (!std::isfinite(pos[i])) return set_err(h, GVIZ_CUDA_ERR_NONFINITE);
+  if (restoreParams) {
+    const int rc = gvizCudaForceSetParams(h, &params);
+    if (rc) return rc;
+  }
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  bool cok = true;
+  if (V) {
+    cok = cudaMemcpy(h->d_pos, pos.data(), V * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+    cok = cok && cudaMemcpy(h->d_sf, sf.data(), V * 16, cudaMemcpyHostToDevice) == cudaSuccess;
+    cok = cok && cudaMemset(h->d_disp, 0, V * 16) == cudaSuccess;
+  }
+  cok = cok && cudaMemcpy(h->d_speed, speed.data(), G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  cok = cok && cudaMemcpy(h->d_eff, eff.data(), G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  cok = cok && cudaMemcpy(h->d_iter, iter.data(), G * 8, cudaMemcpyHostToDevice) == cudaSuccess;
+  cok = cok && cudaMemcpy(h->d_lastStats, last.data(), G * 40, cudaMemcpyHostToDevice) == cudaSuccess;
+  if (rows)
+    cok = cok && cudaMemcpy(h->d_stats, ring.data(), ring.size() * 8, cudaMemcpyHostToDevice) ==
+                     cudaSuccess;
+  if (!cok) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  set_all_active(h, ~0ull, -INFINITY);
+  h->begun = hd.begun != 0;
+  h->hostIteration = hostIt;
+  if (nameOut && nameCap) {
+    const size_t n = std::min(nameCap - 1, name.size());
+    memcpy(nameOut, name.data(), n);
+    nameOut[n] = '\0';
+  }
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceSaveEmbeddingText(gvizCudaForce *h, const char *name, const char *filename) {
+  if (!h || !filename) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  std::vector<double> pos(2 * h->V);
+  if (h->V && cudaMemcpy(pos.data(), h->d_pos, h->V * 16, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  FILE *f = fopen(filename, "w");
+  if (!f) return set_err(h, GVIZ_CUDA_ERR_ARG);
+  // gviz's layout (src/embedders/gvizEmbeddedGraph.c:428-448): name line,
+  // "count dim", one row per vertex; 17 significant digits instead of %f,
+  // so gvizEmbeddedGraphLoadEmbedding's %lf reads every bit back
+  bool ok = fprintf(f, "%s\n%zu %d\n", name ? name : "", h->V, 2) > 0;
+  for (size_t i = 0; ok && i < h->V; i++)
+    ok = fprintf(f, "%.17g %.17g \n", pos[2 * i], pos[2 * i + 1]) > 0;
+  ok = (fclose(f) == 0) && ok;
+  return ok ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_ARG);
 }
 
 }  // extern "C"

@@ -287,6 +287,29 @@ class ForceLayout:
                 "gvizCudaForceCountInteractions")
         return a.value, b.value
 
+    # ------------------------------------------------------------ checkpoints
+    def save_checkpoint(self, filename, name=""):
+        """Lossless checkpoint (positions, FA2 history, counters, stats)."""
+        N.check(self.L.gvizCudaForceSaveCheckpoint(self.h, name.encode(), str(filename).encode()),
+                "gvizCudaForceSaveCheckpoint")
+
+    def load_checkpoint(self, filename, restore_params=False):
+        """Restores a checkpoint of this graph; returns the saved name."""
+        buf = C.create_string_buffer(256)
+        N.check(self.L.gvizCudaForceLoadCheckpoint(self.h, str(filename).encode(),
+                                                   int(restore_params), buf, 256),
+                "gvizCudaForceLoadCheckpoint")
+        if restore_params:
+            self.L.gvizCudaForceGetParams(self.h, C.byref(self.params))
+        self.begun = True
+        return buf.value.decode()
+
+    def save_embedding_text(self, filename, name=""):
+        """Positions in gviz's text format, every bit kept (17 digits)."""
+        N.check(self.L.gvizCudaForceSaveEmbeddingText(self.h, name.encode(),
+                                                      str(filename).encode()),
+                "gvizCudaForceSaveEmbeddingText")
+
     def count_far_rows(self, causes=False):
         """(shared rows, per-target rows) of MLP evaluations in one force
         evaluation with the learned correction on; with causes=True also the

@@ -309,6 +309,36 @@ int gvizCudaFa2SpeedUpdateNoAlloc(const double *d_structForce,
                                   double jitterTolerance, double *d_swing,
                                   double *d_speedState, void *stream);
 
+/* ---- checkpoints ------------------------------------------------------ */
+
+/* Lossless checkpoint of a layout (or batch) in progress: positions,
+ * structForce, global speed and efficiency, iteration counters and the stat
+ * history, as raw bytes with a checksum. gviz's own save
+ * (gvizEmbeddedGraphSaveEmbedding, src/embedders/gvizEmbeddedGraph.c:428-448)
+ * keeps six decimals and no speed state, so it cannot resume a run; loading
+ * this file into a handle of the same graph continues bit for bit as if the
+ * run had not stopped. Returns 0, or GVIZ_CUDA_ERR_ARG when the file cannot
+ * be written. */
+int gvizCudaForceSaveCheckpoint(gvizCudaForce *h, const char *name,
+                                const char *filename);
+
+/* Restores a checkpoint into a handle created from the same graph (vertex
+ * and graph counts, graph offsets and model must match). restoreParams: 1
+ * also restores the configuration saved with it. nameOut (may be NULL)
+ * receives the saved name, truncated to nameCap - 1 bytes. Returns 0, or
+ * GVIZ_CUDA_ERR_ARG for a file that is missing, damaged (checksum) or from
+ * another graph; the handle is unchanged then. */
+int gvizCudaForceLoadCheckpoint(gvizCudaForce *h, const char *filename,
+                                int restoreParams, char *nameOut, size_t nameCap);
+
+/* Positions in gviz's text embedding format (name line, "count dim", one
+ * row per vertex) with 17 significant digits, which
+ * gvizEmbeddedGraphLoadEmbedding (src/embedders/gvizEmbeddedGraph.c:450-485)
+ * reads back exactly. Vertex i is compact index i (the parent id for a full
+ * subgraph). */
+int gvizCudaForceSaveEmbeddingText(gvizCudaForce *h, const char *name,
+                                   const char *filename);
+
 /* ---- graph files straight to CSR ------------------------------------- */
 
 /* A graph loaded from a file, in the layout's CSR form (library-owned

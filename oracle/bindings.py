@@ -346,6 +346,14 @@ class RefLayout:
     def state_ptr(self):
         return C.c_void_p(self.L.ref_state(self.h))
 
+    def load_embedding(self, path):
+        """gvizEmbeddedGraphLoadEmbedding; 0 or -1."""
+        return int(self.L.ref_load_embedding(self.h, str(path).encode()))
+
+    def save_embedding(self, path, name="ref"):
+        """gvizEmbeddedGraphSaveEmbedding (six decimals); 0 or -1."""
+        return int(self.L.ref_save_embedding(self.h, name.encode(), str(path).encode()))
+
     def run(self, max_iters, eps):
         return self.L.ref_run(self.h, C.c_size_t(max_iters), D(eps))
 

@@ -444,3 +444,12 @@ long long ref_load_obj_csr(const char *path, uint64_t *row, uint32_t *col, size_
   gvizGraphRelease(&g);
   return V;
 }
+
+/* gviz's own text embedding load / save on the embedder's graph. */
+int ref_load_embedding(refLayout *r, const char *path) {
+  return gvizEmbeddedGraphLoadEmbedding((gvizEmbeddedGraph *)&r->s, path);
+}
+
+int ref_save_embedding(refLayout *r, const char *name, const char *path) {
+  return gvizEmbeddedGraphSaveEmbedding((gvizEmbeddedGraph *)&r->s, name, path);
+}
