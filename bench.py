@@ -1,7 +1,7 @@
 """Benchmark of the B200 force-layout step (libgvizcuda).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ba1m_learned|ba1m|batch4096|grid32|er65k_exact]
+                    [--workload ba1m_learned|rmat4m_learned|ba1m|batch4096|grid32|er65k_exact]
 
 Default workload (the headline metric: learned vs plain Barnes-Hut at equal
 force error): Barabasi-Albert graph, n = 1,048,576, m = 4 (4,194,294 edges,
@@ -15,6 +15,10 @@ The plain walk runs at theta = 0.5; the learned walk at the largest theta of
 1.2, 1.1, ..., 0.6 whose error is not above the plain walk's. ``value`` is
 the learned path's iterations/s; the plain path's are in ``plain``. Both are
 timed from the same saved layout state.
+rmat4m_learned: the same comparison on an R-MAT graph, scale 22 (4,194,304
+vertices), 33,554,432 edge draws with (a,b,c,d) = (.57,.19,.19,.05),
+deduplicated, no self-loops, start uniform in [-1000, 1000]^2; adds the
+error of both paths every 20 iterations over 100 untimed iterations.
 ba1m: the same graph with degree-sized prevent-overlap
 (r = 1.0 * (1 + 0.5 sqrt(deg))), plain theta = 0.8, FP32 walk.
 batch4096: 4096 independent graphs, sizes log-uniform in [32, 8192], each an
@@ -53,6 +57,8 @@ MLP_FLOP_PER_ROW = 2 * (10 * 64 + 64 * 64 + 64 * 2)  # one 10-64-64-2 evaluation
 SPECS = {
     "ba1m_learned": dict(model=1, theta=0.5, gravity=1.0, radius_base=0.0,
                          radius_per_degree=0.0, overlap=False, bh=True),
+    "rmat4m_learned": dict(model=1, theta=0.5, gravity=1.0, radius_base=0.0,
+                           radius_per_degree=0.0, overlap=False, bh=True),
     "ba1m": dict(model=1, theta=0.8, gravity=1.0, radius_base=1.0, radius_per_degree=0.5,
                  overlap=True, bh=True),
     "batch4096": dict(model=0, theta=0.7, gravity=0.0, radius_base=0.0,
@@ -73,7 +79,13 @@ class Workload:
         self.name = name
         self.spec = SPECS[name]
         self.graphs = []  # (V, a, b, box, seed)
-        if name in ("ba1m", "ba1m_learned"):
+        if name == "rmat4m_learned":
+            V = 1 << 22
+            a, b = graphs.rmat(22, 1 << 25, 0.57, 0.19, 0.19, SEED)
+            self.graphs.append((V, a, b, 1000.0, SEED))
+            self.desc = (f"rmat scale=22 draws=33554432 (a,b,c,d)=(.57,.19,.19,.05) "
+                         f"deduplicated, edges={len(a)}")
+        elif name in ("ba1m", "ba1m_learned"):
             V = 1 << 20
             a, b = graphs.barabasi_albert(V, 4, SEED)
             self.graphs.append((V, a, b, 1000.0, SEED))
@@ -376,6 +388,28 @@ def learned_setup(lay, w):
     return model, info
 
 
+def error_trajectory(lay, w, linfo, chunks=5, every=20):
+    """Normalised RMS force error of the learned and the plain walk every
+    `every` iterations along `chunks` x `every` iterations from one state."""
+    rng = np.random.default_rng(SEED + 1)
+    targets = np.sort(rng.choice(w.V, min(JUDGE_VERTICES, w.V), replace=False)).astype(np.uint32)
+    x_s, (sf_s, sp_s, ef_s) = lay.positions(), lay.fa2_state()
+    out = {}
+    for name, th, ff in (("learned", linfo["learned_theta"], 1), ("plain", w.spec["theta"], 0)):
+        lay.set_positions(x_s)
+        lay.set_fa2_state(sf_s, sp_s, ef_s)
+        lay.set_params(theta=th, farField=ff)
+        errs = []
+        for c in range(chunks):
+            lay.time_steps(every)
+            exact = lay.exact_repulsion(targets)
+            errs.append(force_error(lay, targets, exact)[0])
+        out[name] = {"theta": th, "iterations": [every * (c + 1) for c in range(chunks)],
+                     "rms_err": errs}
+    lay.set_params(theta=linfo["learned_theta"], farField=1)
+    return out
+
+
 # ---------------------------------------------------------------------- ours
 def main():
     ap = argparse.ArgumentParser()
@@ -388,7 +422,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     w = Workload(args.workload)
-    learned = args.workload == "ba1m_learned"
+    learned = args.workload in ("ba1m_learned", "rmat4m_learned")
     if args.impl == "reference":
         return run_reference_arm(args, w)
 
@@ -518,9 +552,14 @@ def main():
         "vertex_updates_per_s": value * V, "roofline": roofline,
         "kernel_ms": {k: round(v, 4) for k, v in prof}, "peaks": peak_src,
     }
+    if learned and args.workload == "rmat4m_learned":
+        # the error along the run, every 20 iterations, for both paths from
+        # the state after the timed steps (untimed)
+        line["error_every_20"] = error_trajectory(lay, w, linfo)
     if learned:
-        line["metric"] = ("layout iters/sec, 1M-vertex BA graph: learned vs plain BH at "
-                          "equal force error")
+        line["metric"] = (("layout iters/sec, 1M-vertex BA graph" if args.workload == "ba1m_learned"
+                           else "layout iters/sec, R-MAT scale-22 graph")
+                          + ": learned vs plain BH at equal force error")
         line["learned"] = dict(linfo, value=value, theta=linfo["learned_theta"],
                                rms_err=linfo["learned_errors"][str(linfo["learned_theta"])]["rms_err"])
         line["plain"] = plain_line

@@ -86,6 +86,12 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_gChunkEnd);
   dfree(h->d_attrLight);
   dfree(h->d_attrHeavy);
+  dfree(h->d_hubV);
+  dfree(h->d_hubFirst);
+  dfree(h->d_hubChunkV);
+  dfree(h->d_hubChunkE0);
+  dfree(h->d_hubChunkE1);
+  dfree(h->d_hubPartial);
   dfree(h->d_pos);
   dfree(h->d_sf);
   dfree(h->d_sfOld);
@@ -442,11 +448,28 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
     gce[gg] = (uint32_t)cb.size();
   }
   h->nChunks = (uint32_t)cb.size();
-  std::vector<uint32_t> light, heavy;
-  for (size_t v = 0; v < V; v++)
-    (row[v + 1] - row[v] > GVIZ_HEAVY_DEGREE ? heavy : light).push_back((uint32_t)v);
+  std::vector<uint32_t> light, heavy, hubV, hubFirst, hcV, hcE0, hcE1;
+  for (size_t v = 0; v < V; v++) {
+    const uint64_t d = row[v + 1] - row[v];
+    if (d <= GVIZ_HEAVY_DEGREE) {
+      light.push_back((uint32_t)v);
+    } else if (d <= GVIZ_HUB_DEGREE) {
+      heavy.push_back((uint32_t)v);
+    } else {
+      hubV.push_back((uint32_t)v);
+      hubFirst.push_back((uint32_t)hcV.size());
+      for (uint64_t e = row[v]; e < row[v + 1]; e += GVIZ_HUB_CHUNK) {
+        hcV.push_back((uint32_t)v);
+        hcE0.push_back((uint32_t)e);
+        hcE1.push_back((uint32_t)std::min<uint64_t>(e + GVIZ_HUB_CHUNK, row[v + 1]));
+      }
+    }
+  }
+  hubFirst.push_back((uint32_t)hcV.size());
   h->nAttrLight = (uint32_t)light.size();
   h->nAttrHeavy = (uint32_t)heavy.size();
+  h->nHubs = (uint32_t)hubV.size();
+  h->nHubChunks = (uint32_t)hcV.size();
   h->h_graphOff = (uint64_t *)malloc(sizeof(uint64_t) * (G + 1));
   h->h_meanDegPlusOne = (double *)malloc(sizeof(double) * G);
   memcpy(h->h_graphOff, goff.data(), sizeof(uint64_t) * (G + 1));
@@ -478,6 +501,12 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_gChunkEnd, G);
   rc |= dalloc(h, &h->d_attrLight, light.size());
   rc |= dalloc(h, &h->d_attrHeavy, heavy.size());
+  rc |= dalloc(h, &h->d_hubV, hubV.size());
+  rc |= dalloc(h, &h->d_hubFirst, hubFirst.size());
+  rc |= dalloc(h, &h->d_hubChunkV, hcV.size());
+  rc |= dalloc(h, &h->d_hubChunkE0, hcE0.size());
+  rc |= dalloc(h, &h->d_hubChunkE1, hcE1.size());
+  rc |= dalloc(h, &h->d_hubPartial, hcV.size());
   rc |= dalloc(h, &h->d_pos, Vs);
   rc |= dalloc(h, &h->d_sf, Vs);
   rc |= dalloc(h, &h->d_sfOld, Vs);
@@ -571,6 +600,11 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   up(h->d_gChunkEnd, gce.data(), G * 4);
   up(h->d_attrLight, light.data(), light.size() * 4);
   up(h->d_attrHeavy, heavy.data(), heavy.size() * 4);
+  up(h->d_hubV, hubV.data(), hubV.size() * 4);
+  up(h->d_hubFirst, hubFirst.data(), hubFirst.size() * 4);
+  up(h->d_hubChunkV, hcV.data(), hcV.size() * 4);
+  up(h->d_hubChunkE0, hcE0.data(), hcE0.size() * 4);
+  up(h->d_hubChunkE1, hcE1.data(), hcE1.size() * 4);
   ok = ok && cudaMemset(h->d_nCounter, 0, Vs * 4) == cudaSuccess;
   ok = ok && cudaMemset(h->d_pos, 0, Vs * 16) == cudaSuccess;
   ok = ok && cudaMemset(h->d_counters, 0, 64) == cudaSuccess;

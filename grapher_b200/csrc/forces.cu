@@ -114,6 +114,57 @@ __global__ __launch_bounds__(kAttrThreads) void k_attr_f32_heavy(AttrArgs a) {
   if (lane == 0) a.out[v] = make_float2((float)sx, (float)sy);
 }
 
+// Hubs above GVIZ_HUB_DEGREE: one warp per GVIZ_HUB_CHUNK-entry chunk of
+// the hub's adjacency, each writing an FP64 partial ...
+struct HubArgs {
+  const uint32_t *rowOff, *cols, *gid, *active;
+  const uint32_t *chunkV, *chunkE0, *chunkE1, *hubV, *hubFirst;
+  const double2 *pos;
+  double2 *partial;
+  float2 *out;
+  float invK;
+  uint32_t nChunks, nHubs;
+};
+
+template <int MODEL>
+__global__ __launch_bounds__(kAttrThreads) void k_attr_f32_hub_chunks(HubArgs a) {
+  const uint32_t w = (blockIdx.x * kAttrThreads + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (w >= a.nChunks) return;
+  const uint32_t v = a.chunkV[w];
+  if (a.active && !a.active[a.gid ? a.gid[v] : 0u]) return;
+  const double2 p = a.pos[v];
+  Kahan kx, ky;
+  const uint32_t e1 = a.chunkE1[w];
+  for (uint32_t e = a.chunkE0[w] + lane; e < e1; e += 32) {
+    float tx, ty;
+    if (attr_term<MODEL>(p, a.pos[a.cols[e]], a.invK, tx, ty)) {
+      kx.add(tx);
+      ky.add(ty);
+    }
+  }
+  double sx = kx.value(), sy = ky.value();
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+  }
+  if (lane == 0) a.partial[w] = make_double2(sx, sy);
+}
+
+// ... then each hub's partials summed in chunk order (deterministic).
+__global__ __launch_bounds__(kAttrThreads) void k_attr_hub_sum(HubArgs a) {
+  const uint32_t i = blockIdx.x * kAttrThreads + threadIdx.x;
+  if (i >= a.nHubs) return;
+  const uint32_t v = a.hubV[i];
+  if (a.active && !a.active[a.gid ? a.gid[v] : 0u]) return;
+  double sx = 0.0, sy = 0.0;
+  for (uint32_t c = a.hubFirst[i]; c < a.hubFirst[i + 1]; c++) {
+    sx += a.partial[c].x;
+    sy += a.partial[c].y;
+  }
+  a.out[v] = make_float2((float)sx, (float)sy);
+}
+
 struct WalkArgs {
   const NodeF *nodes;
   const uint32_t *idx, *gid, *active, *graphBase, *rootT;
@@ -612,6 +663,28 @@ void enqueue_attraction_f32(gvizCudaForce *h) {
     const uint32_t g = blocks((size_t)a.n * 32, kAttrThreads);
     if (fr) k_attr_f32_heavy<GVIZ_CUDA_MODEL_FR><<<g, kAttrThreads, 0, h->stream>>>(a);
     else k_attr_f32_heavy<GVIZ_CUDA_MODEL_LINLOG><<<g, kAttrThreads, 0, h->stream>>>(a);
+  }
+  if (h->nHubs) {
+    HubArgs b;
+    b.rowOff = h->d_rowOff;
+    b.cols = h->d_cols;
+    b.gid = h->d_gid;
+    b.active = h->d_active;
+    b.chunkV = h->d_hubChunkV;
+    b.chunkE0 = h->d_hubChunkE0;
+    b.chunkE1 = h->d_hubChunkE1;
+    b.hubV = h->d_hubV;
+    b.hubFirst = h->d_hubFirst;
+    b.pos = h->d_pos;
+    b.partial = h->d_hubPartial;
+    b.out = h->d_attF;
+    b.invK = a.invK;
+    b.nChunks = h->nHubChunks;
+    b.nHubs = h->nHubs;
+    const uint32_t g = blocks((size_t)b.nChunks * 32, kAttrThreads);
+    if (fr) k_attr_f32_hub_chunks<GVIZ_CUDA_MODEL_FR><<<g, kAttrThreads, 0, h->stream>>>(b);
+    else k_attr_f32_hub_chunks<GVIZ_CUDA_MODEL_LINLOG><<<g, kAttrThreads, 0, h->stream>>>(b);
+    k_attr_hub_sum<<<blocks(b.nHubs, kAttrThreads), kAttrThreads, 0, h->stream>>>(b);
   }
   prof_mark(h, "attraction_f32");
 }

@@ -14,6 +14,8 @@
 #define GVIZ_DIR_TABLE 256       // coincident-direction table entries
 #define GVIZ_STATS_CAP 4096      // stat rows kept per graph (ring)
 #define GVIZ_HEAVY_DEGREE 16     // attraction: warp per vertex above this
+#define GVIZ_HUB_DEGREE 4096  // above: split across warps (attraction)
+#define GVIZ_HUB_CHUNK 2048   // adjacency entries per hub chunk
 // The radix sort orders the top 48 bits of the composite (graph, path) key:
 // 24 quadtree levels of one graph. Runs equal in those bits and longer than
 // the leaf capacity are finished by the shared-memory fix-up sort.
@@ -108,6 +110,13 @@ struct gvizCudaForce {
   // thread, hubs above it a warp
   uint32_t *d_attrLight = nullptr, *d_attrHeavy = nullptr;
   uint32_t nAttrLight = 0, nAttrHeavy = 0;
+  // hubs above GVIZ_HUB_DEGREE (power-law graphs reach degrees in the
+  // hundreds of thousands): GVIZ_HUB_CHUNK-entry chunks, a warp each, then
+  // the chunk partials summed per hub in chunk order
+  uint32_t *d_hubV = nullptr, *d_hubFirst = nullptr;  // hubs, nHubs + 1
+  uint32_t *d_hubChunkV = nullptr, *d_hubChunkE0 = nullptr, *d_hubChunkE1 = nullptr;
+  double2 *d_hubPartial = nullptr;
+  uint32_t nHubs = 0, nHubChunks = 0;
 
   // --- layout state (device) ---
   double2 *d_pos = nullptr;

@@ -155,3 +155,32 @@ def test_free_run_fp64_tracks_oracle(oracle):
     e_ref = np.linalg.norm(pos_o.reshape(-1, 2)[a] - pos_o.reshape(-1, 2)[b], axis=1).mean()
     assert abs(e_gpu - e_ref) <= 1e-3 * e_ref
     lay.close()
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_hub_attraction_split_across_warps(model):
+    """A hub above 4096 neighbours is summed in 2048-entry chunks by
+    separate warps and the partials added in chunk order; its attraction
+    must still match an FP64 sum of the reference's per-pair formula
+    (include/core/gvizVec.h:320-334 and 486-499)."""
+    from grapher_b200 import graphs
+    rng = np.random.default_rng(11)
+    V = 30001
+    a = np.zeros(V - 1, np.uint32)                 # hub 0 to every vertex
+    b = np.arange(1, V, dtype=np.uint32)
+    extra = rng.integers(1, V, (2000, 2)).astype(np.uint32)
+    a = np.concatenate([a, extra[:, 0]])
+    b = np.concatenate([b, extra[:, 1]])
+    row, col = graphs.to_csr(V, a, b)
+    x0 = graphs.randomize_positions(V, 500.0, 2)
+    lay = make_layout(row, col, cfg(model=model, theta=0.8))
+    lay.begin(0, positions=x0)
+    lay.step()
+    att = lay.forces()["attMag"]
+    p = x0.reshape(-1, 2)
+    for v in (0, 7):   # the hub, and a light vertex
+        q = p[col[row[v]:row[v + 1]]] - p[v]
+        d = np.linalg.norm(q, axis=1)
+        s = d / 10.0 if model == 0 else np.log1p(d) / d
+        want = np.linalg.norm((s[:, None] * q).sum(0))
+        assert abs(att[v] - want) <= 1e-5 * want, (v, att[v], want)
