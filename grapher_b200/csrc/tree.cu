@@ -402,7 +402,7 @@ __global__ __launch_bounds__(kThreads) void k_karras(
 }
 
 struct BU {
-  const uint32_t *idx, *bStart, *bGid, *counts, *nLeft, *nRight;
+  const uint32_t *idx, *bStart, *bGid, *counts, *nLeft, *nRight, *nFirst, *nLast;
   const int32_t *nDelta;
   const double *mass;
   const double2 *pos;
@@ -417,8 +417,8 @@ struct BU {
 // second central moments of a child about its own centre of mass
 __device__ __forceinline__ double4 child_q(const BU &a, uint32_t c) {
   const double4 *p = (c & GVIZ_LEAF_BIT) ? a.bQ + (c & ~GVIZ_LEAF_BIT) : a.nQ + c;
-  const double2 lo = __ldcg(reinterpret_cast<const double2 *>(p));
-  const double2 hi = __ldcg(reinterpret_cast<const double2 *>(p) + 1);
+  const double2 lo = reinterpret_cast<const double2 *>(p)[0];
+  const double2 hi = reinterpret_cast<const double2 *>(p)[1];
   return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
@@ -440,19 +440,21 @@ __device__ __forceinline__ void add_shifted(double4 &q, const double4 qc,
 __device__ __forceinline__ void child_vals(const BU &a, uint32_t c, double &M,
                                            double &SX, double &SY,
                                            uint32_t &cnt, uint32_t &T) {
+  // plain loads: the acquire on the arrival counter (block or device scope)
+  // makes the sibling's stores visible
   if (c & GVIZ_LEAF_BIT) {
     uint32_t b = c & ~GVIZ_LEAF_BIT;
-    M = __ldcg(a.bM + b);
-    SX = __ldcg(a.bSX + b);
-    SY = __ldcg(a.bSY + b);
-    cnt = __ldcg(a.bCnt + b);
-    T = __ldcg(a.bT + b);
+    M = a.bM[b];
+    SX = a.bSX[b];
+    SY = a.bSY[b];
+    cnt = a.bCnt[b];
+    T = a.bT[b];
   } else {
-    M = __ldcg(a.nM + c);
-    SX = __ldcg(a.nSX + c);
-    SY = __ldcg(a.nSY + c);
-    cnt = __ldcg(a.nCnt + c);
-    T = __ldcg(a.nT + c);
+    M = a.nM[c];
+    SX = a.nSX[c];
+    SY = a.nSY[c];
+    cnt = a.nCnt[c];
+    T = a.nT[c];
   }
 }
 
@@ -461,10 +463,18 @@ __device__ __forceinline__ uint2 *up_of(const BU &a, uint32_t c) {
 }
 
 // Sums per bucket, then each thread climbs; the second child to arrive at a
-// node combines both (left first: fixed order, deterministic sums).
+// node combines both (left first: fixed order, deterministic sums). A node
+// whose buckets all belong to this block has both children summed by
+// threads of this block: its arrivals meet in shared memory with block-scope
+// ordering; only nodes spanning blocks pay for device-scope ordering.
 __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
+  __shared__ uint32_t sArrive[kThreads];
+  sArrive[threadIdx.x] = 0u;
+  __syncthreads();
   const uint32_t U = a.counts[2];
-  const uint32_t b = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t B0 = blockIdx.x * kThreads;
+  const uint32_t B1 = min(B0 + kThreads, U);
+  const uint32_t b = B0 + threadIdx.x;
   if (b >= U) return;
   const uint32_t start = a.bStart[b];
   const uint32_t end = (b + 1 < U) ? a.bStart[b + 1] : a.V;
@@ -518,10 +528,16 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       return;
     }
     // release this child's sums / acquire the sibling's: the second thread
-    // to arrive combines both
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrivals(a.nCounter[p]);
-    if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
-    a.nCounter[p] = 0u;
+    // to arrive combines both (Karras node p is one end of its own range,
+    // so an in-block node has p in [B0, B1))
+    if (p >= B0 && p < B1 && a.nFirst[p] >= B0 && a.nLast[p] < B1) {
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrivals(sArrive[p - B0]);
+      if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
+    } else {
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrivals(a.nCounter[p]);
+      if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
+      a.nCounter[p] = 0u;
+    }
     const uint32_t l = a.nLeft[p], r = a.nRight[p];
     double Ml, SXl, SYl, Mr, SXr, SYr;
     uint32_t cl, Tl, cr, Tr;
@@ -910,6 +926,8 @@ void enqueue_tree_build(gvizCudaForce *h) {
   bu.counts = h->d_counts;
   bu.nLeft = h->d_nLeft;
   bu.nRight = h->d_nRight;
+  bu.nFirst = h->d_nFirst;
+  bu.nLast = h->d_nLast;
   bu.nDelta = h->d_nDelta;
   bu.mass = h->d_mass;
   bu.pos = h->d_pos;
