@@ -324,7 +324,7 @@ class nvtx_range:
 
 # ------------------------------------------------------------ learned setup
 LEARNED_THETAS = (1.2, 1.1, 1.0, 0.9, 0.8, 0.7, 0.6)
-LEARNED_SPREAD = 0.5
+LEARNED_SPREAD = 1.0
 JUDGE_VERTICES = 65536
 
 

@@ -340,7 +340,7 @@ void gvizCudaForceDefaultParams(gvizCudaForceParams *p) {
   p->jitterTolerance = 1.0;    // GVIZ_FORCE_EMBEDDER_JITTER_TOLERANCE_DEFAULT
   p->strictReductions = 0;
   p->farField = 0;
-  p->farGroupSpread = 0.25;
+  p->farGroupSpread = 1.0;
 }
 
 int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
