@@ -444,6 +444,9 @@ def main():
     lay.begin(0, positions=w.x0)
     for _ in range(args.warmup):
         lay.step()
+    # the walk's launch shape for this layout (block size, static or
+    # persistent schedule), timed on the warmed-up positions
+    shape = lay.autotune() if w.spec["bh"] else None
 
     def barrier():
         if dist:
@@ -552,6 +555,9 @@ def main():
         "vertex_updates_per_s": value * V, "roofline": roofline,
         "kernel_ms": {k: round(v, 4) for k, v in prof}, "peaks": peak_src,
     }
+    if shape:
+        line["walk_shape"] = {"threads": shape[0], "persistent": shape[1],
+                              "autotune_walk_ms": round(shape[2], 4)}
     if learned and args.workload == "rmat4m_learned":
         # the error along the run, every 20 iterations, for both paths from
         # the state after the timed steps (untimed)

@@ -151,6 +151,8 @@ _SIGS = {
     "gvizCudaGenErdosRenyi": (SZ, [SZ, SZ, C.c_uint64, U32P, U32P]),
     "gvizCudaGenRmat": (SZ, [C.c_uint32, SZ, D, D, D, C.c_uint64, U32P, U32P]),
     "gvizCudaEdgesToCsr": (C.c_int, [SZ, U32P, U32P, SZ, U64P, U32P]),
+    "gvizCudaForceAutotune": (C.c_int, [P, U32P, I32P, C.POINTER(C.c_float)]),
+    "gvizCudaForceSetWalkShape": (C.c_int, [P, C.c_uint32, C.c_int32]),
     "gvizCudaForceSaveCheckpoint": (C.c_int, [P, C.c_char_p, C.c_char_p]),
     "gvizCudaForceLoadCheckpoint": (C.c_int, [P, C.c_char_p, C.c_int, C.c_char_p, SZ]),
     "gvizCudaForceSaveEmbeddingText": (C.c_int, [P, C.c_char_p, C.c_char_p]),

@@ -160,6 +160,7 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_nodes);
   dfree(h->d_leafDepth);
   dfree(h->d_counters);
+  dfree(h->d_walkQueue);
 }
 
 int upload_radius(gvizCudaForce *h) {
@@ -577,6 +578,7 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_nodes, h->maxNodes * sizeof(NodeD));
   rc |= dalloc(h, &h->d_leafDepth, Vs);
   rc |= dalloc(h, &h->d_counters, 8);
+  rc |= dalloc(h, &h->d_walkQueue, 1);
   if (rc) {
     gvizCudaForceDestroy(h);
     return GVIZ_CUDA_ERR_ALLOC;
@@ -1360,6 +1362,81 @@ int gvizCudaForceSaveEmbeddingText(gvizCudaForce *h, const char *name, const cha
     ok = fprintf(f, "%.17g %.17g \n", pos[2 * i], pos[2 * i + 1]) > 0;
   ok = (fclose(f) == 0) && ok;
   return ok ? GVIZ_CUDA_OK : set_err(h, GVIZ_CUDA_ERR_ARG);
+}
+
+
+// ---- walk launch autotuning ------------------------------------------------
+
+int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threadsOut, int32_t *persistentOut,
+                          float *walkMsOut) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  if (h->V == 0 || !h->params.barnesHutEnabled || h->params.farField ||
+      h->params.precision != GVIZ_CUDA_FP32)
+    return GVIZ_CUDA_OK;  // only the FP32 plain walk has launch choices
+  static const uint32_t kCandidates[] = {64, 128, 256, 512};
+  const gvizCudaForceParams saved = h->params;
+  h->forceOnly = true;
+  cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+  enqueue_tree_build(h);
+  enqueue_attraction_f32(h);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = INFINITY;
+  uint32_t bestThreads = kWalkDefaultThreads;
+  bool bestPersistent = false;
+  uint32_t bestResident = 0;
+  for (int persistent = 0; persistent < 2; persistent++) {
+    for (uint32_t t : kCandidates) {
+      h->walkThreads = t;
+      h->walkPersistent = persistent != 0;
+      h->walkResident = persistent ? walk_resident_blocks(h, t) : 0;
+      if (persistent && !h->walkResident) continue;
+      enqueue_walk_f32(h, nullptr);  // warm-up; forces-only launches repeat cleanly
+      float ms = INFINITY;
+      for (int r = 0; r < 3; r++) {
+        cudaEventRecord(e0, h->stream);
+        enqueue_walk_f32(h, nullptr);
+        cudaEventRecord(e1, h->stream);
+        float m = 0.f;
+        if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&m, e0, e1) == cudaSuccess)
+          ms = std::min(ms, m);
+      }
+      if (ms < best) {
+        best = ms;
+        bestThreads = t;
+        bestPersistent = persistent != 0;
+        bestResident = h->walkResident;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->forceOnly = false;
+  h->params = saved;
+  h->walkThreads = bestThreads;
+  h->walkPersistent = bestPersistent;
+  h->walkResident = bestResident;
+  h->graphDirty = true;
+  const int rc = sync_and_check(h);
+  if (threadsOut) *threadsOut = bestThreads;
+  if (persistentOut) *persistentOut = bestPersistent ? 1 : 0;
+  if (walkMsOut) *walkMsOut = best;
+  return rc;
+}
+
+
+int gvizCudaForceSetWalkShape(gvizCudaForce *h, uint32_t threads, int32_t persistent) {
+  if (!h || threads < 32 || threads > 512 || threads % 32 != 0) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
+  const uint32_t resident = persistent ? walk_resident_blocks(h, threads) : 0;
+  if (persistent && !resident) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  h->walkThreads = threads;
+  h->walkPersistent = persistent != 0;
+  h->walkResident = resident;
+  h->graphDirty = true;
+  return GVIZ_CUDA_OK;
 }
 
 }  // extern "C"

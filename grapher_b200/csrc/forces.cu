@@ -26,7 +26,8 @@ int dir_table_upload_forces(const double *t) {
 
 namespace {
 
-constexpr int kWalkThreads = 128;
+constexpr int kWalkThreads = 128;     // default block size of the walk
+constexpr int kWalkMaxThreads = 512;  // largest block size the autotuner tries
 constexpr int kAttrThreads = 256;
 constexpr int kExactThreads = 256;
 constexpr int kExactTile = 256;
@@ -177,6 +178,7 @@ struct WalkArgs {
   float overlapC;
   uint32_t V;
   unsigned long long *counters;  // [0] interactions, [1] warp node visits
+  uint32_t *queue;               // next task of the persistent schedule
 };
 
 // One pair or pseudo-body term of FR / LinLog repulsion
@@ -212,10 +214,12 @@ __device__ __forceinline__ void rep_term(float dx, float dy, float d2,
   }
 }
 
+// One walk task: the 32 path-sorted targets starting at sorted position
+// 32 * task, one per lane.
 template <int MODEL, bool OVERLAP, bool COUNT>
-__global__ __launch_bounds__(kWalkThreads) void k_walk_f32(WalkArgs a) {
+__device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task) {
   const unsigned lane = threadIdx.x & 31u;
-  const uint32_t s = ((blockIdx.x * kWalkThreads + threadIdx.x) >> 5) * 32u + lane;
+  const uint32_t s = task * 32u + lane;
   const bool valid = s < a.V;
   const uint32_t v = valid ? a.idx[s] : 0u;
   const uint32_t g = (valid && a.gid) ? a.gid[v] : 0u;
@@ -276,6 +280,27 @@ __global__ __launch_bounds__(kWalkThreads) void k_walk_f32(WalkArgs a) {
   if (!act) return;
   const float2 at = a.attF[v];
   force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value(), ky.value());
+}
+
+// Static schedule: warp w of the grid takes task w.
+template <int MODEL, bool OVERLAP, bool COUNT>
+__global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32(WalkArgs a) {
+  walk_task<MODEL, OVERLAP, COUNT>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+}
+
+// Persistent schedule: a grid sized to fill the GPU once; each warp takes
+// the next task from a device counter (reset before every launch) until
+// the queue is empty, so warps that drew cheap tasks take more of them.
+template <int MODEL, bool OVERLAP, bool COUNT>
+__global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32_queue(WalkArgs a) {
+  const uint32_t tasks = (a.V + 31u) / 32u;
+  for (;;) {
+    uint32_t t = 0;
+    if ((threadIdx.x & 31u) == 0u) t = atomicAdd(a.queue, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= tasks) return;
+    walk_task<MODEL, OVERLAP, COUNT>(a, t);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -691,9 +716,17 @@ void enqueue_attraction_f32(gvizCudaForce *h) {
 
 template <int MODEL, bool OVERLAP, bool COUNT>
 static void launch_walk(gvizCudaForce *h, const WalkArgs &a) {
-  uint32_t warps = (uint32_t)((h->V + 31) / 32);
-  uint32_t grid = blocks((size_t)warps * 32, kWalkThreads);
-  k_walk_f32<MODEL, OVERLAP, COUNT><<<grid, kWalkThreads, 0, h->stream>>>(a);
+  const uint32_t threads = h->walkThreads ? h->walkThreads : kWalkThreads;
+  const uint32_t warps = (uint32_t)((h->V + 31) / 32);
+  if (h->walkPersistent && h->walkResident) {
+    cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), h->stream);
+    const uint32_t need = blocks((size_t)warps * 32, threads);
+    const uint32_t grid = need < h->walkResident ? need : h->walkResident;
+    k_walk_f32_queue<MODEL, OVERLAP, COUNT><<<grid, threads, 0, h->stream>>>(a);
+    return;
+  }
+  k_walk_f32<MODEL, OVERLAP, COUNT><<<blocks((size_t)warps * 32, threads), threads, 0,
+                                      h->stream>>>(a);
 }
 
 template <int MODEL, bool OVERLAP>
@@ -723,6 +756,30 @@ static void enqueue_far(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters)
   prof_mark(h, "bh_walk_f32_learned");
 }
 
+// Blocks of `threads` threads that fill the GPU once with the persistent
+// walk of this handle's model and overlap setting.
+uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool ov = h->params.preventOverlap != 0;
+  const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
+  cudaError_t e;
+  if (fr) {
+    e = ov ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, true, false>, threads, 0)
+           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, false, false>, threads, 0);
+  } else {
+    e = ov ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, true, false>, threads, 0)
+           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, false, false>, threads, 0);
+  }
+  if (e != cudaSuccess || per <= 0 || sms <= 0) return 0;
+  return (uint32_t)(per * sms);
+}
+
 void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   WalkArgs a;
   a.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
@@ -740,6 +797,7 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   a.overlapC = (float)h->params.overlapConstant;
   a.V = (uint32_t)h->V;
   a.counters = reinterpret_cast<unsigned long long *>(counters);
+  a.queue = h->d_walkQueue;
   a.maxNodes = (uint32_t)h->maxNodes;
   const bool ov = h->params.preventOverlap != 0;
   const bool fr = h->model == GVIZ_CUDA_MODEL_FR;

@@ -16,6 +16,7 @@
 #define GVIZ_HEAVY_DEGREE 16     // attraction: warp per vertex above this
 #define GVIZ_HUB_DEGREE 4096  // above: split across warps (attraction)
 #define GVIZ_HUB_CHUNK 2048   // adjacency entries per hub chunk
+constexpr uint32_t kWalkDefaultThreads = 128;  // walk block size before autotuning
 // The radix sort orders the top 48 bits of the composite (graph, path) key:
 // 24 quadtree levels of one graph. Runs equal in those bits and longer than
 // the leaf capacity are finished by the shared-memory fix-up sort.
@@ -134,6 +135,12 @@ struct gvizCudaForce {
   double *d_stats = nullptr;        // [GVIZ_STATS_CAP][G][5]
   double *d_lastStats = nullptr;    // [G][5], the latest row per graph
   uint64_t *d_counters = nullptr;   // instrumentation counters
+  uint32_t *d_walkQueue = nullptr;  // task counter of the persistent walk
+  // walk launch shape (gvizCudaForceAutotune): block size, persistent
+  // work-queue schedule, and the resident grid for it (0: not measured)
+  uint32_t walkThreads = 0;
+  bool walkPersistent = false;
+  uint32_t walkResident = 0;
   ChunkStat *d_chunkStat = nullptr;
   uint32_t *d_status = nullptr;
 
@@ -265,6 +272,7 @@ int dir_table_upload_precise(const double *t);
 // forces.cu (FP32, fused multiply-add on)
 void enqueue_attraction_f32(gvizCudaForce *h);
 void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters);
+uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads);
 void enqueue_exact_f32(gvizCudaForce *h);
 
 // precise.cu (FP64 + FA2, compiled without fused multiply-add)

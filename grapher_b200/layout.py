@@ -287,6 +287,18 @@ class ForceLayout:
                 "gvizCudaForceCountInteractions")
         return a.value, b.value
 
+    def autotune(self):
+        """Times the FP32 walk's launch shapes on the current positions and
+        keeps the fastest: returns (threads per block, persistent, walk ms)."""
+        t, p, ms = C.c_uint32(), C.c_int32(), C.c_float()
+        N.check(self.L.gvizCudaForceAutotune(self.h, C.byref(t), C.byref(p), C.byref(ms)),
+                "gvizCudaForceAutotune")
+        return int(t.value), bool(p.value), float(ms.value)
+
+    def set_walk_shape(self, threads, persistent):
+        N.check(self.L.gvizCudaForceSetWalkShape(self.h, threads, int(persistent)),
+                "gvizCudaForceSetWalkShape")
+
     # ------------------------------------------------------------ checkpoints
     def save_checkpoint(self, filename, name=""):
         """Lossless checkpoint (positions, FA2 history, counters, stats)."""

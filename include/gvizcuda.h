@@ -309,6 +309,20 @@ int gvizCudaFa2SpeedUpdateNoAlloc(const double *d_structForce,
                                   double jitterTolerance, double *d_swing,
                                   double *d_speedState, void *stream);
 
+/* Picks the FP32 walk's launch shape for this layout by timing it on the
+ * current positions: blocks of 64 to 512 threads, and a static grid (warp w
+ * takes the 32 path-sorted targets of task w) or a persistent one (a grid
+ * that fills the GPU once; each warp takes tasks from a device counter until
+ * none are left). Forces do not depend on the choice. Keeps the fastest for
+ * later steps; reports it (each output may be NULL). Does nothing for FP64,
+ * exact or learned walks. No reference counterpart. */
+int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threads,
+                          int32_t *persistent, float *walkMs);
+
+/* Sets the FP32 walk's launch shape directly: threads per block (a multiple
+ * of 32, at most 512) and the persistent schedule (1) or the static one. */
+int gvizCudaForceSetWalkShape(gvizCudaForce *h, uint32_t threads, int32_t persistent);
+
 /* ---- checkpoints ------------------------------------------------------ */
 
 /* Lossless checkpoint of a layout (or batch) in progress: positions,

@@ -72,3 +72,36 @@ def test_batch_run_stops_each_graph_on_its_own():
         s = slice(2 * int(offs[g]), 2 * int(offs[g + 1]))
         assert np.array_equal(batch.positions()[s], lay.positions())
     assert rounds.min() < rounds.max() or rounds.min() == 200
+
+
+def test_walk_shapes_and_autotune_give_identical_forces():
+    """The walk's launch shape (block size, static or persistent work-queue
+    schedule) changes which warp runs a task, never what it computes: every
+    shape gives the same forces and steps bit for bit, single and batched."""
+    from grapher_b200 import graphs
+    from grapher_b200._native import GvizCudaError
+    gs = small_graphs(3)
+    row, col, offs = graphs.batch(gs)
+    x0 = np.concatenate([graphs.randomize_positions(V, 10.0, 3 + i) for i, (V, _, _) in enumerate(gs)])
+    c = cfg(model=1, theta=0.8, gravity=1.0)
+    ref = make_layout(row, col, c, graph_offsets=offs)
+    ref.begin(0, positions=x0)
+    want = ref.repulsion()
+    for _ in range(3):
+        ref.step()
+    for threads in (64, 128, 256, 512):
+        for persistent in (False, True):
+            lay = make_layout(row, col, c, graph_offsets=offs)
+            lay.begin(0, positions=x0)
+            lay.set_walk_shape(threads, persistent)
+            assert np.array_equal(lay.repulsion(), want)
+            for _ in range(3):
+                lay.step()
+            assert np.array_equal(lay.positions(), ref.positions())
+    lay = make_layout(row, col, c, graph_offsets=offs)
+    lay.begin(0, positions=x0)
+    threads, persistent, ms = lay.autotune()
+    assert threads in (64, 128, 256, 512) and ms > 0
+    assert np.array_equal(lay.repulsion(), want)
+    with pytest.raises(GvizCudaError):
+        lay.set_walk_shape(100, False)
