@@ -198,19 +198,42 @@ __device__ __forceinline__ void rep_term(float dx, float dy, float d2,
       const float gap = dist - radiusSum;
       const float mag = gap > 0.0f ? __fdividef(numer, gap) : numer * C;
       const float s = mag * inv * mult;
-      fx = -s * dx;
-      fy = -s * dy;
+      fx = __fmul_rn(-s, dx);  // never fused into the caller's sums
+      fy = __fmul_rn(-s, dy);
     } else {
       const float s = __fdividef(numer, d2) * mult;
-      fx = -s * dx;
-      fy = -s * dy;
+      fx = __fmul_rn(-s, dx);  // never fused into the caller's sums
+      fy = __fmul_rn(-s, dy);
     }
   } else {
     double ux, uy;
     coincident_dir(self, other, ux, uy);
     const float mag = numer * C * mult;
-    fx = -mag * (float)ux;
-    fy = -mag * (float)uy;
+    fx = __fmul_rn(-mag, (float)ux);
+    fy = __fmul_rn(-mag, (float)uy);
+  }
+}
+
+// rep_term for d2 > 0: the same arithmetic, without the coincident branch,
+// so the common case compiles to straight-line predicated code.
+template <int MODEL, bool OVERLAP>
+__device__ __forceinline__ void rep_term_apart(float dx, float dy, float d2, float mv,
+                                               float mo, float radiusSum, float num,
+                                               float C, float &fx, float &fy) {
+  const float numer = (MODEL == GVIZ_CUDA_MODEL_FR) ? num : mv * mo;
+  const float mult = (MODEL == GVIZ_CUDA_MODEL_FR) ? truncf(mo) : 1.0f;
+  if (OVERLAP) {
+    const float inv = rsqrtf(d2);
+    const float dist = d2 * inv;
+    const float gap = dist - radiusSum;
+    const float mag = gap > 0.0f ? __fdividef(numer, gap) : numer * C;
+    const float s = mag * inv * mult;
+    fx = __fmul_rn(-s, dx);  // never fused into the caller's sums
+    fy = __fmul_rn(-s, dy);
+  } else {
+    const float s = __fdividef(numer, d2) * mult;
+    fx = __fmul_rn(-s, dx);  // never fused into the caller's sums
+    fy = __fmul_rn(-s, dy);
   }
 }
 
@@ -256,7 +279,9 @@ __device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task) {
     const bool doForce =
         active && massOk && (isLeaf ? ((uint32_t)ninfo != v) : accept);
     const bool open = active && massOk && !isLeaf && !accept;
-    if (__any_sync(0xffffffffu, doForce)) {
+    // coincident points are rare: one vote keeps their branch off the
+    // common path, which stays straight-line
+    if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {
       if (doForce) {
         float fx, fy;
         rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass,
@@ -265,9 +290,15 @@ __device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task) {
                                  fx, fy);
         kx.add(fx);
         ky.add(fy);
-        if (COUNT) nInter++;
       }
+    } else if (doForce) {
+      float fx, fy;
+      rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + (isLeaf ? nsize : 0.0f),
+                                     a.num, a.overlapC, fx, fy);
+      kx.add(fx);
+      ky.add(fy);
     }
+    if (COUNT && doForce) nInter++;
     if (active) resume = open ? cur + 1u : max((uint32_t)nnext, cur + 1u);
     nxt = resume < myEnd ? resume : kInf;
     if (COUNT) nVisit++;
@@ -449,15 +480,20 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
     const bool doForce = active && massOk && (isLeaf ? ((uint32_t)ninfo != v) : accept);
     const bool open = active && massOk && !isLeaf && !accept;
     float fx = 0.f, fy = 0.f;
-    if (__any_sync(0xffffffffu, doForce)) {
+    if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {  // coincident points: rare
       if (doForce) {
         rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + (isLeaf ? nsize : 0.0f), a.num,
                                  a.overlapC, v, isLeaf ? (uint32_t)ninfo : v, fx, fy);
         kx.add(fx);
         ky.add(fy);
-        if (COUNT) nInter++;
       }
+    } else if (doForce) {
+      rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + (isLeaf ? nsize : 0.0f),
+                                     a.num, a.overlapC, fx, fy);
+      kx.add(fx);
+      ky.add(fy);
     }
+    if (COUNT && doForce) nInter++;
     const bool wantMlp = doForce && !isLeaf;
     const uint32_t ball = __ballot_sync(0xffffffffu, wantMlp);
     if (ball) {
