@@ -322,6 +322,22 @@ class nvtx_range:
         torch.cuda.nvtx.range_pop()
 
 
+def reduce_max(x, dist=None, device="cpu"):
+    """The maximum of x over all ranks (x itself without a process group)."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ms_max, steps, world):
+    """Whole-job iterations/s of `world` replicas that each ran `steps`
+    steps, the slowest in ms_max milliseconds."""
+    return world * steps / (ms_max / 1e3)
+
+
 # ------------------------------------------------------------ learned setup
 LEARNED_THETAS = (1.2, 1.1, 1.0, 0.9, 0.8, 0.7, 0.6)
 LEARNED_SPREAD = 1.0
@@ -453,12 +469,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if not dist:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, f"cuda:{local}")
 
     model, linfo, plain_line = None, None, None
     if learned:
@@ -492,7 +503,7 @@ def main():
     barrier()
     clocks = sampler.stop()
     ms = max_over_ranks(ms)
-    value = world * args.steps / (ms / 1e3)
+    value = replica_value(ms, args.steps, world)
 
     # e2e: host buffers through gvizCudaForceStepHost
     import torch
