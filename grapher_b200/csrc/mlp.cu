@@ -16,6 +16,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "mlp.cuh"
@@ -386,7 +387,7 @@ struct HarvestArgs {
   const double2 *pos;
   const double *mass, *radius;
   float *feat, *tgt, *fmono;
-  uint32_t *vert, *count;
+  uint32_t *vert, *cell, *count;
   uint32_t n, cap, maxNodes;
   double kk, overlapC;
   int model;
@@ -461,14 +462,17 @@ __global__ __launch_bounds__(128) void k_far_harvest(HarvestArgs a) {
       const double fm = sqrt(mx * mx + my * my);
       float f[MLP_IN], e1x, e1y;
       far_features(dx, dy, d2, c, (float)rv, f, e1x, e1y);
-      const uint32_t slot = atomicAdd(a.count, 1u);
-      if (slot < a.cap && fm > 0.0) {
+      // a pair whose monopole vanishes (FR's pseudo-body mass below one
+      // truncates to zero) has no relative correction: not a sample
+      const uint32_t slot = fm > 0.0 ? atomicAdd(a.count, 1u) : 0xffffffffu;
+      if (slot < a.cap) {
         for (int k = 0; k < MLP_IN; k++) a.feat[(size_t)slot * MLP_IN + k] = f[k];
         const double ex = fx - mx, ey = fy - my;
         a.tgt[(size_t)slot * 2] = (float)((ex * e1x + ey * e1y) / fm);
         a.tgt[(size_t)slot * 2 + 1] = (float)((-ex * e1y + ey * e1x) / fm);
         a.fmono[slot] = (float)fm;
         a.vert[slot] = v;
+        a.cell[slot] = cur;
       }
     }
     cur = next;
@@ -772,13 +776,13 @@ int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
   enqueue_tree_build(h);
   h->farSide = savedSide;
   h->params = saved;
-  uint32_t *dT = nullptr, *dCount = nullptr, *dV = nullptr;
+  uint32_t *dT = nullptr, *dCount = nullptr, *dV = nullptr, *dC = nullptr;
   float *dF = nullptr, *dG = nullptr, *dM = nullptr;
   const size_t c = cap ? cap : 1;
   if (cudaMalloc(&dT, (nTargets ? nTargets : 1) * 4) != cudaSuccess ||
       cudaMalloc(&dCount, 4) != cudaSuccess || cudaMalloc(&dF, c * MLP_IN * 4) != cudaSuccess ||
       cudaMalloc(&dG, c * 8) != cudaSuccess || cudaMalloc(&dM, c * 4) != cudaSuccess ||
-      cudaMalloc(&dV, c * 4) != cudaSuccess) {
+      cudaMalloc(&dV, c * 4) != cudaSuccess || cudaMalloc(&dC, c * 4) != cudaSuccess) {
     rc = GVIZ_CUDA_ERR_ALLOC;
   }
   uint32_t count = 0;
@@ -801,6 +805,7 @@ int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
     a.tgt = dG;
     a.fmono = dM;
     a.vert = dV;
+    a.cell = dC;
     a.count = dCount;
     a.n = (uint32_t)nTargets;
     a.cap = (uint32_t)cap;
@@ -813,13 +818,32 @@ int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
     cudaMemcpyAsync(&count, dCount, 4, cudaMemcpyDeviceToHost, h->stream);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = GVIZ_CUDA_ERR_CUDA;
   }
-  if (!rc) {
-    const size_t w = std::min<size_t>(count, cap);
-    if (features) cudaMemcpy(features, dF, w * MLP_IN * 4, cudaMemcpyDeviceToHost);
-    if (target) cudaMemcpy(target, dG, w * 8, cudaMemcpyDeviceToHost);
-    if (fmono) cudaMemcpy(fmono, dM, w * 4, cudaMemcpyDeviceToHost);
-    if (vertex) cudaMemcpy(vertex, dV, w * 4, cudaMemcpyDeviceToHost);
+  if (!rc && count > 0 && count <= cap) {
+    // the kernel appends in scheduling order; return the pairs in one
+    // canonical order (target vertex, then cell) so that results built on
+    // them (training) do not depend on it
+    const size_t n = count;
+    std::vector<float> F(n * MLP_IN), G(n * 2), M(n);
+    std::vector<uint32_t> Vv(n), Cc(n), perm(n);
+    bool ok = cudaMemcpy(F.data(), dF, n * MLP_IN * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(G.data(), dG, n * 8, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(M.data(), dM, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(Vv.data(), dV, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(Cc.data(), dC, n * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (!ok) rc = GVIZ_CUDA_ERR_CUDA;
+    for (size_t i = 0; i < n; i++) perm[i] = (uint32_t)i;
+    std::sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+      return Vv[x] != Vv[y] ? Vv[x] < Vv[y] : Cc[x] < Cc[y];
+    });
+    for (size_t o = 0; !rc && o < n; o++) {
+      const uint32_t i = perm[o];
+      if (features) memcpy(features + o * MLP_IN, &F[i * MLP_IN], MLP_IN * 4);
+      if (target) memcpy(target + 2 * o, &G[2 * i], 8);
+      if (fmono) fmono[o] = M[i];
+      if (vertex) vertex[o] = Vv[i];
+    }
   }
+  cudaFree(dC);
   cudaFree(dT);
   cudaFree(dCount);
   cudaFree(dF);

@@ -514,23 +514,29 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
   a.bT[b] = T;
   const uint32_t g = a.bGid[b];
   uint32_t x = b | GVIZ_LEAF_BIT;
+  uint32_t p = up_of(a, x)->x;
   for (int guard = 0;; guard++) {
     if (guard > GVIZ_MAX_CLIMB) {
       atomicOr(a.status, GVIZ_ST_TREE);
       return;
     }
-    uint2 *ux = up_of(a, x);
-    const uint32_t p = ux->x;
-    if (p == GVIZ_NONE || a.nDelta[p] < 32) {
+    const int dp = p == GVIZ_NONE ? 0 : a.nDelta[p];
+    if (p == GVIZ_NONE || dp < 32) {
       a.rootNode[g] = x;
       a.rootT[g] = T;
-      *ux = make_uint2(GVIZ_NONE, 0u);
+      *up_of(a, x) = make_uint2(GVIZ_NONE, 0u);
       return;
     }
+    // p's shape comes from the previous kernel: fetch all of it (and the
+    // grandparent's level) before waiting on the arrival
+    const uint32_t l = a.nLeft[p], r = a.nRight[p];
+    const uint32_t first = a.nFirst[p], last = a.nLast[p];
+    const uint32_t pp = a.upInt[p].x;
+    const int dpp = pp == GVIZ_NONE ? 0 : a.nDelta[pp];
     // release this child's sums / acquire the sibling's: the second thread
     // to arrive combines both (Karras node p is one end of its own range,
     // so an in-block node has p in [B0, B1))
-    if (p >= B0 && p < B1 && a.nFirst[p] >= B0 && a.nLast[p] < B1) {
+    if (p >= B0 && p < B1 && first >= B0 && last < B1) {
       cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrivals(sArrive[p - B0]);
       if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
     } else {
@@ -538,7 +544,6 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
       a.nCounter[p] = 0u;
     }
-    const uint32_t l = a.nLeft[p], r = a.nRight[p];
     double Ml, SXl, SYl, Mr, SXr, SYr;
     uint32_t cl, Tl, cr, Tr;
     child_vals(a, l, Ml, SXl, SYl, cl, Tl);
@@ -547,10 +552,7 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
     SX = SXl + SXr;
     SY = SYl + SYr;
     cnt = cl + cr;
-    const int dp = a.nDelta[p];
-    const uint32_t pp = a.upInt[p].x;
-    const bool absorbed = pp != GVIZ_NONE && a.nDelta[pp] >= 32 &&
-                          ((dp - 32) >> 1) == ((a.nDelta[pp] - 32) >> 1);
+    const bool absorbed = pp != GVIZ_NONE && dpp >= 32 && ((dp - 32) >> 1) == ((dpp - 32) >> 1);
     const bool collapsed = !absorbed && cnt <= a.k;
     T = absorbed ? Tl + Tr : (collapsed ? 1u + cnt : 1u + Tl + Tr);
     if (a.nQ) {
@@ -575,6 +577,7 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
     up_of(a, l)->y = base | dead;
     up_of(a, r)->y = (base + Tl) | dead;
     x = p;
+    p = pp;
   }
 }
 

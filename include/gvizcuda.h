@@ -276,7 +276,8 @@ int gvizCudaForceSetFarFieldModel(gvizCudaForce *h, gvizCudaMlp *m);
  * each target vertex and each cell the learned walk accepts, the features
  * (10), the exact relative correction (2, from the cell's points in FP64),
  * the monopole magnitude and the target. Returns the number of pairs found;
- * at most cap are written. */
+ * they are written, ordered by target vertex and then cell, only when cap
+ * holds them all (call again with a larger cap otherwise). */
 int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
                                      size_t nTargets, double theta,
                                      float *features, float *target,

@@ -138,6 +138,19 @@ def test_harvest_targets_follow_quadrupole(trained):
     assert np.all(M > 0)
 
 
+def test_harvest_is_deterministic(trained):
+    """Pairs come back in one canonical order (target vertex, then cell),
+    whatever order the GPU found them in, so training on them is
+    repeatable."""
+    from grapher_b200.farfield import harvest
+    lay, _, targets, _ = trained
+    a = harvest(lay, targets[:256], 1.0)
+    b = harvest(lay, targets[:256], 1.0, cap=7)   # too small: retried inside
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    assert np.all(np.diff(a[3].astype(np.int64)) >= 0)
+
+
 def test_zero_model_is_the_plain_walk(trained):
     """With all weights zero the learned walk adds nothing; below
     theta = 1/sqrt(2) no cell can contain its target, so it visits the same
