@@ -22,6 +22,7 @@
 #include "internal.cuh"
 
 void tree_set_smem_limits();
+void sort_set_smem_limits();
 void enqueue_cell_dump(gvizCudaForce *h, int32_t *depth, uint64_t *hi,
                        uint64_t *lo, double *mass, double *cx, double *cy,
                        uint64_t *cnt);
@@ -615,6 +616,7 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
     return GVIZ_CUDA_ERR_CUDA;
   }
   tree_set_smem_limits();
+  sort_set_smem_limits();
   for (int i = 0; i < 65; i++) cudaEventCreate(&h->profEv[i]);
   // Init leaves the FA2 state zeroed (src/embedders/gvizForceEmbedder.c:221);
   // Begin sets it up.

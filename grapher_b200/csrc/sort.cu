@@ -153,12 +153,21 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_hist(
 
 // Stable scatter: warp w of a tile owns 512 consecutive keys, taken in
 // rounds of 32; __match_any_sync ranks equal digits inside a round.
+// Shared memory of the scatter beyond its static arrays: the tile's keys
+// and values reordered by digit.
+constexpr size_t kScatterDyn = (size_t)kSortTile * (sizeof(uint64_t) + sizeof(uint32_t));
+
 __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
     const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin,
     uint64_t *__restrict__ kout, uint32_t *__restrict__ vout, uint32_t n,
     int shift, const uint32_t *__restrict__ offs, uint32_t numTiles) {
+  extern __shared__ __align__(16) unsigned char dyn[];
+  uint64_t *sk = reinterpret_cast<uint64_t *>(dyn);
+  uint32_t *sv = reinterpret_cast<uint32_t *>(sk + kSortTile);
   __shared__ uint32_t wcnt[kSortWarps][256];
   __shared__ uint32_t base[256];
+  __shared__ uint32_t start[256];  // first in-tile position of each digit
+  __shared__ uint32_t wsum[kSortWarps];
   const unsigned tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
   for (unsigned d = tid; d < kSortWarps * 256; d += kSortThreads)
     (&wcnt[0][0])[d] = 0;
@@ -184,24 +193,48 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
     __syncwarp();
   }
   __syncthreads();
-  {
-    uint32_t run = 0;
+  // per digit (thread tid = digit): warps' offsets, then the tile's digit
+  // starts by a block-wide exclusive scan of the digit totals
+  uint32_t run = 0;
 #pragma unroll
-    for (int ww = 0; ww < kSortWarps; ww++) {
-      uint32_t t = wcnt[ww][tid];
-      wcnt[ww][tid] = run;
-      run += t;
-    }
+  for (int ww = 0; ww < kSortWarps; ww++) {
+    uint32_t t = wcnt[ww][tid];
+    wcnt[ww][tid] = run;
+    run += t;
   }
+  uint32_t incl = run;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (unsigned)o) incl += y;
+  }
+  if (lane == 31) wsum[w] = incl;
   __syncthreads();
+  uint32_t before = 0;
+  for (unsigned ww = 0; ww < w; ww++) before += wsum[ww];
+  start[tid] = before + incl - run;
+  __syncthreads();
+  // the tile reordered by digit in shared memory (stable: warp, round, lane
+  // is input order) ...
 #pragma unroll
   for (int r = 0; r < kSortRounds; r++) {
     uint32_t i = tileBase + r * 32 + lane;
     if (i >= n) continue;
     uint32_t d = (uint32_t)(k[r] >> shift) & 255u;
-    uint32_t dst = base[d] + wcnt[w][d] + rank[r];
-    kout[dst] = k[r];
-    vout[dst] = v[r];
+    const uint32_t pos = start[d] + wcnt[w][d] + rank[r];
+    sk[pos] = k[r];
+    sv[pos] = v[r];
+  }
+  __syncthreads();
+  // ... then written out in order: each digit's run lands contiguously
+  const uint32_t t0 = blockIdx.x * kSortTile;
+  const uint32_t cnt = n - t0 < (uint32_t)kSortTile ? n - t0 : (uint32_t)kSortTile;
+  for (uint32_t j = tid; j < cnt; j += kSortThreads) {
+    const uint64_t kk = sk[j];
+    const uint32_t d = (uint32_t)(kk >> shift) & 255u;
+    const uint32_t dst = base[d] + (j - start[d]);
+    kout[dst] = kk;
+    vout[dst] = sv[j];
   }
 }
 
@@ -239,6 +272,13 @@ void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
 // Stable sort by the key bits above GVIZ_SORT_SKIP_BITS (an even number of
 // 8-bit passes, so the result ends in (keys, vals)); keys equal in those bits
 // keep their input order.
+// The scatter's shared memory exceeds the default per-block budget: opted
+// into once per device, at handle creation (outside any stream capture).
+void sort_set_smem_limits() {
+  cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)kScatterDyn);
+}
+
 void radix_sort_pairs(gvizCudaForce *h, uint64_t *keys, uint32_t *vals,
                       uint64_t *keysAlt, uint32_t *valsAlt, size_t n) {
   if (n <= 1) return;
@@ -250,7 +290,7 @@ void radix_sort_pairs(gvizCudaForce *h, uint64_t *keys, uint32_t *vals,
                                                         h->d_radixHist, tiles);
     scan_exclusive(h, h->d_radixHist, h->d_radixHist, (size_t)256 * tiles,
                    nullptr);
-    k_radix_scatter<<<tiles, kSortThreads, 0, h->stream>>>(
+    k_radix_scatter<<<tiles, kSortThreads, kScatterDyn, h->stream>>>(
         ka, va, kb, vb, (uint32_t)n, shift, h->d_radixHist, tiles);
     uint64_t *tk = ka;
     ka = kb;
