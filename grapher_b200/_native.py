@@ -51,6 +51,7 @@ class ForceParams(C.Structure):
         ("strictReductions", C.c_int32),
         ("farField", C.c_int32),
         ("farGroupSpread", C.c_double),
+        ("farCellGroups", C.c_int32),
     ]
 
 
@@ -122,6 +123,7 @@ _SIGS = {
     "gvizCudaForceRepulsion": (C.c_int, [P, DP]),
     "gvizCudaForceCountInteractions": (C.c_int, [P, U64P, U64P]),
     "gvizCudaForceCountFarRows": (C.c_int, [P, U64P, U64P, U64P]),
+    "gvizCudaForceFarGroups": (C.c_int, [P, U32P, U64P]),
     "gvizCudaForceProfileStep": (C.c_int, [P, SZ, C.POINTER(C.c_char_p), DP]),
     "gvizCudaForceTimeSteps": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_float)]),
     "gvizCudaForceStepKernelCount": (C.c_int, [P]),

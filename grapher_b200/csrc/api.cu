@@ -343,6 +343,7 @@ void gvizCudaForceDefaultParams(gvizCudaForceParams *p) {
   p->strictReductions = 0;
   p->farField = 0;
   p->farGroupSpread = 1.0;
+  p->farCellGroups = 0;
 }
 
 int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
@@ -617,6 +618,7 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   }
   tree_set_smem_limits();
   sort_set_smem_limits();
+  forces_set_smem_limits();
   for (int i = 0; i < 65; i++) cudaEventCreate(&h->profEv[i]);
   // Init leaves the FA2 state zeroed (src/embedders/gvizForceEmbedder.c:221);
   // Begin sets it up.
@@ -660,7 +662,8 @@ int gvizCudaForceSetParams(gvizCudaForce *h, const gvizCudaForceParams *p) {
   // the learned correction lives in the FP32 walk and needs a model
   if (p->farField && (!h->d_mlp || p->precision != GVIZ_CUDA_FP32 || !p->barnesHutEnabled))
     return set_err(h, GVIZ_CUDA_ERR_ARG);
-  if (!(p->farGroupSpread >= 0.0 && p->farGroupSpread <= 1.0))
+  if (!(p->farGroupSpread >= 0.0 && p->farGroupSpread <= 1.0) ||
+      (p->farCellGroups != 0 && p->farCellGroups != 1))
     return set_err(h, GVIZ_CUDA_ERR_ARG);
   DeviceGuard guard(h->device);
   const bool radiusChanged = p->preventOverlap != h->params.preventOverlap ||

@@ -614,6 +614,258 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
                  ky.value() + (double)corry);
 }
 
+// ---------------------------------------------------------------------------
+// The learned cell-group walk. One warp per target group cut from the tree
+// (k_far_groups: a cell of <= 32 points, sibling cells packed), so the 32
+// targets of a warp always lie in one cell and its parent bounds them. The
+// warp walks the tree once for the whole group with warp-uniform decisions:
+//   leaf         - every target takes the pair term (self excluded);
+//   cell         - opened when its preorder range meets the group's, or when
+//                  the opening test fails from the group's bounding box
+//                  (2h/theta against the distance from the box to the
+//                  cell's centre of mass, the nearest any target can be);
+//                  otherwise accepted for every target: each takes its own
+//                  monopole term, and one MLP row with the cell seen from
+//                  the group's centroid corrects them all (p1 F + p2
+//                  rot90(F) with each target's own F).
+// Rows are queued per warp and evaluated in 16-row mma.sync tiles, applied
+// in queue order; a group's forces depend only on the group, so the result
+// does not depend on which warp drew it.
+// ---------------------------------------------------------------------------
+
+// A plain FP32 running sum (the Kahan interface): the cell-group walk's
+// error is set by the far field, thousands of times the rounding of a
+// ~200-term FP32 sum, so it does not pay for compensation.
+struct SumF {
+  float s = 0.f;
+  __device__ __forceinline__ void add(float x) { s += x; }
+  __device__ __forceinline__ double value() const { return (double)s; }
+};
+
+// per warp: the accepted cells of the current tile (preorder index), each
+// lane's monopole force of each of them, and the tile's rows, which are
+// filled at flush time, one row per lane
+struct __align__(16) CellWarpSmem {
+  __nv_bfloat16 gx[kFarTile * MLP_XS];
+  float2 gF[kFarTile][32];
+  uint32_t cell[kFarTile];
+  float2 out[kFarTile];
+  uint32_t tgt[32];
+};
+
+constexpr int kCellThreads = 384;  // one block of 16 warps shares the staged network
+constexpr int kCellBlocksPerSM = 2;
+constexpr size_t kCellDyn = (kCellThreads / 32) * sizeof(CellWarpSmem);
+
+struct CellArgs {
+  FarArgs f;
+  const uint4 *groups;
+  const uint32_t *nGroups;  // [0] groups written, [1] the walk's task counter
+  uint32_t cap;
+};
+
+__device__ __forceinline__ float warp_minf(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fminf(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+__device__ __forceinline__ float warp_maxf(float x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x = fmaxf(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+
+// Evaluates the queued cells: lane r < rows builds row r (cell r seen from
+// the group's centroid), the tile runs on the tensor cores, and every lane
+// adds each row's correction of its own monopole force of that cell.
+__device__ __forceinline__ void cell_flush(const MlpSmem &W, CellWarpSmem &q, int rows,
+                                           const NodeF *__restrict__ nodes,
+                                           const FarCell *__restrict__ cells, float wxh,
+                                           float wxl, float wyh, float wyl, float wrv,
+                                           float &corrx, float &corry) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  if (lane < rows) {
+    const uint32_t cc = q.cell[lane];
+    const float4 n0 = __ldg(reinterpret_cast<const float4 *>(nodes + cc));
+    const float4 c0 = __ldg(reinterpret_cast<const float4 *>(cells + cc));
+    const uint4 c1 = __ldg(reinterpret_cast<const uint4 *>(cells + cc) + 1);
+    FarCell c;
+    c.qa = c0.x;
+    c.qb = c0.y;
+    c.tr = c0.z;
+    c.h = c0.w;
+    c.ox = __uint_as_float(c1.x);
+    c.oy = __uint_as_float(c1.y);
+    c.s0 = c1.z;
+    c.s1 = c1.w;
+    const float wdx = (n0.x - wxh) + (n0.z - wxl);
+    const float wdy = (n0.y - wyh) + (n0.w - wyl);
+    const float wd2 = wdx * wdx + wdy * wdy;
+    float f[MLP_IN], e1x, e1y;
+    far_features(wdx, wdy, wd2, c, wrv, f, e1x, e1y);
+    far_put_row(q.gx + lane * MLP_XS, f);
+  }
+  __syncwarp();
+  mlp_forward_tile<true>(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
+  __syncwarp();
+  for (int r = 0; r < rows; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
+  __syncwarp();
+}
+
+template <int MODEL, bool OVERLAP, bool COUNT>
+__global__ __launch_bounds__(kCellThreads, kCellBlocksPerSM) void k_walk_f32_cells(CellArgs ca) {
+  __shared__ MlpSmem W;
+  extern __shared__ __align__(16) unsigned char cellDyn[];
+  CellWarpSmem *Q = reinterpret_cast<CellWarpSmem *>(cellDyn);  // one per warp
+  mlp_stage(W, ca.f.mlp);
+  const WalkArgs &a = ca.f.w;
+  const FarCell *__restrict__ cells = ca.f.cells;
+  CellWarpSmem &q = Q[threadIdx.x >> 5];
+  const unsigned lane = threadIdx.x & 31u;
+  for (int e = lane; e < kFarTile * MLP_XS / 8; e += 32)
+    reinterpret_cast<uint4 *>(q.gx)[e] = make_uint4(0u, 0u, 0u, 0u);
+  __syncthreads();
+  const uint32_t nGroups = min(ca.nGroups[0], ca.cap);
+  uint32_t *queue = const_cast<uint32_t *>(ca.nGroups) + 1;
+  unsigned long long nInter = 0, nVisit = 0, nRows = 0, nGrp = 0;
+  for (;;) {
+    uint32_t gi = 0;
+    if (lane == 0) gi = atomicAdd(queue, 1u);
+    gi = __shfl_sync(0xffffffffu, gi, 0);
+    if (gi >= nGroups) break;
+    const uint4 G = ca.groups[gi];
+    // the group's targets: the leaves of its preorder range, one per lane
+    uint32_t found = 0;
+    for (uint32_t b = G.x; b < G.y && found < 32u; b += 32u) {
+      const uint32_t j = b + lane;
+      const int32_t info = j < G.y ? __ldg(reinterpret_cast<const int4 *>(a.nodes + j) + 1).w : -1;
+      const uint32_t ball = __ballot_sync(0xffffffffu, info >= 0);
+      const uint32_t r = found + __popc(ball & ((1u << lane) - 1u));
+      if (info >= 0 && r < 32u) q.tgt[r] = (uint32_t)info;
+      found += __popc(ball);
+    }
+    __syncwarp();
+    const uint32_t nT = min(found, 32u);
+    const bool has = lane < nT;
+    const uint32_t v = has ? q.tgt[lane] : 0u;
+    __syncwarp();
+    if (nT == 0) continue;
+    const uint32_t v0 = __shfl_sync(0xffffffffu, v, 0);
+    const uint32_t g = a.gid ? a.gid[v0] : 0u;
+    if (a.active && a.active[g] == 0u) continue;
+    const uint32_t root = a.graphBase[g];
+    const uint32_t end = min(root + a.rootT[g], a.maxNodes);
+    float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
+    double2 pv = make_double2(0.0, 0.0);
+    if (has) {
+      pv = a.pos[v];
+      ds_split(pv.x, vxh, vxl);
+      ds_split(pv.y, vyh, vyl);
+      mv = a.massF[v];
+      if (OVERLAP) rv = a.radiusF[v];
+    }
+    float wxh, wxl, wyh, wyl, wr2, wrv;
+    group_centroid<32, OVERLAP>(has, pv, vxh, vxl, vyh, vyl, rv, wxh, wxl, wyh, wyl, wr2, wrv);
+    const float bx0 = warp_minf(has ? vxh : INFINITY), bx1 = warp_maxf(has ? vxh : -INFINITY);
+    const float by0 = warp_minf(has ? vyh : INFINITY), by1 = warp_maxf(has ? vyh : -INFINITY);
+    SumF kx, ky;
+    float corrx = 0.f, corry = 0.f;
+    int qg = 0;
+    const unsigned long long visit0 = nVisit;
+    if (COUNT) nGrp++;
+    for (uint32_t cur = root; cur < end;) {
+      const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
+      const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+      const float nmass = n1.x, nsize = n1.y;
+      const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
+      const uint32_t skip = max((uint32_t)nnext, cur + 1u);
+      if (COUNT) nVisit++;
+      if (nmass == 0.0f) {  // empty: skipped as the reference does
+        cur = skip;
+        continue;
+      }
+      const float dx = (n0.x - vxh) + (n0.z - vxl);
+      const float dy = (n0.y - vyh) + (n0.w - vyl);
+      const float d2 = dx * dx + dy * dy;
+      if (ninfo >= 0) {  // a point: pair term for every other target
+        const bool doForce = has && (uint32_t)ninfo != v;
+        float fx = 0.f, fy = 0.f;
+        if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {
+          if (doForce) {
+            rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + nsize, a.num, a.overlapC, v,
+                                     (uint32_t)ninfo, fx, fy);
+            kx.add(fx);
+            ky.add(fy);
+          }
+        } else if (doForce) {
+          rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + nsize, a.num, a.overlapC,
+                                         fx, fy);
+          kx.add(fx);
+          ky.add(fy);
+        }
+        if (COUNT && doForce) nInter++;
+        cur = cur + 1u;
+        continue;
+      }
+      bool accept = false;
+      if (!(cur < G.y && skip > G.x)) {  // outside the group
+        const float ex = fmaxf(fmaxf(bx0 - n0.x, n0.x - bx1), 0.0f);
+        const float ey = fmaxf(fmaxf(by0 - n0.y, n0.y - by1), 0.0f);
+        accept = nsize < ex * ex + ey * ey;
+      }
+      if (!accept) {
+        cur = cur + 1u;
+        continue;
+      }
+      float fx = 0.f, fy = 0.f;
+      if (__any_sync(0xffffffffu, has && !(d2 > 0.0f))) {
+        if (has) rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv, a.num, a.overlapC, v, v, fx, fy);
+      } else if (has) {
+        rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv, a.num, a.overlapC, fx, fy);
+      }
+      if (has) {
+        kx.add(fx);
+        ky.add(fy);
+      }
+      if (COUNT && has) nInter++;
+      q.gF[qg][lane] = make_float2(fx, fy);  // zero for lanes without a target
+      if (lane == 0) q.cell[qg] = cur;
+      if (COUNT) nRows++;
+      if (++qg == kFarTile) {
+        cell_flush(W, q, kFarTile, a.nodes, cells, wxh, wxl, wyh, wyl, OVERLAP ? wrv : 0.f,
+                   corrx, corry);
+        qg = 0;
+      }
+      cur = skip;
+    }
+    if (qg > 0)
+      cell_flush(W, q, qg, a.nodes, cells, wxh, wxl, wyh, wyl, OVERLAP ? wrv : 0.f, corrx,
+                 corry);
+    if (COUNT && lane == 0) {  // the longest group walk and its group
+      const unsigned long long len = nVisit - visit0;
+      const float ext = fmaxf(bx1 - bx0, by1 - by0);
+      if (atomicMax(a.counters + 4, len) < len) {
+        atomicExch(a.counters + 5, ((unsigned long long)nT << 32) | __float_as_uint(ext));
+      }
+      atomicAdd(a.counters + 6, (unsigned long long)nT);
+    }
+    if (has) {
+      const float2 at = a.attF[v];
+      force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value() + (double)corrx,
+                     ky.value() + (double)corry);
+    }
+  }
+  if (COUNT) {
+    atomicAdd(a.counters, nInter);
+    if (lane == 0) {
+      atomicAdd(a.counters + 1, nVisit);
+      atomicAdd(a.counters + 2, nRows);
+      atomicAdd(a.counters + 7, nGrp);
+    }
+  }
+}
+
 struct ExactArgs {
   const double2 *pos;
   const float *massF, *radiusF;
@@ -772,7 +1024,49 @@ static void launch_far(gvizCudaForce *h, const FarArgs &fa, bool count) {
   else k_walk_f32_far<MODEL, OVERLAP, false><<<grid, kFarThreads, 0, h->stream>>>(fa);
 }
 
-// The learned walk (see k_walk_f32_far).
+template <int MODEL, bool OVERLAP>
+static void launch_cells(gvizCudaForce *h, const CellArgs &ca, bool count) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (count)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_walk_f32_cells<MODEL, OVERLAP, true>,
+                                                  kCellThreads, kCellDyn);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_walk_f32_cells<MODEL, OVERLAP, false>,
+                                                  kCellThreads, kCellDyn);
+  const uint32_t resident = (uint32_t)((per > 0 ? per : 1) * (sms > 0 ? sms : 1));
+  const uint32_t need = blocks(((h->V + 31) / 32) * 32, kCellThreads);
+  const uint32_t grid = need < resident ? need : resident;
+  cudaMemsetAsync(h->d_groupCount + 1, 0, sizeof(uint32_t), h->stream);
+  if (count)
+    k_walk_f32_cells<MODEL, OVERLAP, true><<<grid, kCellThreads, kCellDyn, h->stream>>>(ca);
+  else
+    k_walk_f32_cells<MODEL, OVERLAP, false><<<grid, kCellThreads, kCellDyn, h->stream>>>(ca);
+}
+
+// The cell-group walk's per-warp queues exceed the default dynamic shared
+// memory of a block; opted in once per process for every instance.
+void forces_set_smem_limits() {
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_FR, false, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_FR, false, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_FR, true, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_FR, true, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_LINLOG, false, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_LINLOG, false, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_LINLOG, true, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+  cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_LINLOG, true, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
+}
+
+// The learned walk (see k_walk_f32_far and k_walk_f32_cells).
 static void enqueue_far(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters) {
   FarArgs fa;
   fa.w = a;
@@ -782,6 +1076,22 @@ static void enqueue_far(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters)
   fa.spread2 = (float)(h->params.farGroupSpread * h->params.farGroupSpread);
   const bool ov = h->params.preventOverlap != 0;
   const bool count = counters != nullptr;
+  if (h->params.farCellGroups) {
+    CellArgs ca;
+    ca.f = fa;
+    ca.groups = h->d_groups;
+    ca.nGroups = h->d_groupCount;
+    ca.cap = (uint32_t)(h->V ? h->V : 1);
+    if (h->model == GVIZ_CUDA_MODEL_FR) {
+      if (ov) launch_cells<GVIZ_CUDA_MODEL_FR, true>(h, ca, count);
+      else launch_cells<GVIZ_CUDA_MODEL_FR, false>(h, ca, count);
+    } else {
+      if (ov) launch_cells<GVIZ_CUDA_MODEL_LINLOG, true>(h, ca, count);
+      else launch_cells<GVIZ_CUDA_MODEL_LINLOG, false>(h, ca, count);
+    }
+    prof_mark(h, "bh_walk_f32_learned");
+    return;
+  }
   if (h->model == GVIZ_CUDA_MODEL_FR) {
     if (ov) launch_far<GVIZ_CUDA_MODEL_FR, true>(h, fa, count);
     else launch_far<GVIZ_CUDA_MODEL_FR, false>(h, fa, count);

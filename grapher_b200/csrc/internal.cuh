@@ -183,6 +183,9 @@ struct gvizCudaForce {
   double4 *d_bQ = nullptr, *d_nQ = nullptr;
   FarCell *d_cells = nullptr;       // maxNodes records
   uint32_t *d_leafPre = nullptr;    // per vertex: preorder index of its leaf
+  uint32_t *d_cellCnt = nullptr;    // per cell node: points below it
+  uint4 *d_groups = nullptr;        // target groups: preorder [x, y), z points
+  uint32_t *d_groupCount = nullptr; // [0] groups written, [1] walk queue
 
   // --- CUDA graph of one step ---
   cudaGraphExec_t stepExec = nullptr;
@@ -261,6 +264,7 @@ size_t scan_scratch_entries(size_t n);
 // tree.cu
 void enqueue_tree_build(gvizCudaForce *h);
 void enqueue_tree_export(gvizCudaForce *h, int32_t *leafDepth);
+void enqueue_group_export(gvizCudaForce *h, uint32_t *groupOf);
 
 // mlp.cu
 void mlp_free(gvizCudaForce *h);
@@ -273,6 +277,7 @@ int dir_table_upload_precise(const double *t);
 void enqueue_attraction_f32(gvizCudaForce *h);
 void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters);
 uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads);
+void forces_set_smem_limits();
 void enqueue_exact_f32(gvizCudaForce *h);
 
 // precise.cu (FP64 + FA2, compiled without fused multiply-add)

@@ -493,7 +493,10 @@ int far_side_alloc(gvizCudaForce *h) {
   if (cudaMalloc(&h->d_bQ, Vs * sizeof(double4)) != cudaSuccess ||
       cudaMalloc(&h->d_nQ, Vs * sizeof(double4)) != cudaSuccess ||
       cudaMalloc(&h->d_cells, h->maxNodes * sizeof(FarCell)) != cudaSuccess ||
-      cudaMalloc(&h->d_leafPre, Vs * sizeof(uint32_t)) != cudaSuccess)
+      cudaMalloc(&h->d_leafPre, Vs * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&h->d_cellCnt, h->maxNodes * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&h->d_groups, Vs * sizeof(uint4)) != cudaSuccess ||
+      cudaMalloc(&h->d_groupCount, 2 * sizeof(uint32_t)) != cudaSuccess)
     return GVIZ_CUDA_ERR_ALLOC;
   return GVIZ_CUDA_OK;
 }
@@ -503,9 +506,15 @@ void far_side_free(gvizCudaForce *h) {
   cudaFree(h->d_nQ);
   cudaFree(h->d_cells);
   cudaFree(h->d_leafPre);
+  cudaFree(h->d_cellCnt);
+  cudaFree(h->d_groups);
+  cudaFree(h->d_groupCount);
   h->d_bQ = h->d_nQ = nullptr;
   h->d_cells = nullptr;
   h->d_leafPre = nullptr;
+  h->d_cellCnt = nullptr;
+  h->d_groups = nullptr;
+  h->d_groupCount = nullptr;
 }
 
 // ---------------------------------------------------------------------------
@@ -751,6 +760,38 @@ int gvizCudaForceSetFarFieldModel(gvizCudaForce *h, gvizCudaMlp *m) {
     return GVIZ_CUDA_ERR_CUDA;
   int rc = far_side_alloc(h);
   h->graphDirty = true;
+  return rc;
+}
+
+// The target groups of the learned cell-group walk on the current positions
+// (built as a step builds them): per vertex the index of its group.
+int gvizCudaForceFarGroups(gvizCudaForce *h, uint32_t *groupOf, uint64_t *groupCount) {
+  if (!h || (h->V && !groupOf) || !groupCount) return GVIZ_CUDA_ERR_ARG;
+  cudaSetDevice(h->device);
+  *groupCount = 0;
+  if (!h->V) return GVIZ_CUDA_OK;
+  int rc = far_side_alloc(h);
+  if (rc) return rc;
+  const gvizCudaForceParams saved = h->params;
+  h->params.precision = GVIZ_CUDA_FP32;
+  h->params.farCellGroups = 1;
+  const bool savedSide = h->farSide;
+  h->farSide = true;
+  cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+  enqueue_tree_build(h);
+  h->farSide = savedSide;
+  h->params = saved;
+  uint32_t *dOut = nullptr, count = 0, status = 0;
+  if (cudaMalloc(&dOut, h->V * 4) != cudaSuccess) return GVIZ_CUDA_ERR_ALLOC;
+  cudaMemsetAsync(dOut, 0xff, h->V * 4, h->stream);
+  enqueue_group_export(h, dOut);
+  cudaMemcpyAsync(groupOf, dOut, h->V * 4, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(&count, h->d_groupCount, 4, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(&status, h->d_status, 4, cudaMemcpyDeviceToHost, h->stream);
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) rc = GVIZ_CUDA_ERR_CUDA;
+  cudaFree(dOut);
+  if (!rc && status) rc = GVIZ_CUDA_ERR_LIMIT;
+  *groupCount = count;
   return rc;
 }
 

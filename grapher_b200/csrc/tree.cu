@@ -616,7 +616,12 @@ struct EM {
   const uint64_t *bHi, *bLo;
   FarCell *cells;
   uint32_t *leafPre;
+  uint32_t *cellCnt;  // per cell: points below it (null unless requested)
 };
+
+__device__ __forceinline__ void put_count(const EM &a, uint32_t at, uint32_t c) {
+  if (a.cellCnt && at < a.maxNodes) a.cellCnt[at] = c;
+}
 
 // Geometric centre of the cell at `depth` on the path (hi, lo): the same
 // FP64 descent as k_keys (centres c +/- halfSize/2).
@@ -753,6 +758,7 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
       const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
       put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], INFINITY,
                pre + a.nT[p]);
+      put_count(a, pre, s1 - s0);
       uint32_t ids[GVIZ_MAX_NODES_PER_CELL];
       uint32_t c = s1 - s0;
       for (uint32_t j = 0; j < c; j++) {
@@ -772,8 +778,11 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
              pre + a.nT[p]);
     if (a.cells) {
       const uint32_t lb = a.nLast[p];
+      const uint32_t s0 = a.bStart[fb];
+      const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
       put_far(a, pre, R, fb, q, ldexp(R.h0, -q), a.nQ[p], a.nM[p], a.nSX[p],
-              a.nSY[p], a.bStart[fb], (lb + 1 < U) ? a.bStart[lb + 1] : a.V);
+              a.nSY[p], s0, s1);
+      put_count(a, pre, s1 - s0);
     }
     return;
   }
@@ -796,10 +805,144 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
   const bool testable = c > a.k && qp < R.D - 1;
   const double h = testable ? ldexp(R.h0, -(R.D - 1)) : (double)INFINITY;
   put_cell(a, pre, a.bM[b], a.bSX[b], a.bSY[b], h, pre + 1 + c);
+  put_count(a, pre, c);
   if (a.cells && testable)
     put_far(a, pre, R, b, R.D - 1, h, a.bQ[b], a.bM[b], a.bSX[b], a.bSY[b], s0,
             s0 + c);
   for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, a.idx[s0 + j]);
+}
+
+// Target groups of the learned cell-group walk: every cell of at most
+// kGroupMax points whose parent holds more (or a root of at most kGroupMax
+// points) is one group. Consecutive such children of one parent are packed
+// into one group while the sum stays <= kGroupMax and the rectangle of
+// their quadrants holds no other child of the parent (NW+NE, SW+SE, NW+SW
+// with NE empty, ...), so a group's bounding box never covers points that
+// are not its own; a group is a preorder range [x, y). A cell of more than
+// four children is a leaf bucket (all its points in one smallest cell): its
+// points are cut into runs of kGroupMax. Thread t < total handles the
+// children of node t; thread maxNodes + g the root of graph g. The order of
+// the groups in the list does not matter: a group's forces depend only on
+// the group.
+constexpr uint32_t kGroupMax = 32;
+
+struct GroupArgs {
+  const NodeF *nodes;
+  const FarCell *cells;
+  const uint32_t *cellCnt, *counts, *graphBase, *rootT;
+  uint4 *groups;
+  uint32_t *nGroups;
+  uint32_t maxNodes, G, cap;
+};
+
+__device__ __forceinline__ int4 node_link(const NodeF *nodes, uint32_t j) {
+  return __ldg(reinterpret_cast<const int4 *>(nodes + j) + 1);  // mass, size, next, info
+}
+
+__device__ __forceinline__ void push_group(const GroupArgs &a, uint32_t x, uint32_t y,
+                                           uint32_t c) {
+  const uint32_t slot = atomicAdd(a.nGroups, 1u);
+  if (slot < a.cap) a.groups[slot] = make_uint4(x, y, c, 0u);
+}
+
+// quadrant (NW 0, NE 1, SW 2, SE 3) of the point set of node j inside a
+// cell centred at (cx, cy), from its centre of mass
+__device__ __forceinline__ uint32_t child_quadrant(const NodeF *nodes, uint32_t j, double cx,
+                                                   double cy) {
+  const NodeF n = nodes[j];
+  const double x = (double)n.xh + (double)n.xl, y = (double)n.yh + (double)n.yl;
+  return (x >= cx ? 1u : 0u) | (y < cy ? 2u : 0u);
+}
+
+__global__ __launch_bounds__(kThreads) void k_far_groups(GroupArgs a) {
+  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t total = min(a.counts[3], a.maxNodes);
+  if (t >= a.maxNodes) {
+    const uint32_t g = t - a.maxNodes;
+    if (g >= a.G) return;
+    const uint32_t r = a.graphBase[g], T = a.rootT[g];
+    if (T == 0 || r >= total) return;
+    const int4 l = node_link(a.nodes, r);
+    const uint32_t c = l.w >= 0 ? 1u : a.cellCnt[r];
+    if (c <= kGroupMax) push_group(a, r, min(r + T, total), c);
+    return;
+  }
+  if (t >= total) return;
+  const int4 l = node_link(a.nodes, t);
+  if (l.w >= 0 || a.cellCnt[t] <= kGroupMax) return;  // a leaf, or a group's own cell
+  const uint32_t end = min(max((uint32_t)l.z, t + 1u), total);
+  // the children: at most four for a branching cell
+  uint32_t chX[4], chY[4], chC[4], chQ[4];
+  int nc = 0;
+  bool bucket = false;
+  for (uint32_t ch = t + 1u; ch < end;) {
+    const int4 m = node_link(a.nodes, ch);
+    const bool leaf = m.w >= 0;
+    const uint32_t sib = min(leaf ? ch + 1u : max((uint32_t)m.z, ch + 1u), end);
+    if (nc == 4) {
+      bucket = true;
+      break;
+    }
+    chX[nc] = ch;
+    chY[nc] = sib;
+    chC[nc] = leaf ? 1u : a.cellCnt[ch];
+    nc++;
+    ch = sib;
+  }
+  if (bucket) {  // points of one smallest cell: runs of kGroupMax leaves
+    for (uint32_t x = t + 1u; x < end; x += kGroupMax) {
+      const uint32_t y = min(x + kGroupMax, end);
+      push_group(a, x, y, y - x);
+    }
+    return;
+  }
+  const NodeF pn = a.nodes[t];
+  const FarCell pc = a.cells[t];
+  const double cx = (double)pn.xh + (double)pn.xl + (double)pc.ox * (double)pc.h;
+  const double cy = (double)pn.yh + (double)pn.yl + (double)pc.oy * (double)pc.h;
+  for (int i = 0; i < nc; i++) chQ[i] = child_quadrant(a.nodes, chX[i], cx, cy);
+  int first = -1;
+  uint32_t pcnt = 0, r0 = 0, r1 = 0, c0 = 0, c1 = 0;  // pack, its quadrant rectangle
+  for (int i = 0; i <= nc; i++) {
+    bool fits = false;
+    if (i < nc && chC[i] <= kGroupMax && first >= 0 && pcnt + chC[i] <= kGroupMax) {
+      const uint32_t R0 = min(r0, chQ[i] >> 1), R1 = max(r1, chQ[i] >> 1);
+      const uint32_t C0 = min(c0, chQ[i] & 1u), C1 = max(c1, chQ[i] & 1u);
+      fits = true;
+      for (int k = 0; k < nc; k++) {
+        if (k >= first && k <= i) continue;
+        const uint32_t r = chQ[k] >> 1, c = chQ[k] & 1u;
+        if (r >= R0 && r <= R1 && c >= C0 && c <= C1) fits = false;
+      }
+      if (fits) {
+        r0 = R0, r1 = R1, c0 = C0, c1 = C1;
+        pcnt += chC[i];
+        continue;
+      }
+    }
+    if (first >= 0) push_group(a, chX[first], chY[i - 1], pcnt);
+    first = -1;
+    if (i < nc && chC[i] <= kGroupMax) {  // a larger child is cut by its own thread
+      first = i;
+      pcnt = chC[i];
+      r0 = r1 = chQ[i] >> 1;
+      c0 = c1 = chQ[i] & 1u;
+    }
+  }
+}
+
+// Inspection: per vertex, the index of its target group.
+__global__ __launch_bounds__(kThreads) void k_group_members(const NodeF *nodes,
+                                                            const uint4 *groups,
+                                                            const uint32_t *nGroups,
+                                                            uint32_t cap, uint32_t *groupOf) {
+  const uint32_t gi = blockIdx.x * kThreads + threadIdx.x;
+  if (gi >= min(*nGroups, cap)) return;
+  const uint4 G = groups[gi];
+  for (uint32_t j = G.x; j < G.y; j++) {
+    const int4 l = node_link(nodes, j);
+    if (l.w >= 0) groupOf[l.w] = gi;
+  }
 }
 
 // Inspection: per point, the depth of the reference leaf holding it.
@@ -871,6 +1014,7 @@ EM make_em(gvizCudaForce *h) {
   a.bLo = h->d_bLo;
   a.cells = h->farSide ? h->d_cells : nullptr;
   a.leafPre = h->farSide ? h->d_leafPre : nullptr;
+  a.cellCnt = (h->farSide && h->params.farCellGroups) ? h->d_cellCnt : nullptr;
   return a;
 }
 
@@ -959,6 +1103,22 @@ void enqueue_tree_build(gvizCudaForce *h) {
   scan_exclusive(h, h->d_rootT, h->d_graphBase, h->G, h->d_counts + 3);
   EM em = make_em(h);
   k_emit<<<blocks_for(2 * (size_t)V), kThreads, 0, st>>>(em);
+  if (em.cellCnt && !em.f64) {
+    GroupArgs ga;
+    ga.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
+    ga.cells = h->d_cells;
+    ga.cellCnt = h->d_cellCnt;
+    ga.counts = h->d_counts;
+    ga.graphBase = h->d_graphBase;
+    ga.rootT = h->d_rootT;
+    ga.groups = h->d_groups;
+    ga.nGroups = h->d_groupCount;
+    ga.maxNodes = (uint32_t)h->maxNodes;
+    ga.G = (uint32_t)h->G;
+    ga.cap = (uint32_t)(V ? V : 1);
+    cudaMemsetAsync(h->d_groupCount, 0, sizeof(uint32_t), st);
+    k_far_groups<<<blocks_for((size_t)h->maxNodes + h->G), kThreads, 0, st>>>(ga);
+  }
   prof_mark(h, "tree_nodes");
 }
 
@@ -966,6 +1126,12 @@ void enqueue_tree_export(gvizCudaForce *h, int32_t *leafDepth) {
   EM em = make_em(h);
   k_leaf_depth<<<blocks_for(2 * h->V), kThreads, 0, h->stream>>>(em,
                                                                  leafDepth);
+}
+
+void enqueue_group_export(gvizCudaForce *h, uint32_t *groupOf) {
+  const uint32_t cap = (uint32_t)(h->V ? h->V : 1);
+  k_group_members<<<blocks_for(cap), kThreads, 0, h->stream>>>(
+      reinterpret_cast<const NodeF *>(h->d_nodes), h->d_groups, h->d_groupCount, cap, groupOf);
 }
 
 void tree_set_smem_limits() {

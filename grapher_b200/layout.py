@@ -335,6 +335,15 @@ class ForceLayout:
             return a.value, b.value, [int(x) for x in why]
         return a.value, b.value
 
+    def far_groups(self):
+        """The target groups of the learned cell-group walk on the current
+        positions: (per-vertex group index, number of groups)."""
+        out = np.zeros(self.V, np.uint32)
+        n = C.c_uint64()
+        N.check(self.L.gvizCudaForceFarGroups(self.h, N.ptr(out, C.c_uint32), C.byref(n)),
+                "gvizCudaForceFarGroups")
+        return out, n.value
+
     def profile_step(self):
         names = (C.c_char_p * 64)()
         ms = np.zeros(64)

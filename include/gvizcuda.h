@@ -95,6 +95,16 @@ typedef struct gvizCudaForceParams {
                                fraction of their mean distance to it from
                                their centroid, one model evaluation at the
                                centroid serves them all; 0: one per target */
+  int32_t farCellGroups;    /* learned correction: 1 walks the tree once per
+                               group of at most 32 targets cut from the tree
+                               itself (a cell of <= 32 points whose parent
+                               holds more, sibling groups packed together);
+                               a cell is accepted for the whole group when
+                               it passes the opening test from the group's
+                               bounding box and lies outside the group, and
+                               one model evaluation at the group's centroid
+                               corrects every target's monopole force;
+                               0: the per-target walk above */
 } gvizCudaForceParams;
 
 /* One step's entries of the five stat series the embedder appends
@@ -283,6 +293,12 @@ int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
                                      float *features, float *target,
                                      float *fmono, uint32_t *vertex,
                                      size_t cap);
+
+/* Inspection: the target groups of the learned cell-group walk
+ * (params.farCellGroups) built on the current positions as a step builds
+ * them: groupOf[V] receives each vertex's group index in [0, *groupCount).
+ * The numbering of the groups is not defined; the partition is. */
+int gvizCudaForceFarGroups(gvizCudaForce *h, uint32_t *groupOf, uint64_t *groupCount);
 
 /* ---- allocation-free speed update ------------------------------------- */
 

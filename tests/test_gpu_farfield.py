@@ -218,6 +218,83 @@ def test_learned_steps_and_graph_replay(trained):
     assert np.array_equal(outs[0], outs[1])
 
 
+# ------------------------------------------------------- cell-group walk
+def test_cell_groups_partition_the_vertices(trained):
+    """Every vertex is in exactly one group of 1..32 targets, and no vertex
+    of another group lies strictly inside a group's bounding box: a group
+    is a cell of the tree, or sibling cells whose quadrant rectangle holds
+    no other sibling."""
+    lay, _, _, _ = trained
+    gof, n = lay.far_groups()
+    assert n > 0 and np.all(gof < n)
+    sizes = np.bincount(gof, minlength=n)
+    assert sizes.min() >= 1 and sizes.max() <= 32
+    assert sizes.sum() == lay.V
+    x = lay.positions().reshape(-1, 2)
+    lo = np.full((n, 2), np.inf)
+    hi = np.full((n, 2), -np.inf)
+    np.minimum.at(lo, gof, x)
+    np.maximum.at(hi, gof, x)
+    bad = 0
+    for s0 in range(0, lay.V, 2048):
+        p = x[s0:s0 + 2048, None, :]
+        inside = np.all((p > lo[None]) & (p < hi[None]), axis=2)
+        inside[np.arange(inside.shape[0]), gof[s0:s0 + 2048]] = False
+        bad += int(inside.sum())
+    assert bad == 0
+
+
+def test_cell_group_walk_is_exact_without_acceptance(trained):
+    """With a zero model and theta so small that no cell is accepted, each
+    target sums the pair terms of every other vertex: the exact repulsion
+    up to the rounding of plain FP32 sums of 32K terms, so every node is
+    reached from every group."""
+    lay, _, targets, exact = trained
+    z = _model(1)
+    z.set_weights(np.zeros(z.nparams, np.float32))
+    z.attach(lay)
+    lay.set_params(theta=1e-4, farField=1, farCellGroups=1)
+    e = _nrms(lay, targets, exact)
+    lay.set_params(theta=1.0, farField=0, farCellGroups=0)
+    assert e < 2e-4, e
+
+
+def test_cell_group_correction_beats_monopole(trained):
+    """The trained network's gain in the cell-group walk at theta = 1.0:
+    well below the same walk with the monopole alone, and below the plain
+    walk at the same theta."""
+    lay, m, targets, exact = trained
+    z = _model(1)
+    z.set_weights(np.zeros(z.nparams, np.float32))
+    z.attach(lay)
+    lay.set_params(theta=1.0, farField=1, farCellGroups=1)
+    e_mono = _nrms(lay, targets, exact)
+    m.attach(lay)
+    e_mlp = _nrms(lay, targets, exact)
+    g, _, why = lay.count_far_rows(causes=True)
+    lay.set_params(farField=0, farCellGroups=0)
+    e_plain = _nrms(lay, targets, exact)
+    assert e_mlp < 0.6 * e_mono, (e_mlp, e_mono)
+    assert e_mlp < 0.6 * e_plain, (e_mlp, e_plain)
+    assert g > 0 and why[2] == lay.V   # one row per accepted cell; every target walked
+
+
+def test_cell_group_steps_are_deterministic(trained):
+    """Steps of the cell-group walk run in the captured step graph and do
+    not depend on which warp drew which group."""
+    _, m, _, _ = trained
+    outs = []
+    for _ in range(2):
+        lay = _ba_layout(V=8192, steps=3)
+        m.attach(lay)
+        lay.set_params(theta=1.0, farField=1, farCellGroups=1)
+        for _ in range(5):
+            lay.step()
+        outs.append(lay.positions())
+    assert np.all(np.isfinite(outs[0]))
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_far_field_argument_checks(trained):
     from grapher_b200._native import GvizCudaError
     lay = _ba_layout(V=512, steps=1)
@@ -231,3 +308,6 @@ def test_far_field_argument_checks(trained):
     lay.set_params(farField=0, precision=0)
     with pytest.raises(GvizCudaError):
         lay.set_params(farField=1, farGroupSpread=-1.0)
+    lay.set_params(farField=0, farGroupSpread=1.0)
+    with pytest.raises(GvizCudaError):
+        lay.set_params(farCellGroups=2)
