@@ -11,10 +11,12 @@ trained on the GPU from pairs harvested at theta = 1.2, 0.9 and 0.6 on three
 snapshots of this layout (untimed setup, reported as train_s). Force error is the
 normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
 65,536 sampled vertices, all configurations judged on the same positions.
-The plain walk runs at theta = 0.5; the learned walk at the largest theta of
-1.2, 1.1, ..., 0.6 whose error is not above the plain walk's. ``value`` is
-the learned path's iterations/s; the plain path's are in ``plain``. Both are
-timed from the same saved layout state.
+The plain walk runs at theta = 0.5; the learned walk (the cell-group walk:
+one warp per group of <= 32 targets cut from the tree, one network row per
+accepted cell) at the largest theta of 1.3, 1.25, ..., 0.6 whose error is
+not above the plain walk's. ``value`` is the learned path's iterations/s;
+the plain path's are in ``plain``. Both are timed from the same saved
+layout state.
 rmat4m_learned: the same comparison on an R-MAT graph, scale 22 (4,194,304
 vertices), 33,554,432 edge draws with (a,b,c,d) = (.57,.19,.19,.05),
 deduplicated, no self-loops, start uniform in [-1000, 1000]^2; adds the
@@ -339,8 +341,9 @@ def replica_value(ms_max, steps, world):
 
 
 # ------------------------------------------------------------ learned setup
-LEARNED_THETAS = (1.2, 1.1, 1.0, 0.9, 0.8, 0.7, 0.6)
+LEARNED_THETAS = tuple(round(1.3 - 0.05 * i, 2) for i in range(15))  # 1.3 ... 0.6
 LEARNED_SPREAD = 1.0
+LEARNED_CELL_GROUPS = 1  # the cell-group walk: one warp per tree-cut group of <= 32 targets
 JUDGE_VERTICES = 65536
 
 
@@ -381,14 +384,15 @@ def learned_setup(lay, w):
     table = {}
     chosen = None
     for th in LEARNED_THETAS:
-        lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD)
+        lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD,
+                       farCellGroups=LEARNED_CELL_GROUPS)
         e, e_pv = force_error(lay, targets, exact)
         table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
         if chosen is None and e <= e_plain:
             chosen = th
     if chosen is None:
         chosen = LEARNED_THETAS[-1]
-    lay.set_params(theta=w.spec["theta"], farField=0)
+    lay.set_params(theta=w.spec["theta"], farField=0, farCellGroups=0)
     plain_table = {}
     for th in (0.3, 0.4, 0.5, 0.6, 0.8, 1.0, 1.2):
         lay.set_params(theta=th)
@@ -400,7 +404,8 @@ def learned_setup(lay, w):
             "judge_vertices": int(len(targets)), "plain_rms_err": e_plain,
             "plain_rms_rel_err_per_vertex": e_plain_pv, "learned_theta": chosen,
             "learned_errors": table, "plain_errors": plain_table,
-            "group_spread": LEARNED_SPREAD}
+            "group_spread": LEARNED_SPREAD,
+            "walk": "cell groups" if LEARNED_CELL_GROUPS else "per target"}
     return model, info
 
 
@@ -414,7 +419,7 @@ def error_trajectory(lay, w, linfo, chunks=5, every=20):
     for name, th, ff in (("learned", linfo["learned_theta"], 1), ("plain", w.spec["theta"], 0)):
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
-        lay.set_params(theta=th, farField=ff)
+        lay.set_params(theta=th, farField=ff, farCellGroups=LEARNED_CELL_GROUPS if ff else 0)
         errs = []
         for c in range(chunks):
             lay.time_steps(every)
@@ -422,7 +427,7 @@ def error_trajectory(lay, w, linfo, chunks=5, every=20):
             errs.append(force_error(lay, targets, exact)[0])
         out[name] = {"theta": th, "iterations": [every * (c + 1) for c in range(chunks)],
                      "rms_err": errs}
-    lay.set_params(theta=linfo["learned_theta"], farField=1)
+    lay.set_params(theta=linfo["learned_theta"], farField=1, farCellGroups=LEARNED_CELL_GROUPS)
     return out
 
 
@@ -490,7 +495,8 @@ def main():
         # then the learned walk from the same state
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
-        lay.set_params(theta=linfo["learned_theta"], farField=1, farGroupSpread=LEARNED_SPREAD)
+        lay.set_params(theta=linfo["learned_theta"], farField=1, farGroupSpread=LEARNED_SPREAD,
+                       farCellGroups=LEARNED_CELL_GROUPS)
         lay.time_steps(args.warmup)
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)

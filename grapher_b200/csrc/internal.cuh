@@ -180,7 +180,7 @@ struct gvizCudaForce {
   // --- learned far-field (mlp.cu) ---
   void *d_mlp = nullptr;
   bool farSide = false;             // build writes FarCell records
-  double4 *d_bQ = nullptr, *d_nQ = nullptr;
+  float4 *d_bQ = nullptr, *d_nQ = nullptr;  // second moments (FP32)
   FarCell *d_cells = nullptr;       // maxNodes records
   uint32_t *d_leafPre = nullptr;    // per vertex: preorder index of its leaf
   uint32_t *d_cellCnt = nullptr;    // per cell node: points below it

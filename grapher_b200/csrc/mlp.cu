@@ -490,8 +490,8 @@ void mlp_free(gvizCudaForce *h) {
 int far_side_alloc(gvizCudaForce *h) {
   if (h->d_cells) return GVIZ_CUDA_OK;
   const size_t Vs = h->V ? h->V : 1;
-  if (cudaMalloc(&h->d_bQ, Vs * sizeof(double4)) != cudaSuccess ||
-      cudaMalloc(&h->d_nQ, Vs * sizeof(double4)) != cudaSuccess ||
+  if (cudaMalloc(&h->d_bQ, Vs * sizeof(float4)) != cudaSuccess ||
+      cudaMalloc(&h->d_nQ, Vs * sizeof(float4)) != cudaSuccess ||
       cudaMalloc(&h->d_cells, h->maxNodes * sizeof(FarCell)) != cudaSuccess ||
       cudaMalloc(&h->d_leafPre, Vs * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&h->d_cellCnt, h->maxNodes * sizeof(uint32_t)) != cudaSuccess ||

@@ -410,20 +410,19 @@ struct BU {
   uint32_t *nCounter;
   double *bM, *bSX, *bSY, *nM, *nSX, *nSY;
   uint32_t *bCnt, *bT, *nCnt, *nT, *nFlag, *rootNode, *rootT, *status;
-  double4 *bQ, *nQ;  // second central moments {Qxx, Qxy, Qyy, -}, or null
+  // second central moments {Qxx, Qxy, Qyy, -}, or null: summed and shifted
+  // in FP64, stored in FP32 (they only feed FP32 features)
+  float4 *bQ, *nQ;
   uint32_t V, k;
 };
 
 // second central moments of a child about its own centre of mass
-__device__ __forceinline__ double4 child_q(const BU &a, uint32_t c) {
-  const double4 *p = (c & GVIZ_LEAF_BIT) ? a.bQ + (c & ~GVIZ_LEAF_BIT) : a.nQ + c;
-  const double2 lo = reinterpret_cast<const double2 *>(p)[0];
-  const double2 hi = reinterpret_cast<const double2 *>(p)[1];
-  return make_double4(lo.x, lo.y, hi.x, hi.y);
+__device__ __forceinline__ float4 child_q(const BU &a, uint32_t c) {
+  return (c & GVIZ_LEAF_BIT) ? a.bQ[c & ~GVIZ_LEAF_BIT] : a.nQ[c];
 }
 
 // parallel-axis shift of a child's moments to the parent's centre of mass
-__device__ __forceinline__ void add_shifted(double4 &q, const double4 qc,
+__device__ __forceinline__ void add_shifted(double4 &q, const float4 qc,
                                             double M, double SX, double SY,
                                             double px, double py) {
   double cx = 0.0, cy = 0.0;
@@ -505,7 +504,7 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       q.y += m * dx * dy;
       q.z += m * dy * dy;
     }
-    a.bQ[b] = q;
+    a.bQ[b] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
   }
   a.bM[b] = M;
   a.bSX[b] = SX;
@@ -564,7 +563,7 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
       add_shifted(q, child_q(a, l), Ml, SXl, SYl, px, py);
       add_shifted(q, child_q(a, r), Mr, SXr, SYr, px, py);
-      a.nQ[p] = q;
+      a.nQ[p] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
     }
     a.nM[p] = M;
     a.nSX[p] = SX;
@@ -612,7 +611,7 @@ struct EM {
   uint32_t V, k, maxNodes;
   int f64;
   // far-field side records (null unless requested)
-  const double4 *bQ, *nQ;
+  const float4 *bQ, *nQ;
   const uint64_t *bHi, *bLo;
   FarCell *cells;
   uint32_t *leafPre;
@@ -623,24 +622,42 @@ __device__ __forceinline__ void put_count(const EM &a, uint32_t at, uint32_t c) 
   if (a.cellCnt && at < a.maxNodes) a.cellCnt[at] = c;
 }
 
-// Geometric centre of the cell at `depth` on the path (hi, lo): the same
-// FP64 descent as k_keys (centres c +/- halfSize/2).
+// the even bits of x (bit 2j -> bit j)
+__device__ __forceinline__ uint64_t even_bits(uint64_t x) {
+  x &= 0x5555555555555555ull;
+  x = (x | (x >> 1)) & 0x3333333333333333ull;
+  x = (x | (x >> 2)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x >> 4)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x >> 8)) & 0x0000ffff0000ffffull;
+  return (x | (x >> 16)) & 0x00000000ffffffffull;
+}
+
+// Geometric centre of the cell at `depth` on the path (hi, lo), in closed
+// form: with E (S) the east (south) bits of the path's first `depth` levels
+// read as an integer, the descent's steps of +-h0 / 2^d sum to
+// cx = cx0 + h0 ((2E + 1) / 2^depth - 1), cy = cy0 - h0 ((2S + 1) / 2^depth - 1).
+// (Only a model feature: FP64 rounding may differ from the step-by-step
+// descent in the last bits.)
 __device__ void cell_center(const GraphRoot &R, uint64_t hi, uint64_t lo,
                             int depth, double &cx, double &cy) {
-  cx = R.cx;
-  cy = R.cy;
-  double h = R.h0;
-  for (int d = 1; d <= depth; d++) {
-    const uint64_t q = d <= 32 ? (hi >> (64 - 2 * d)) & 3ull : (lo >> (128 - 2 * d)) & 3ull;
-    const double quarter = h / 2.0;
-    cx = (q & 1ull) ? cx + quarter : cx + (-quarter);
-    cy = (q & 2ull) ? cy + (-quarter) : cy + quarter;
-    h = quarter;
+  const uint64_t eh = even_bits(hi), sh = even_bits(hi >> 1);  // levels 1..32
+  uint64_t E, S;
+  if (depth <= 32) {
+    E = depth > 0 ? eh >> (32 - depth) : 0ull;
+    S = depth > 0 ? sh >> (32 - depth) : 0ull;
+  } else {
+    const uint64_t el = even_bits(lo), sl = even_bits(lo >> 1);  // levels 33..64
+    E = (eh << (depth - 32)) | (el >> (64 - depth));
+    S = (sh << (depth - 32)) | (sl >> (64 - depth));
   }
+  const double ex = ldexp(2.0 * (double)E + 1.0, -depth) - 1.0;
+  const double sy = ldexp(2.0 * (double)S + 1.0, -depth) - 1.0;
+  cx = R.cx + R.h0 * ex;
+  cy = R.cy - R.h0 * sy;
 }
 
 __device__ void put_far(const EM &a, uint32_t at, const GraphRoot &R,
-                        uint32_t keyBucket, int depth, double h, double4 q,
+                        uint32_t keyBucket, int depth, double h, float4 q,
                         double M, double SX, double SY, uint32_t s0,
                         uint32_t s1) {
   if (!a.cells || at >= a.maxNodes) return;
@@ -839,12 +856,6 @@ __device__ __forceinline__ int4 node_link(const NodeF *nodes, uint32_t j) {
   return __ldg(reinterpret_cast<const int4 *>(nodes + j) + 1);  // mass, size, next, info
 }
 
-__device__ __forceinline__ void push_group(const GroupArgs &a, uint32_t x, uint32_t y,
-                                           uint32_t c) {
-  const uint32_t slot = atomicAdd(a.nGroups, 1u);
-  if (slot < a.cap) a.groups[slot] = make_uint4(x, y, c, 0u);
-}
-
 // quadrant (NW 0, NE 1, SW 2, SE 3) of the point set of node j inside a
 // cell centred at (cx, cy), from its centre of mass
 __device__ __forceinline__ uint32_t child_quadrant(const NodeF *nodes, uint32_t j, double cx,
@@ -854,80 +865,113 @@ __device__ __forceinline__ uint32_t child_quadrant(const NodeF *nodes, uint32_t 
   return (x >= cx ? 1u : 0u) | (y < cy ? 2u : 0u);
 }
 
+// Each thread finds its groups (at most four packs of a branching cell, a
+// root, or the runs of a leaf bucket); one atomic per warp reserves the
+// warp's slots.
 __global__ __launch_bounds__(kThreads) void k_far_groups(GroupArgs a) {
   const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
+  const uint32_t lane = threadIdx.x & 31u;
   const uint32_t total = min(a.counts[3], a.maxNodes);
+  uint32_t px[4], py[4], pc[4];
+  uint32_t np = 0;                 // packs held in px/py/pc
+  uint32_t runX = 0, runEnd = 0;   // a leaf bucket's runs [runX, runEnd)
   if (t >= a.maxNodes) {
     const uint32_t g = t - a.maxNodes;
-    if (g >= a.G) return;
-    const uint32_t r = a.graphBase[g], T = a.rootT[g];
-    if (T == 0 || r >= total) return;
-    const int4 l = node_link(a.nodes, r);
-    const uint32_t c = l.w >= 0 ? 1u : a.cellCnt[r];
-    if (c <= kGroupMax) push_group(a, r, min(r + T, total), c);
-    return;
-  }
-  if (t >= total) return;
-  const int4 l = node_link(a.nodes, t);
-  if (l.w >= 0 || a.cellCnt[t] <= kGroupMax) return;  // a leaf, or a group's own cell
-  const uint32_t end = min(max((uint32_t)l.z, t + 1u), total);
-  // the children: at most four for a branching cell
-  uint32_t chX[4], chY[4], chC[4], chQ[4];
-  int nc = 0;
-  bool bucket = false;
-  for (uint32_t ch = t + 1u; ch < end;) {
-    const int4 m = node_link(a.nodes, ch);
-    const bool leaf = m.w >= 0;
-    const uint32_t sib = min(leaf ? ch + 1u : max((uint32_t)m.z, ch + 1u), end);
-    if (nc == 4) {
-      bucket = true;
-      break;
-    }
-    chX[nc] = ch;
-    chY[nc] = sib;
-    chC[nc] = leaf ? 1u : a.cellCnt[ch];
-    nc++;
-    ch = sib;
-  }
-  if (bucket) {  // points of one smallest cell: runs of kGroupMax leaves
-    for (uint32_t x = t + 1u; x < end; x += kGroupMax) {
-      const uint32_t y = min(x + kGroupMax, end);
-      push_group(a, x, y, y - x);
-    }
-    return;
-  }
-  const NodeF pn = a.nodes[t];
-  const FarCell pc = a.cells[t];
-  const double cx = (double)pn.xh + (double)pn.xl + (double)pc.ox * (double)pc.h;
-  const double cy = (double)pn.yh + (double)pn.yl + (double)pc.oy * (double)pc.h;
-  for (int i = 0; i < nc; i++) chQ[i] = child_quadrant(a.nodes, chX[i], cx, cy);
-  int first = -1;
-  uint32_t pcnt = 0, r0 = 0, r1 = 0, c0 = 0, c1 = 0;  // pack, its quadrant rectangle
-  for (int i = 0; i <= nc; i++) {
-    bool fits = false;
-    if (i < nc && chC[i] <= kGroupMax && first >= 0 && pcnt + chC[i] <= kGroupMax) {
-      const uint32_t R0 = min(r0, chQ[i] >> 1), R1 = max(r1, chQ[i] >> 1);
-      const uint32_t C0 = min(c0, chQ[i] & 1u), C1 = max(c1, chQ[i] & 1u);
-      fits = true;
-      for (int k = 0; k < nc; k++) {
-        if (k >= first && k <= i) continue;
-        const uint32_t r = chQ[k] >> 1, c = chQ[k] & 1u;
-        if (r >= R0 && r <= R1 && c >= C0 && c <= C1) fits = false;
-      }
-      if (fits) {
-        r0 = R0, r1 = R1, c0 = C0, c1 = C1;
-        pcnt += chC[i];
-        continue;
+    if (g < a.G) {
+      const uint32_t r = a.graphBase[g], T = a.rootT[g];
+      if (T != 0 && r < total) {
+        const int4 l = node_link(a.nodes, r);
+        const uint32_t c = l.w >= 0 ? 1u : a.cellCnt[r];
+        if (c <= kGroupMax) {
+          px[0] = r;
+          py[0] = min(r + T, total);
+          pc[0] = c;
+          np = 1;
+        }
       }
     }
-    if (first >= 0) push_group(a, chX[first], chY[i - 1], pcnt);
-    first = -1;
-    if (i < nc && chC[i] <= kGroupMax) {  // a larger child is cut by its own thread
-      first = i;
-      pcnt = chC[i];
-      r0 = r1 = chQ[i] >> 1;
-      c0 = c1 = chQ[i] & 1u;
+  } else if (t < total) {
+    const int4 l = node_link(a.nodes, t);
+    if (l.w < 0 && a.cellCnt[t] > kGroupMax) {
+      const uint32_t end = min(max((uint32_t)l.z, t + 1u), total);
+      uint32_t chX[4], chY[4], chC[4], chQ[4];
+      int nc = 0;
+      bool bucket = false;
+      for (uint32_t ch = t + 1u; ch < end;) {
+        const int4 m = node_link(a.nodes, ch);
+        const bool leaf = m.w >= 0;
+        const uint32_t sib = min(leaf ? ch + 1u : max((uint32_t)m.z, ch + 1u), end);
+        if (nc == 4) {
+          bucket = true;
+          break;
+        }
+        chX[nc] = ch;
+        chY[nc] = sib;
+        chC[nc] = leaf ? 1u : a.cellCnt[ch];
+        nc++;
+        ch = sib;
+      }
+      if (bucket) {  // points of one smallest cell: runs of kGroupMax leaves
+        runX = t + 1u;
+        runEnd = end;
+      } else {
+        const NodeF pn = a.nodes[t];
+        const FarCell pcell = a.cells[t];
+        const double cx = (double)pn.xh + (double)pn.xl + (double)pcell.ox * (double)pcell.h;
+        const double cy = (double)pn.yh + (double)pn.yl + (double)pcell.oy * (double)pcell.h;
+        for (int i = 0; i < nc; i++) chQ[i] = child_quadrant(a.nodes, chX[i], cx, cy);
+        int first = -1;
+        uint32_t pcnt = 0, r0 = 0, r1 = 0, c0 = 0, c1 = 0;  // pack, its quadrant rectangle
+        for (int i = 0; i <= nc; i++) {
+          if (i < nc && chC[i] <= kGroupMax && first >= 0 && pcnt + chC[i] <= kGroupMax) {
+            const uint32_t R0 = min(r0, chQ[i] >> 1), R1 = max(r1, chQ[i] >> 1);
+            const uint32_t C0 = min(c0, chQ[i] & 1u), C1 = max(c1, chQ[i] & 1u);
+            bool fits = true;
+            for (int k = 0; k < nc; k++) {
+              if (k >= first && k <= i) continue;
+              const uint32_t r = chQ[k] >> 1, c = chQ[k] & 1u;
+              if (r >= R0 && r <= R1 && c >= C0 && c <= C1) fits = false;
+            }
+            if (fits) {
+              r0 = R0, r1 = R1, c0 = C0, c1 = C1;
+              pcnt += chC[i];
+              continue;
+            }
+          }
+          if (first >= 0) {
+            px[np] = chX[first];
+            py[np] = chY[i - 1];
+            pc[np] = pcnt;
+            np++;
+          }
+          first = -1;
+          if (i < nc && chC[i] <= kGroupMax) {  // a larger child is cut by its own thread
+            first = i;
+            pcnt = chC[i];
+            r0 = r1 = chQ[i] >> 1;
+            c0 = c1 = chQ[i] & 1u;
+          }
+        }
+      }
     }
+  }
+  const uint32_t nRuns = (runEnd - runX + kGroupMax - 1u) / kGroupMax;
+  const uint32_t mine = np + nRuns;
+  uint32_t incl = mine;  // inclusive warp scan of the group counts
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  const uint32_t warpTotal = __shfl_sync(0xffffffffu, incl, 31);
+  uint32_t base = 0;
+  if (lane == 0 && warpTotal) base = atomicAdd(a.nGroups, warpTotal);
+  base = __shfl_sync(0xffffffffu, base, 0) + incl - mine;
+  for (uint32_t k = 0; k < np; k++)
+    if (base + k < a.cap) a.groups[base + k] = make_uint4(px[k], py[k], pc[k], 0u);
+  for (uint32_t k = 0; k < nRuns; k++) {
+    const uint32_t x = runX + k * kGroupMax, y = min(x + kGroupMax, runEnd);
+    if (base + np + k < a.cap) a.groups[base + np + k] = make_uint4(x, y, y - x, 0u);
   }
 }
 
