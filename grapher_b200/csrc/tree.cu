@@ -422,18 +422,20 @@ __device__ __forceinline__ float4 child_q(const BU &a, uint32_t c) {
 }
 
 // parallel-axis shift of a child's moments to the parent's centre of mass
-__device__ __forceinline__ void add_shifted(double4 &q, const float4 qc,
-                                            double M, double SX, double SY,
-                                            double px, double py) {
-  double cx = 0.0, cy = 0.0;
+// (px, py): M_c (c_c - p)^2 = (S_c - M_c p)^2 / M_c, the difference in FP64,
+// the rest in FP32 like the stored moments
+__device__ __forceinline__ void add_shifted(float4 &q, const float4 qc, double M, double SX,
+                                            double SY, double px, double py) {
+  q.x += qc.x;
+  q.y += qc.y;
+  q.z += qc.z;
   if (M > 1e-9 || M < -1e-9) {
-    cx = SX / M;
-    cy = SY / M;
+    const float tx = (float)(SX - M * px), ty = (float)(SY - M * py);
+    const float im = 1.0f / (float)M;
+    q.x += tx * tx * im;
+    q.y += tx * ty * im;
+    q.z += ty * ty * im;
   }
-  const double dx = cx - px, dy = cy - py;
-  q.x += qc.x + M * dx * dx;
-  q.y += qc.y + M * dx * dy;
-  q.z += qc.z + M * dy * dy;
 }
 
 __device__ __forceinline__ void child_vals(const BU &a, uint32_t c, double &M,
@@ -557,13 +559,14 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
     if (a.nQ) {
       double px = 0.0, py = 0.0;
       if (M > 1e-9 || M < -1e-9) {
-        px = SX / M;
-        py = SY / M;
+        const double im = 1.0 / M;
+        px = SX * im;
+        py = SY * im;
       }
-      double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
       add_shifted(q, child_q(a, l), Ml, SXl, SYl, px, py);
       add_shifted(q, child_q(a, r), Mr, SXr, SYr, px, py);
-      a.nQ[p] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+      a.nQ[p] = q;
     }
     a.nM[p] = M;
     a.nSX[p] = SX;
@@ -661,14 +664,14 @@ __device__ void put_far(const EM &a, uint32_t at, const GraphRoot &R,
                         double M, double SX, double SY, uint32_t s0,
                         uint32_t s1) {
   if (!a.cells || at >= a.maxNodes) return;
+  const double im = (M > 1e-30 || M < -1e-30) ? 1.0 / M : 0.0;
   double comx = 0.0, comy = 0.0;
   if (M > 1e-9 || M < -1e-9) {
-    comx = SX / M;
-    comy = SY / M;
+    comx = SX * im;
+    comy = SY * im;
   }
   double gx, gy;
   cell_center(R, a.bHi[keyBucket], a.bLo[keyBucket], depth, gx, gy);
-  const double im = (M > 1e-30 || M < -1e-30) ? 1.0 / M : 0.0;
   const double ih = h > 0.0 ? 1.0 / h : 0.0;
   FarCell c;
   c.qa = (float)((q.x - q.z) * im);
