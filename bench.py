@@ -7,8 +7,9 @@ Default workload (the headline metric: learned vs plain Barnes-Hut at equal
 force error): Barabasi-Albert graph, n = 1,048,576, m = 4 (4,194,294 edges,
 seeded), LinLog with gravity 1.0, start uniform in [-1000, 1000]^2 (rand_r,
 seed 7). After the warm-up steps (plain, theta = 0.5) the far-field MLP is
-trained on the GPU from pairs harvested at theta = 1.2, 0.9 and 0.6 on three
-snapshots of this layout (untimed setup, reported as train_s). Force error is the
+trained on the GPU (40 epochs) from pairs harvested for 32,768 sampled
+vertices at theta = 1.2, 0.9 and 0.6 on three snapshots of this layout
+(untimed setup, reported as train_s). Force error is the
 normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
 65,536 sampled vertices, all configurations judged on the same positions.
 The plain walk runs at theta = 0.5; the learned walk (the cell-group walk:
@@ -344,6 +345,7 @@ def replica_value(ms_max, steps, world):
 LEARNED_THETAS = tuple(round(1.3 - 0.05 * i, 2) for i in range(15))  # 1.3 ... 0.6
 LEARNED_SPREAD = 1.0
 LEARNED_CELL_GROUPS = 1  # the cell-group walk: one warp per tree-cut group of <= 32 targets
+HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
 JUDGE_VERTICES = 65536
 
 
@@ -369,7 +371,7 @@ def learned_setup(lay, w):
         if snap:
             for _ in range(5):
                 lay.step()
-        t = np.sort(rng.choice(w.V, 16384, replace=False)).astype(np.uint32)
+        t = np.sort(rng.choice(w.V, HARVEST_TARGETS, replace=False)).astype(np.uint32)
         X, T, Wt = harvest_training_set(lay, th, t)
         Xs.append(X), Ts.append(T), Ws.append(Wt)
     model = FarFieldModel(seed=SEED)
