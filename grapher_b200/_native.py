@@ -99,7 +99,24 @@ U64P = C.POINTER(C.c_uint64)
 I32P = C.POINTER(C.c_int32)
 SZ = C.c_size_t
 
+class GripRoundStats(C.Structure):
+    _fields_ = [
+        ("maxDisplacement", C.c_double),
+        ("meanDisplacement", C.c_double),
+        ("meanForce", C.c_double),
+        ("meanHeat", C.c_double),
+    ]
+
+
 _SIGS = {
+    "gvizCudaGripCreate": (C.c_int, [C.POINTER(P), SZ, U64P, U32P, C.c_int32]),
+    "gvizCudaGripDestroy": (None, [P]),
+    "gvizCudaGripSetPositions": (C.c_int, [P, DP]),
+    "gvizCudaGripGetPositions": (C.c_int, [P, DP]),
+    "gvizCudaGripSetLayer": (C.c_int, [P, SZ, U32P, SZ, U64P, U32P, U32P]),
+    "gvizCudaGripRefineRound": (C.c_int, [P, C.POINTER(GripRoundStats)]),
+    "gvizCudaGripSetStrictReductions": (C.c_int, [P, C.c_int32]),
+    "gvizCudaGripGetDecorators": (C.c_int, [P, DP, DP, DP]),
     "gvizCudaForceDefaultParams": (None, [C.POINTER(ForceParams)]),
     "gvizCudaForceCreate": (C.c_int, [C.POINTER(P), C.POINTER(GraphDesc)]),
     "gvizCudaForceDestroy": (None, [P]),

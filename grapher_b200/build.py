@@ -3,8 +3,9 @@
     python -m grapher_b200.build        # or grapher_b200.build.build()
 
 Objects go to grapher_b200/_build/, the library to grapher_b200/lib/.
-precise.cu is compiled with --fmad=false (FP64 path keeps the reference's
-rounding); everything else with fused multiply-add.
+precise.cu, noalloc.cu and grip.cu are compiled with --fmad=false (their FP64
+paths keep the reference's rounding); everything else with fused
+multiply-add.
 """
 from __future__ import annotations
 
@@ -32,6 +33,7 @@ SOURCES = {
     "forces.cu": [],
     "precise.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
+    "grip.cu": ["--fmad=false"],
     "mlp.cu": [],
     "api.cu": [],
     "host_graphs.cpp": [],

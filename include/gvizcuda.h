@@ -300,6 +300,59 @@ int64_t gvizCudaForceHarvestFarField(gvizCudaForce *h, const uint32_t *targets,
  * The numbering of the groups is not defined; the partition is. */
 int gvizCudaForceFarGroups(gvizCudaForce *h, uint32_t *groupOf, uint64_t *groupCount);
 
+/* ---- GRIP force phase -------------------------------------------------- */
+
+/* The refinement round of gviz's GRIP embedder
+ * (src/embedders/gvizGRIPEmbedder.c:1289-1334) on the device, 2-D: spring
+ * forces (calculateSpringForces :892-934: KK springs to the k nearest on
+ * coarse layers; on layer 0 GRIP's FR ops along edges and to the k nearest),
+ * the local temperature (updateLocalTemp :870-889), the heat-scaled step,
+ * removal of the net translation and rotation (:1106-1252) and the move.
+ * The MIS filtration, the placement of a new layer's vertices and the
+ * k-nearest search stay with the caller (gviz), which hands each layer over
+ * with gvizCudaGripSetLayer. Positions are FP64, indexed by vertex. */
+typedef struct gvizCudaGrip gvizCudaGrip; /* opaque handle */
+
+/* gvizGRIPRoundStats (include/embedders/gvizGRIPEmbedder.h), plus the mean
+ * heat the reference appends as the "grip.heat" stat series */
+typedef struct gvizCudaGripRoundStats {
+  double maxDisplacement;
+  double meanDisplacement;
+  double meanForce;
+  double meanHeat;
+} gvizCudaGripRoundStats;
+
+/* Graph structure (CSR over vertex ids in gviz's neighbour order, the
+ * order gvizSubgraphNeighborIterate yields) and device; positions start at 0. */
+int gvizCudaGripCreate(gvizCudaGrip **out, size_t vertexCount, const uint64_t *rowOffsets,
+                       const uint32_t *neighbors, int32_t device);
+void gvizCudaGripDestroy(gvizCudaGrip *h);
+
+/* Positions, 2 * vertexCount doubles (the embedding's vertex positions). */
+int gvizCudaGripSetPositions(gvizCudaGrip *h, const double *xy);
+int gvizCudaGripGetPositions(gvizCudaGrip *h, double *xy);
+
+/* Makes `layer` current (gvizGRIPEmbedderBegin / NextStage after placement
+ * and updateKNNs, :1010-1069): the active vertices in filtration order and
+ * each one's k-nearest list (vertex, graph distance) as CSR over that order;
+ * resets the decorators of the active vertices and the "displacement
+ * calculated" marks of all vertices as clearDecorators (:936-951) does. */
+int gvizCudaGripSetLayer(gvizCudaGrip *h, size_t layer, const uint32_t *active,
+                         size_t activeCount, const uint64_t *knnOffsets,
+                         const uint32_t *knnVertices, const uint32_t *knnDistances);
+
+/* One round (gvizGRIPEmbedderRefineRound); stats may be NULL. Returns
+ * GVIZ_CUDA_ERR_NOT_BEGUN before the first gvizCudaGripSetLayer. */
+int gvizCudaGripRefineRound(gvizCudaGrip *h, gvizCudaGripRoundStats *stats);
+
+/* 1: the layer sums (mean displacement, centroid, angular momentum,
+ * inertia, stats) in the reference's serial order, so every round is
+ * bit-identical to the reference's; 0 (default): chunked, deterministic. */
+int gvizCudaGripSetStrictReductions(gvizCudaGrip *h, int32_t strict);
+
+/* Inspection: per vertex heat, last displacement (2) and previous cosine. */
+int gvizCudaGripGetDecorators(gvizCudaGrip *h, double *heat, double *disp, double *oldCos);
+
 /* ---- allocation-free speed update ------------------------------------- */
 
 /* No counterpart in the reference. For callers that may not allocate device

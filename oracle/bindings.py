@@ -287,6 +287,95 @@ class Reference:
     def quadtree_nodes(self, pts, mass, k=1, cap=None):
         return _nodes_call(self.lib.ref_quadtree_nodes, pts, mass, k, cap)
 
+    def create_grip(self, V, ea, eb, serial=True):
+        """The reference's GRIP embedder (2-D) on an ordered edge list;
+        serial=True runs its parallel phases on the calling thread (see
+        ref_grip_create: pooled rounds race on the dispCalculated marks)."""
+        return RefGrip(self, V, ea, eb, serial)
+
+
+class RefGrip:
+    """gvizGRIPEmbedder driven through ref_driver.c: Begin / NextStage /
+    RefineRound, and the layer's filtration order, k-nearest lists,
+    positions and decorators read back."""
+
+    def __init__(self, ref: Reference, V, ea, eb, serial=True):
+        L = ref.lib
+        L.ref_grip_create.restype = C.c_void_p
+        for name in ("ref_grip_layer", "ref_grip_layer_count", "ref_grip_active", "ref_grip_knn"):
+            getattr(L, name).restype = C.c_size_t
+        self.L = L
+        self.V = int(V)
+        self._ea = np.ascontiguousarray(ea, dtype=np.uint32)
+        self._eb = np.ascontiguousarray(eb, dtype=np.uint32)
+        self.h = C.c_void_p(L.ref_grip_create(C.c_size_t(V), _ptr(self._ea, U32),
+                                              _ptr(self._eb, U32),
+                                              C.c_size_t(self._ea.shape[0]),
+                                              C.c_int(int(bool(serial)))))
+        assert L.ref_grip_init_result(self.h) == 0
+
+    def begin(self):
+        self.L.ref_grip_begin(self.h)
+
+    def next_stage(self):
+        self.L.ref_grip_next_stage(self.h)
+
+    @property
+    def layer(self):
+        return int(self.L.ref_grip_layer(self.h))
+
+    @property
+    def layer_count(self):
+        return int(self.L.ref_grip_layer_count(self.h))
+
+    def active(self):
+        out = np.zeros(self.V, np.uint32)
+        n = int(self.L.ref_grip_active(self.h, _ptr(out, U32), C.c_size_t(self.V)))
+        return out[:n]
+
+    def knn(self):
+        """(offsets over the active order, vertices, graph distances)"""
+        n = len(self.active())
+        total = int(self.L.ref_grip_knn(self.h, None, None, None, C.c_size_t(0)))
+        off = np.zeros(n + 1, np.uint64)
+        v = np.zeros(max(total, 1), np.uint32)
+        d = np.zeros(max(total, 1), np.uint32)
+        self.L.ref_grip_knn(self.h, _ptr(off, U64), _ptr(v, U32), _ptr(d, U32), C.c_size_t(total))
+        return off, v[:total], d[:total]
+
+    def refine(self):
+        """one round; (maxDisplacement, meanDisplacement, meanForce)"""
+        st = np.zeros(3)
+        self.L.ref_grip_refine(self.h, _ptr(st, D))
+        return st
+
+    def positions(self):
+        xy = np.zeros(2 * self.V)
+        self.L.ref_grip_get_positions(self.h, _ptr(xy, D))
+        return xy
+
+    def set_positions(self, xy):
+        xy = np.ascontiguousarray(xy, dtype=np.float64).reshape(-1)
+        self.L.ref_grip_set_positions(self.h, _ptr(xy, D))
+
+    def decorators(self):
+        heat = np.zeros(self.V)
+        disp = np.zeros(2 * self.V)
+        oc = np.zeros(self.V)
+        self.L.ref_grip_get_decorators(self.h, _ptr(heat, D), _ptr(disp, D), _ptr(oc, D))
+        return heat, disp, oc
+
+    def close(self):
+        if self.h:
+            self.L.ref_grip_release(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
 
 class RefLayout:
     def __init__(self, ref: Reference, handle):

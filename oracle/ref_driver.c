@@ -453,3 +453,128 @@ int ref_load_embedding(refLayout *r, const char *path) {
 int ref_save_embedding(refLayout *r, const char *name, const char *path) {
   return gvizEmbeddedGraphSaveEmbedding((gvizEmbeddedGraph *)&r->s, name, path);
 }
+
+/* ---------------------------------------------------------------------- */
+/* GRIP (src/embedders/gvizGRIPEmbedder.c), 2-D, full subgraph: the        */
+/* reference's own Begin / NextStage / RefineRound, with its filtration,   */
+/* k-nearest lists, positions and heat read back for the device round.    */
+/* ---------------------------------------------------------------------- */
+#include "core/gvizThreadPool.h"
+#include "ds/gvizArray.h"
+#include "embedders/gvizGRIPEmbedder.h"
+
+typedef struct refGrip {
+  gvizGraph g;
+  gvizGRIPState s;
+  int initRes;
+} refGrip;
+
+/* serial != 0 runs the reference's parallel phases on the calling thread
+ * (its own NULL-pool fallback, src/embedders/gvizGRIPEmbedder.c:310-311):
+ * refinementPass1Range (:1081-1083) sets the dispCalculated bits of one
+ * word from several pool threads without atomics, so with the pool a
+ * vertex can lose its mark and restart at heat L/6 in the next round, which
+ * makes pooled rounds irreproducible. */
+refGrip *ref_grip_create(size_t V, const uint32_t *ea, const uint32_t *eb, size_t E,
+                         int serial) {
+  refGrip *r = calloc(1, sizeof(refGrip));
+  if (!r)
+    return NULL;
+  gvizGraphInitAtCapacity(&r->g, 0, V ? V : 1);
+  for (size_t i = 0; i < V; i++)
+    gvizGraphAddVertex(&r->g, NULL, NULL, NULL);
+  for (size_t e = 0; e < E; e++)
+    gvizGraphAddEdge(&r->g, ea[e], eb[e]);
+  gvizGraphBuildLayout(&r->g);
+  gvizSubgraph sg = gvizSubgraphCreateFull(&r->g);
+  gvizGRIPEmbedderConfigureStats(&r->s, false);
+  r->initRes = gvizGRIPEmbedderInit(&r->s, sg, 0, 2);
+  if (serial && r->initRes == 0) {
+    gvizThreadPoolDestroy(r->s.pool);
+    r->s.pool = NULL;
+  }
+  return r;
+}
+
+int ref_grip_init_result(refGrip *r) { return r->initRes; }
+void ref_grip_begin(refGrip *r) { gvizGRIPEmbedderBegin(&r->s); }
+void ref_grip_next_stage(refGrip *r) { gvizGRIPEmbedderNextStage(&r->s); }
+size_t ref_grip_layer(refGrip *r) { return r->s.currLayer; }
+size_t ref_grip_layer_count(refGrip *r) { return r->s.layerCount; }
+
+/* the active vertices of the current layer, in filtration order */
+size_t ref_grip_active(refGrip *r, uint32_t *out, size_t cap) {
+  const size_t n = *(const size_t *)gvizArrayAtIndex(&r->s.misBorder, r->s.currLayer);
+  for (size_t i = 0; i < n && i < cap; i++)
+    out[i] = (uint32_t)r->s.misFiltration[i];
+  return n;
+}
+
+/* each active vertex's k-nearest list (vertex, graph distance), CSR over
+ * the filtration order; returns the total entries */
+size_t ref_grip_knn(refGrip *r, uint64_t *off, uint32_t *v, uint32_t *dist, size_t cap) {
+  const size_t n = *(const size_t *)gvizArrayAtIndex(&r->s.misBorder, r->s.currLayer);
+  size_t k = 0;
+  for (size_t i = 0; i < n; i++) {
+    const gvizGRIPDecorators *d = r->s.dec + r->s.misFiltration[i];
+    if (off)
+      off[i] = k;
+    for (size_t j = 0; j < d->knn.count; j++, k++) {
+      if (k < cap) {
+        const gvizFoundVertex *f = (const gvizFoundVertex *)gvizArrayAtIndex(&d->knn, j);
+        v[k] = (uint32_t)f->v;
+        dist[k] = (uint32_t)f->dist;
+      }
+    }
+  }
+  if (off)
+    off[n] = k;
+  return k;
+}
+
+/* one refinement round; stats = {maxDisplacement, meanDisplacement, meanForce} */
+void ref_grip_refine(refGrip *r, double *stats) {
+  gvizGRIPEmbedderRefineRound(&r->s);
+  const gvizGRIPRoundStats st = gvizGRIPEmbedderLastRoundStats(&r->s);
+  stats[0] = st.maxDisplacement;
+  stats[1] = st.meanDisplacement;
+  stats[2] = st.meanForce;
+}
+
+void ref_grip_get_positions(refGrip *r, double *xy) {
+  gvizEmbeddedGraph *eg = (gvizEmbeddedGraph *)&r->s;
+  const size_t V = gvizGraphSize(&r->g);
+  for (size_t i = 0; i < V; i++) {
+    const double *p = gvizEmbeddedGraphGetVPosition(eg, i);
+    xy[2 * i] = p[0];
+    xy[2 * i + 1] = p[1];
+  }
+}
+
+void ref_grip_set_positions(refGrip *r, const double *xy) {
+  gvizEmbeddedGraph *eg = (gvizEmbeddedGraph *)&r->s;
+  const size_t V = gvizGraphSize(&r->g);
+  for (size_t i = 0; i < V; i++) {
+    double p[2] = {xy[2 * i], xy[2 * i + 1]};
+    gvizEmbeddedGraphSetVPosition(eg, i, p);
+  }
+}
+
+/* per vertex: heat, last displacement (2), previous cosine */
+void ref_grip_get_decorators(refGrip *r, double *heat, double *disp, double *oldCos) {
+  const size_t V = gvizGraphSize(&r->g);
+  for (size_t i = 0; i < V; i++) {
+    heat[i] = r->s.dec[i].heat;
+    disp[2 * i] = r->s.dec[i].disp[0];
+    disp[2 * i + 1] = r->s.dec[i].disp[1];
+    oldCos[i] = r->s.dec[i].oldCos;
+  }
+}
+
+void ref_grip_release(refGrip *r) {
+  if (!r)
+    return;
+  gvizGRIPEmbedderRelease(&r->s);
+  gvizGraphRelease(&r->g);
+  free(r);
+}
