@@ -1,7 +1,8 @@
 """Benchmark of the B200 force-layout step (libgvizcuda).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ba1m_learned|rmat4m_learned|ba1m|batch4096|grid32|er65k_exact]
+                    [--workload ba1m_learned|rmat4m_learned|ba1m|batch4096|grid32|er65k_exact
+                                |grip_ba200k]
 
 Default workload (the headline metric: learned vs plain Barnes-Hut at equal
 force error): Barabasi-Albert graph, n = 1,048,576, m = 4 (4,194,294 edges,
@@ -27,6 +28,7 @@ ba1m: the same graph with degree-sized prevent-overlap
 batch4096: 4096 independent graphs, sizes log-uniform in [32, 8192], each an
 Erdos-Renyi graph (mean degree U[3,6]), a random tree or a square grid,
 FR theta = 0.7, laid out together in one handle (one step = every graph steps).
+grip_ba200k: GRIP refinement rounds at layer 0 (see grip_bench).
 
 A step is one full gvizForceEmbedderStep equivalent: quadtree rebuild,
 attraction, Barnes-Hut repulsion, gravity, FA2 speed and position update.
@@ -433,6 +435,128 @@ def error_trajectory(lay, w, linfo, chunks=5, every=20):
     return out
 
 
+# ---------------------------------------------------------------------- GRIP
+GRIP_V, GRIP_M, GRIP_K = 200_000, 3, 128
+
+
+def grip_graph():
+    from grapher_b200 import graphs
+    a, b = graphs.barabasi_albert(GRIP_V, GRIP_M, SEED)
+    row, col = graphs.to_csr(GRIP_V, a, b)
+    return a, b, row, col
+
+
+def grip_reference_rounds(a, b, max_rounds, budget_s=20.0):
+    """Seconds per round of the reference's own GRIP (pooled, as it runs by
+    default) at layer 0 of its pipeline on the same graph, and its threads."""
+    from oracle.bindings import Reference
+    ref = Reference()
+    rg = ref.create_grip(GRIP_V, a, b, serial=False)
+    rg.begin()
+    while rg.layer > 0:
+        rg.next_stage()
+    rg.refine()  # warm-up
+    times = []
+    t_start = time.perf_counter()
+    while len(times) < max_rounds and time.perf_counter() - t_start < budget_s:
+        t0 = time.perf_counter()
+        rg.refine()
+        times.append(time.perf_counter() - t0)
+    rg.close()
+    return float(np.mean(times)), ref.pool_threads(), len(times)
+
+
+def grip_bench(args):
+    """GRIP refinement rounds at layer 0 (every vertex active): BA
+    n = 200,000, m = 3, k = 128 nearest by graph distance, positions uniform
+    in [-1000, 1000]^2. value = rounds/s on the device; e2e = rounds with the
+    positions copied from and back to host memory every round."""
+    a, b, row, col = grip_graph()
+    metric = "GRIP refinement rounds/sec, layer 0"
+    config = {"workload": f"grip_ba200k: barabasi_albert n={GRIP_V} m={GRIP_M} "
+                          f"edges={len(a)}, layer 0, k={GRIP_K}",
+              "precision": "fp64", "parallelism": "replicas1",
+              "l2": "positions fit in L2; k-nearest lists (200 MB) do not"}
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        t, cores, n = grip_reference_rounds(a, b, max(args.steps, 1))
+        base = {"value": 1.0 / t, "unit": "rounds/s", "cores": cores, "kind": "reference",
+                "sample": f"{n} rounds of the reference's GRIP (gvizGRIPEmbedderRefineRound, "
+                          f"gvizThreadPool over {cores} threads) at layer 0 of its own pipeline"}
+        print(json.dumps({"impl": "reference", "metric": metric, "value": base["value"],
+                          "unit": "rounds/s", "n_gpus": args.gpus, "steps": n, "warmup": 1,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "f64", "data": "synthetic", "config": config,
+                          "cpu_baseline": base,
+                          "e2e": {"value": base["value"], "unit": "rounds/s",
+                                  "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return 0
+    from grapher_b200 import graphs
+    from grapher_b200.grip import GripRefiner, k_nearest
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    act = np.arange(GRIP_V, dtype=np.uint32)
+    off, kv, kd = k_nearest(row, col, act, GRIP_K)
+    x0 = graphs.randomize_positions(GRIP_V, 1000.0, SEED)
+    g = GripRefiner(row, col, device=local)
+    g.set_positions(x0)
+    g.set_layer(0, act, off, kv, kd)
+    g.time_rounds(args.warmup)
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms, fms = g.time_rounds(args.steps)
+    clocks = sampler.stop()
+    value = args.steps / (ms / 1e3)
+    # e2e through the C ABI with host positions every round
+    import torch
+    pinned = torch.empty(2 * GRIP_V, dtype=torch.float64, pin_memory=True)
+    pinned.numpy()[:] = g.positions()
+    xy = pinned.numpy()
+    n_e2e = max(3, min(args.steps, 50))
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        g.set_positions(xy)
+        g.refine_round()
+        xy[:] = g.positions()
+    e2e_s = time.perf_counter() - t0
+    # force kernel: algorithmic bytes per launch
+    E2, K = int(row[-1]), int(off[-1])
+    per_vertex = 8 + 16 + 4 + 16 + 16 + 16 + 16 + 16 + 8 + 2  # offsets, row, id, state
+    bytes_launch = GRIP_V * per_vertex + K * (4 + 4 + 16) + E2 * (4 + 16)
+    fwd_ms = fms / args.steps
+    peaks, src = load_peaks()
+    achieved = bytes_launch / (fwd_ms * 1e-3) / 1e9
+    line = {
+        "metric": metric, "value": value, "unit": "rounds/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config, "clocks": clocks,
+        "e2e": {"value": n_e2e / e2e_s, "unit": "rounds/s", "h2d_bytes_per_step": 16 * GRIP_V,
+                "d2h_bytes_per_step": 16 * GRIP_V + 32, "steps": n_e2e,
+                "timer": "host wall clock around synchronous calls"},
+        "gpu_launches": 5 * args.steps, "kernels_per_step": 5,
+        "roofline": {"kernel": "k_grip_pass1", "bound": "hbm", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "peak_source": f"hbm_gbs ({src})",
+                     "algorithmic": (f"{bytes_launch} B per launch: {GRIP_V} vertices x "
+                                     f"{per_vertex} B + {K} nearest x 24 B + {E2} edge "
+                                     "entries x 20 B (the gathered positions mostly hit L2)"),
+                     "share_of_step": fms / ms},
+        "knn_entries": K, "peaks": src,
+    }
+    if not args.no_cpu_baseline:
+        t, cores, n = grip_reference_rounds(a, b, 10)
+        line["cpu_baseline"] = {"value": 1.0 / t, "unit": "rounds/s", "cores": cores,
+                                "kind": "reference",
+                                "sample": f"{n} rounds of the reference's GRIP at layer 0 of its "
+                                          f"own pipeline on the same graph, gvizThreadPool over "
+                                          f"{cores} threads"}
+    g.close()
+    print(json.dumps(line))
+    return 0
+
+
 # ---------------------------------------------------------------------- ours
 def main():
     ap = argparse.ArgumentParser()
@@ -440,10 +564,12 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ba1m_learned", choices=sorted(SPECS))
+    ap.add_argument("--workload", default="ba1m_learned", choices=sorted(SPECS) + ["grip_ba200k"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "grip_ba200k":
+        return grip_bench(args)
     w = Workload(args.workload)
     learned = args.workload in ("ba1m_learned", "rmat4m_learned")
     if args.impl == "reference":

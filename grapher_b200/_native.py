@@ -117,6 +117,10 @@ _SIGS = {
     "gvizCudaGripRefineRound": (C.c_int, [P, C.POINTER(GripRoundStats)]),
     "gvizCudaGripSetStrictReductions": (C.c_int, [P, C.c_int32]),
     "gvizCudaGripGetDecorators": (C.c_int, [P, DP, DP, DP]),
+    "gvizCudaGripTimeRounds": (C.c_int, [P, C.c_uint32, C.POINTER(C.c_float),
+                                         C.POINTER(C.c_float)]),
+    "gvizCudaGripKNearest": (C.c_int64, [SZ, U64P, U32P, U32P, SZ, C.POINTER(C.c_uint8),
+                                         C.c_uint32, U64P, U32P, U32P]),
     "gvizCudaForceDefaultParams": (None, [C.POINTER(ForceParams)]),
     "gvizCudaForceCreate": (C.c_int, [C.POINTER(P), C.POINTER(GraphDesc)]),
     "gvizCudaForceDestroy": (None, [P]),

@@ -16,6 +16,9 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "gvizcuda.h"
 
 namespace {
@@ -28,20 +31,48 @@ constexpr double kS = 3;             // gvizGRIPs
 constexpr double kFrScale = 0.05;    // FR_SCALE_FACTOR
 constexpr double kEps = 1e-7;        // gvizNumericEpsilon
 constexpr int kThreads = 256;
-constexpr int kSumThreads = 1024;
+constexpr int kSumThreads = 1024;  // room of the partial kernels' staging
+constexpr int kPartThreads = 256;
+constexpr uint32_t kMaxParts = 592;  // 4 blocks per SM
 
 struct GripArgs {
   const uint64_t *row;
   const uint32_t *col;
-  const uint32_t *active;
-  const uint64_t *knnOff;
-  const uint32_t *knnV, *knnD;
+  const uint32_t *active;   // the layer in filtration order (sums, move)
+  const uint32_t *work;     // the layer in label order (force kernel)
+  const uint64_t *knnOff;   // list t (of work[t]) has knnOff[t+1] - knnOff[t] entries
+  const uint64_t *warpBase; // lists of warp w start at warpBase[w]
+  const uint32_t *knnV, *knnD;  // entry e of list 32w + l at warpBase[w] + 32e + l
+  double *part;             // per-block partial sums of the ordered reductions
   double2 *pos, *disp, *oldDisp;
   double *heat, *oldCos, *lastF, *nrm;
   uint8_t *calc;
   double *red;  // [0,1] mean disp, [2,3] centroid, [4] omega, [5] rotate, [6..9] stats
-  uint32_t n, layer;
+  uint32_t n, layer, parts;  // parts: blocks of the partial-sum kernels
 };
+
+constexpr int kBatch = 8;
+
+// gvizVecAccKKForce (include/core/gvizVec.h:138-186) at L = dist * 10
+__device__ __forceinline__ void kk_term(double2 p, double2 q, uint32_t dist, double &fx,
+                                        double &fy) {
+  const double L = (double)dist * kEdge;
+  if (L < 1e-9) return;
+  const double dx = q.x - p.x, dy = q.y - p.y;
+  const double s = sqrt(dx * dx + dy * dy) / L - 1.0;
+  fx += s * dx;
+  fy += s * dy;
+}
+
+// gvizVecAccGRIPFRAttForce (include/core/gvizVec.h:115-180), frScale 0.05
+__device__ __forceinline__ void grip_att_term(double2 p, double2 q, double &fx, double &fy) {
+  const double dx = p.x - q.x, dy = p.y - q.y;
+  const double d2 = dx * dx + dy * dy;
+  if (d2 < 1e-18) return;
+  const double s = kFrScale * (kEdge * kEdge) / d2;
+  fx += s * dx;
+  fy += s * dy;
+}
 
 // Spring forces (calculateSpringForces :892-934; the ops of
 // include/core/gvizVec.h:138-316 via src/embedders/gvizForceDirected.c:6-20),
@@ -50,22 +81,32 @@ struct GripArgs {
 __global__ __launch_bounds__(kThreads) void k_grip_pass1(GripArgs a) {
   const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= a.n) return;
-  const uint32_t v = a.active[i];
+  const uint32_t v = a.work[i];
   const double2 prev = a.disp[v];
   a.oldDisp[v] = prev;
   const double2 p = a.pos[v];
   double fx = 0.0, fy = 0.0;
-  const uint64_t k0 = a.knnOff[i], k1 = a.knnOff[i + 1];
+  // this thread's list, stored warp-interleaved so that the lanes' loads of
+  // entry e are coalesced
+  const uint32_t len = (uint32_t)(a.knnOff[i + 1] - a.knnOff[i]);
+  const uint64_t k0 = a.warpBase[i >> 5] + (i & 31u);
+  const uint64_t k1 = k0 + 32ull * len;
+  // the list is walked in batches of kBatch entries: all their loads are
+  // issued first (the gathers are what bounds this kernel), then the terms
+  // are added in list order, as the reference adds them
   if (a.layer > 0) {
-    for (uint64_t e = k0; e < k1; e++) {  // KK springs at graph distance
-      const double L = (double)a.knnD[e] * kEdge;
-      if (L < 1e-9) continue;
-      const double2 q = a.pos[a.knnV[e]];
-      const double dx = q.x - p.x, dy = q.y - p.y;
-      const double s = sqrt(dx * dx + dy * dy) / L - 1.0;
-      fx += s * dx;
-      fy += s * dy;
+    uint64_t e = k0;
+    for (; e + 32ull * (kBatch - 1) < k1; e += 32ull * kBatch) {  // KK springs
+      uint32_t dist[kBatch];
+      double2 q[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; j++) dist[j] = a.knnD[e + 32ull * j];
+#pragma unroll
+      for (int j = 0; j < kBatch; j++) q[j] = a.pos[a.knnV[e + 32ull * j]];
+#pragma unroll
+      for (int j = 0; j < kBatch; j++) kk_term(p, q[j], dist[j], fx, fy);
     }
+    for (; e < k1; e += 32) kk_term(p, a.pos[a.knnV[e]], a.knnD[e], fx, fy);
   } else {
     const double lenSq = kEdge * kEdge;
     for (uint64_t j = a.row[v]; j < a.row[v + 1]; j++) {  // along edges
@@ -77,15 +118,15 @@ __global__ __launch_bounds__(kThreads) void k_grip_pass1(GripArgs a) {
       fx += s * dx;
       fy += s * dy;
     }
-    for (uint64_t e = k0; e < k1; e++) {  // from the k nearest
-      const double2 q = a.pos[a.knnV[e]];
-      const double dx = p.x - q.x, dy = p.y - q.y;
-      const double d2 = dx * dx + dy * dy;
-      if (d2 < 1e-18) continue;
-      const double s = kFrScale * lenSq / d2;
-      fx += s * dx;
-      fy += s * dy;
+    uint64_t e = k0;
+    for (; e + 32ull * (kBatch - 1) < k1; e += 32ull * kBatch) {  // from the k nearest
+      double2 q[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; j++) q[j] = a.pos[a.knnV[e + 32ull * j]];
+#pragma unroll
+      for (int j = 0; j < kBatch; j++) grip_att_term(p, q[j], fx, fy);
     }
+    for (; e < k1; e += 32) grip_att_term(p, a.pos[a.knnV[e]], fx, fy);
   }
   double heat = a.heat[v], oc = a.oldCos[v];
   if (!a.calc[v]) {
@@ -117,25 +158,39 @@ __global__ __launch_bounds__(kThreads) void k_grip_pass1(GripArgs a) {
   a.oldCos[v] = oc;
 }
 
-// Chunked ordered sums in one block (strict: one thread): thread t sums
-// items [t*c, (t+1)*c) in order, thread 0 adds the chunk sums in order.
+// Ordered sums over the layer in two launches. Partial: block b takes the
+// contiguous range of items [b*B, (b+1)*B); each thread sums a contiguous
+// chunk of it in order and thread 0 adds the chunk sums in order. Final:
+// one thread adds the block partials in order. Deterministic; with one block
+// of one thread (strict reductions) the whole sum runs in the reference's
+// serial order.
 template <int K>
-__device__ __forceinline__ void block_ordered_sum(double (&acc)[K], double (*part)[K]) {
-  for (int k = 0; k < K; k++) part[threadIdx.x][k] = acc[k];
+__device__ __forceinline__ void block_partial(double (&acc)[K], double *out,
+                                              double (*tmp)[K]) {
+  for (int k = 0; k < K; k++) tmp[threadIdx.x][k] = acc[k];
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int k = 0; k < K; k++) acc[k] = part[0][k];
+    for (int k = 0; k < K; k++) acc[k] = tmp[0][k];
     for (unsigned t = 1; t < blockDim.x; t++)
-      for (int k = 0; k < K; k++) acc[k] += part[t][k];
+      for (int k = 0; k < K; k++) acc[k] += tmp[t][k];
+    for (int k = 0; k < K; k++) out[blockIdx.x * K + k] = acc[k];
   }
 }
 
-// mean displacement (removeNetTranslation :1106-1121) and centroid of the
-// positions (removeNetRotation :1192-1203)
-__global__ __launch_bounds__(kSumThreads) void k_grip_sums1(GripArgs a) {
-  __shared__ double part[kSumThreads][4];
-  const uint32_t c = (a.n + blockDim.x - 1) / blockDim.x;
-  const uint32_t b = threadIdx.x * c, e = min(b + c, a.n);
+__device__ __forceinline__ void item_range(uint32_t n, uint32_t &b, uint32_t &e) {
+  const uint32_t per = (n + gridDim.x - 1) / gridDim.x;
+  const uint32_t lo = blockIdx.x * per, hi = min(lo + per, n);
+  const uint32_t c = (per + blockDim.x - 1) / blockDim.x;
+  b = min(lo + threadIdx.x * c, hi);
+  e = min(b + c, hi);
+}
+
+// sums of the displacements and the positions (removeNetTranslation
+// :1106-1121, the centroid of removeNetRotation :1192-1203)
+__global__ __launch_bounds__(kSumThreads) void k_grip_part1(GripArgs a) {
+  __shared__ double tmp[kSumThreads][4];
+  uint32_t b, e;
+  item_range(a.n, b, e);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   for (uint32_t i = b; i < e; i++) {
     const uint32_t v = a.active[i];
@@ -145,22 +200,27 @@ __global__ __launch_bounds__(kSumThreads) void k_grip_sums1(GripArgs a) {
     acc[2] += p.x;
     acc[3] += p.y;
   }
-  block_ordered_sum<4>(acc, part);
-  if (threadIdx.x == 0) {
-    const double inv = 1.0 / (double)a.n;
-    a.red[0] = acc[0] * inv;
-    a.red[1] = acc[1] * inv;
-    a.red[2] = acc[2] / (double)a.n;
-    a.red[3] = acc[3] / (double)a.n;
-  }
+  block_partial<4>(acc, a.part, tmp);
+}
+
+__global__ void k_grip_final1(GripArgs a) {
+  double acc[4];
+  for (int k = 0; k < 4; k++) acc[k] = a.part[k];
+  for (uint32_t b = 1; b < a.parts; b++)
+    for (int k = 0; k < 4; k++) acc[k] += a.part[b * 4 + k];
+  const double inv = 1.0 / (double)a.n;
+  a.red[0] = acc[0] * inv;
+  a.red[1] = acc[1] * inv;
+  a.red[2] = acc[2] / (double)a.n;
+  a.red[3] = acc[3] / (double)a.n;
 }
 
 // angular momentum of the translated displacements and the polar moment of
 // inertia about the centroid; omega = L / I (:1204-1252, dim 2)
-__global__ __launch_bounds__(kSumThreads) void k_grip_sums2(GripArgs a) {
-  __shared__ double part[kSumThreads][2];
-  const uint32_t c = (a.n + blockDim.x - 1) / blockDim.x;
-  const uint32_t b = threadIdx.x * c, e = min(b + c, a.n);
+__global__ __launch_bounds__(kSumThreads) void k_grip_part2(GripArgs a) {
+  __shared__ double tmp[kSumThreads][2];
+  uint32_t b, e;
+  item_range(a.n, b, e);
   const double mx = a.red[0], my = a.red[1], cx = a.red[2], cy = a.red[3];
   double acc[2] = {0.0, 0.0};
   for (uint32_t i = b; i < e; i++) {
@@ -173,12 +233,18 @@ __global__ __launch_bounds__(kSumThreads) void k_grip_sums2(GripArgs a) {
     acc[0] += rx * d.y - ry * d.x;
     acc[1] += rx * rx + ry * ry;
   }
-  block_ordered_sum<2>(acc, part);
-  if (threadIdx.x == 0) {
-    const bool rotate = a.n >= 3 && !(fabs(acc[1]) < kEps);
-    a.red[4] = rotate ? acc[0] / acc[1] : 0.0;
-    a.red[5] = rotate ? 1.0 : 0.0;
+  block_partial<2>(acc, a.part, tmp);
+}
+
+__global__ void k_grip_final2(GripArgs a) {
+  double L = a.part[0], I = a.part[1];
+  for (uint32_t b = 1; b < a.parts; b++) {
+    L += a.part[b * 2];
+    I += a.part[b * 2 + 1];
   }
+  const bool rotate = a.n >= 3 && !(fabs(I) < kEps);
+  a.red[4] = rotate ? L / I : 0.0;
+  a.red[5] = rotate ? 1.0 : 0.0;
 }
 
 // remove the translation and the rotation, move (gvizEmbeddedGraphAdd-
@@ -203,10 +269,10 @@ __global__ __launch_bounds__(kThreads) void k_grip_apply(GripArgs a) {
 }
 
 // round statistics (:1302-1331): max and sums of |disp|, heat, force
-__global__ __launch_bounds__(kSumThreads) void k_grip_stats(GripArgs a) {
-  __shared__ double part[kSumThreads][4];
-  const uint32_t c = (a.n + blockDim.x - 1) / blockDim.x;
-  const uint32_t b = threadIdx.x * c, e = min(b + c, a.n);
+__global__ __launch_bounds__(kSumThreads) void k_grip_part3(GripArgs a) {
+  __shared__ double tmp[kSumThreads][4];
+  uint32_t b, e;
+  item_range(a.n, b, e);
   double acc[4] = {0.0, 0.0, 0.0, 0.0};  // max, sum disp, sum heat, sum force
   for (uint32_t i = b; i < e; i++) {
     const uint32_t v = a.active[i];
@@ -216,19 +282,26 @@ __global__ __launch_bounds__(kSumThreads) void k_grip_stats(GripArgs a) {
     acc[2] += a.heat[v];
     acc[3] += a.lastF[v];
   }
-  part[threadIdx.x][0] = acc[0];
+  tmp[threadIdx.x][0] = acc[0];
   __syncthreads();
   double mx = acc[0];
   if (threadIdx.x == 0)
-    for (unsigned t = 1; t < blockDim.x; t++) mx = fmax(mx, part[t][0]);
+    for (unsigned t = 1; t < blockDim.x; t++) mx = fmax(mx, tmp[t][0]);
   __syncthreads();
-  block_ordered_sum<4>(acc, part);
-  if (threadIdx.x == 0) {
-    a.red[6] = mx;
-    a.red[7] = a.n ? acc[1] / a.n : 0.0;
-    a.red[8] = a.n ? acc[2] / a.n : 0.0;
-    a.red[9] = a.n ? acc[3] / a.n : 0.0;
+  block_partial<4>(acc, a.part, tmp);
+  if (threadIdx.x == 0) a.part[blockIdx.x * 4] = mx;
+}
+
+__global__ void k_grip_final3(GripArgs a) {
+  double mx = a.part[0], acc[3] = {a.part[1], a.part[2], a.part[3]};
+  for (uint32_t b = 1; b < a.parts; b++) {
+    mx = fmax(mx, a.part[b * 4]);
+    for (int k = 0; k < 3; k++) acc[k] += a.part[b * 4 + 1 + k];
   }
+  a.red[6] = mx;
+  a.red[7] = a.n ? acc[0] / a.n : 0.0;
+  a.red[8] = a.n ? acc[1] / a.n : 0.0;
+  a.red[9] = a.n ? acc[2] / a.n : 0.0;
 }
 
 // clearDecorators (:936-951) for the vertices of the new layer
@@ -258,9 +331,16 @@ struct gvizCudaGrip {
   double *d_red = nullptr;
   uint8_t *d_calc = nullptr;
   uint32_t *d_active = nullptr, *d_knnV = nullptr, *d_knnD = nullptr;
-  uint64_t *d_knnOff = nullptr;
+  uint64_t *d_knnOff = nullptr, *d_warpBase = nullptr;
+  double *d_part = nullptr;  // kMaxParts x 4 partial sums
+  uint32_t *d_work = nullptr;
   size_t n = 0, knnCap = 0, layer = 0;
   bool hasLayer = false;
+  // Vertices are relabelled in breadth-first order inside the handle (old
+  // id perm[n] is label n), so that graph-near vertices, whose k-nearest
+  // lists overlap, sit near each other in memory and in the force kernel's
+  // warps. The API keeps the caller's ids.
+  std::vector<uint32_t> perm, inv;
 };
 
 namespace {
@@ -286,7 +366,10 @@ GripArgs grip_args(gvizCudaGrip *h) {
   a.row = h->d_row;
   a.col = h->d_col;
   a.active = h->d_active;
+  a.work = h->d_work;
   a.knnOff = h->d_knnOff;
+  a.warpBase = h->d_warpBase;
+  a.part = h->d_part;
   a.knnV = h->d_knnV;
   a.knnD = h->d_knnD;
   a.pos = h->d_pos;
@@ -300,6 +383,8 @@ GripArgs grip_args(gvizCudaGrip *h) {
   a.red = h->d_red;
   a.n = (uint32_t)h->n;
   a.layer = (uint32_t)h->layer;
+  const uint32_t want = (uint32_t)((h->n + 1023) / 1024);
+  a.parts = h->strict ? 1u : (want < 1 ? 1u : (want > kMaxParts ? kMaxParts : want));
   return a;
 }
 
@@ -317,6 +402,9 @@ void grip_free(gvizCudaGrip *h) {
   cudaFree(h->d_calc);
   cudaFree(h->d_active);
   cudaFree(h->d_knnOff);
+  cudaFree(h->d_warpBase);
+  cudaFree(h->d_part);
+  cudaFree(h->d_work);
   cudaFree(h->d_knnV);
   cudaFree(h->d_knnD);
 }
@@ -359,15 +447,53 @@ int gvizCudaGripCreate(gvizCudaGrip **out, size_t vertexCount, const uint64_t *r
   if (!rc) rc |= galloc(&h->d_calc, V);
   if (!rc) rc |= galloc(&h->d_active, V);
   if (!rc) rc |= galloc(&h->d_knnOff, V + 1);
+  if (!rc) rc |= galloc(&h->d_warpBase, V / 32 + 2);
+  if (!rc) rc |= galloc(&h->d_part, (size_t)kMaxParts * 4);
+  if (!rc) rc |= galloc(&h->d_work, V);
   if (rc) {
     grip_free(h);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return rc;
   }
+  // breadth-first labels: from the highest-degree vertex, then from every
+  // vertex not reached yet, in id order
+  h->perm.reserve(V);
+  h->inv.assign(V, 0);
+  std::vector<uint8_t> seen(V, 0);
+  size_t hub = 0;
+  for (size_t v = 1; v < V; v++)
+    if (rowOffsets[v + 1] - rowOffsets[v] > rowOffsets[hub + 1] - rowOffsets[hub]) hub = v;
+  for (size_t k = 0; k <= V; k++) {
+    const size_t s0 = k == 0 ? hub : k - 1;
+    if (s0 >= V || seen[s0]) continue;
+    seen[s0] = 1;
+    size_t head = h->perm.size();
+    h->perm.push_back((uint32_t)s0);
+    for (; head < h->perm.size(); head++) {
+      const uint32_t u = h->perm[head];
+      for (uint64_t j = rowOffsets[u]; j < rowOffsets[u + 1]; j++) {
+        const uint32_t w = neighbors[j];
+        if (!seen[w]) {
+          seen[w] = 1;
+          h->perm.push_back(w);
+        }
+      }
+    }
+  }
+  for (size_t n = 0; n < V; n++) h->inv[h->perm[n]] = (uint32_t)n;
+  // the CSR in labels, each row keeping the caller's neighbour order
+  std::vector<uint64_t> row2(V + 1, 0);
+  std::vector<uint32_t> col2(E2);
+  for (size_t n = 0; n < V; n++) {
+    const uint32_t o = h->perm[n];
+    row2[n + 1] = row2[n] + (rowOffsets[o + 1] - rowOffsets[o]);
+    for (uint64_t j = rowOffsets[o]; j < rowOffsets[o + 1]; j++)
+      col2[row2[n] + (j - rowOffsets[o])] = h->inv[neighbors[j]];
+  }
   if (V) {
-    cudaMemcpyAsync(h->d_row, rowOffsets, (V + 1) * 8, cudaMemcpyHostToDevice, h->stream);
-    if (E2) cudaMemcpyAsync(h->d_col, neighbors, E2 * 4, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_row, row2.data(), (V + 1) * 8, cudaMemcpyHostToDevice, h->stream);
+    if (E2) cudaMemcpyAsync(h->d_col, col2.data(), E2 * 4, cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(h->d_pos, 0, V * 16, h->stream);
     cudaMemsetAsync(h->d_disp, 0, V * 16, h->stream);
     cudaMemsetAsync(h->d_old, 0, V * 16, h->stream);
@@ -405,7 +531,12 @@ int gvizCudaGripSetPositions(gvizCudaGrip *h, const double *xy) {
   if (!h || (h->V && !xy)) return GVIZ_CUDA_ERR_ARG;
   GripGuard guard(h->device);
   if (!h->V) return GVIZ_CUDA_OK;
-  if (cudaMemcpyAsync(h->d_pos, xy, h->V * 16, cudaMemcpyHostToDevice, h->stream) !=
+  std::vector<double> tmp(2 * h->V);
+  for (size_t n = 0; n < h->V; n++) {
+    tmp[2 * n] = xy[2 * (size_t)h->perm[n]];
+    tmp[2 * n + 1] = xy[2 * (size_t)h->perm[n] + 1];
+  }
+  if (cudaMemcpyAsync(h->d_pos, tmp.data(), h->V * 16, cudaMemcpyHostToDevice, h->stream) !=
           cudaSuccess ||
       cudaStreamSynchronize(h->stream) != cudaSuccess)
     return GVIZ_CUDA_ERR_CUDA;
@@ -416,10 +547,15 @@ int gvizCudaGripGetPositions(gvizCudaGrip *h, double *xy) {
   if (!h || (h->V && !xy)) return GVIZ_CUDA_ERR_ARG;
   GripGuard guard(h->device);
   if (!h->V) return GVIZ_CUDA_OK;
-  if (cudaMemcpyAsync(xy, h->d_pos, h->V * 16, cudaMemcpyDeviceToHost, h->stream) !=
+  std::vector<double> tmp(2 * h->V);
+  if (cudaMemcpyAsync(tmp.data(), h->d_pos, h->V * 16, cudaMemcpyDeviceToHost, h->stream) !=
           cudaSuccess ||
       cudaStreamSynchronize(h->stream) != cudaSuccess)
     return GVIZ_CUDA_ERR_CUDA;
+  for (size_t n = 0; n < h->V; n++) {
+    xy[2 * (size_t)h->perm[n]] = tmp[2 * n];
+    xy[2 * (size_t)h->perm[n] + 1] = tmp[2 * n + 1];
+  }
   return GVIZ_CUDA_OK;
 }
 
@@ -436,32 +572,80 @@ int gvizCudaGripSetLayer(gvizCudaGrip *h, size_t layer, const uint32_t *active,
   if (knnOffsets && activeCount && knnOffsets[0] != 0) return GVIZ_CUDA_ERR_ARG;
   for (size_t e = 0; e < K; e++)
     if (knnVertices[e] >= h->V) return GVIZ_CUDA_ERR_ARG;
+  // the layer in labels (filtration order kept for the sums and the move);
+  // the force kernel takes it in label order, its lists warp-interleaved:
+  // entry e of list t = 32w + l at base[w] + 32e + l
+  std::vector<uint32_t> act2(activeCount), order(activeCount), work(activeCount);
+  for (size_t i = 0; i < activeCount; i++) {
+    act2[i] = h->inv[active[i]];
+    order[i] = (uint32_t)i;
+  }
+  std::sort(order.begin(), order.end(),
+            [&](uint32_t x, uint32_t y) { return act2[x] < act2[y]; });
+  std::vector<uint64_t> woff(activeCount + 1, 0);
+  for (size_t t = 0; t < activeCount; t++) {
+    work[t] = act2[order[t]];
+    woff[t + 1] = woff[t] + (knnOffsets[order[t] + 1] - knnOffsets[order[t]]);
+  }
+  const size_t warps = (activeCount + 31) / 32;
+  std::vector<uint64_t> base(warps + 1, 0);
+  for (size_t w = 0; w < warps; w++) {
+    uint64_t mx = 0;
+    for (size_t t = 32 * w; t < activeCount && t < 32 * w + 32; t++)
+      mx = std::max<uint64_t>(mx, woff[t + 1] - woff[t]);
+    base[w + 1] = base[w] + 32 * mx;
+  }
+  const size_t T = base[warps];
+  std::vector<uint32_t> iv(T, 0), id(T, 0);
+  for (size_t t = 0; t < activeCount; t++) {
+    const uint64_t b = base[t / 32] + (t % 32), src = knnOffsets[order[t]];
+    for (uint64_t e = 0; e < woff[t + 1] - woff[t]; e++) {
+      iv[b + 32 * e] = h->inv[knnVertices[src + e]];
+      id[b + 32 * e] = knnDistances[src + e];
+    }
+  }
   GripGuard guard(h->device);
-  if (K > h->knnCap) {
+  if (T > h->knnCap) {
     cudaStreamSynchronize(h->stream);
     cudaFree(h->d_knnV);
     cudaFree(h->d_knnD);
     h->d_knnV = h->d_knnD = nullptr;
     h->knnCap = 0;
-    if (galloc(&h->d_knnV, K) || galloc(&h->d_knnD, K)) return GVIZ_CUDA_ERR_ALLOC;
-    h->knnCap = K;
+    if (galloc(&h->d_knnV, T) || galloc(&h->d_knnD, T)) return GVIZ_CUDA_ERR_ALLOC;
+    h->knnCap = T;
   }
   h->n = activeCount;
   h->layer = layer;
   h->hasLayer = true;
   if (activeCount) {
-    cudaMemcpyAsync(h->d_active, active, activeCount * 4, cudaMemcpyHostToDevice, h->stream);
-    cudaMemcpyAsync(h->d_knnOff, knnOffsets, (activeCount + 1) * 8, cudaMemcpyHostToDevice,
+    cudaMemcpyAsync(h->d_active, act2.data(), activeCount * 4, cudaMemcpyHostToDevice,
                     h->stream);
-    if (K) {
-      cudaMemcpyAsync(h->d_knnV, knnVertices, K * 4, cudaMemcpyHostToDevice, h->stream);
-      cudaMemcpyAsync(h->d_knnD, knnDistances, K * 4, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_work, work.data(), activeCount * 4, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_knnOff, woff.data(), (activeCount + 1) * 8, cudaMemcpyHostToDevice,
+                    h->stream);
+    cudaMemcpyAsync(h->d_warpBase, base.data(), (warps + 1) * 8, cudaMemcpyHostToDevice,
+                    h->stream);
+    if (T) {
+      cudaMemcpyAsync(h->d_knnV, iv.data(), T * 4, cudaMemcpyHostToDevice, h->stream);
+      cudaMemcpyAsync(h->d_knnD, id.data(), T * 4, cudaMemcpyHostToDevice, h->stream);
     }
   }
   if (h->V) cudaMemsetAsync(h->d_calc, 0, h->V, h->stream);
   if (activeCount) k_grip_clear<<<grid_for(activeCount), kThreads, 0, h->stream>>>(grip_args(h));
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return GVIZ_CUDA_ERR_CUDA;
   return GVIZ_CUDA_OK;
+}
+
+// everything of a round after the force kernel
+void grip_after_forces(gvizCudaGrip *h, const GripArgs &a) {
+  const uint32_t th = h->strict ? 1u : (uint32_t)kPartThreads;
+  k_grip_part1<<<a.parts, th, 0, h->stream>>>(a);
+  k_grip_final1<<<1, 1, 0, h->stream>>>(a);
+  k_grip_part2<<<a.parts, th, 0, h->stream>>>(a);
+  k_grip_final2<<<1, 1, 0, h->stream>>>(a);
+  k_grip_apply<<<grid_for(h->n), kThreads, 0, h->stream>>>(a);
+  k_grip_part3<<<a.parts, th, 0, h->stream>>>(a);
+  k_grip_final3<<<1, 1, 0, h->stream>>>(a);
 }
 
 int gvizCudaGripRefineRound(gvizCudaGrip *h, gvizCudaGripRoundStats *stats) {
@@ -471,12 +655,8 @@ int gvizCudaGripRefineRound(gvizCudaGrip *h, gvizCudaGripRoundStats *stats) {
   double red[16] = {0};
   if (h->n) {
     const GripArgs a = grip_args(h);
-    const uint32_t sumThreads = h->strict ? 1u : (uint32_t)kSumThreads;
     k_grip_pass1<<<grid_for(h->n), kThreads, 0, h->stream>>>(a);
-    k_grip_sums1<<<1, sumThreads, 0, h->stream>>>(a);
-    k_grip_sums2<<<1, sumThreads, 0, h->stream>>>(a);
-    k_grip_apply<<<grid_for(h->n), kThreads, 0, h->stream>>>(a);
-    k_grip_stats<<<1, sumThreads, 0, h->stream>>>(a);
+    grip_after_forces(h, a);
     if (cudaGetLastError() != cudaSuccess) return GVIZ_CUDA_ERR_CUDA;
     if (cudaMemcpyAsync(red, h->d_red, sizeof red, cudaMemcpyDeviceToHost, h->stream) !=
             cudaSuccess ||
@@ -492,14 +672,60 @@ int gvizCudaGripRefineRound(gvizCudaGrip *h, gvizCudaGripRoundStats *stats) {
   return GVIZ_CUDA_OK;
 }
 
+int gvizCudaGripTimeRounds(gvizCudaGrip *h, uint32_t rounds, float *totalMs, float *forcesMs) {
+  if (!h || !totalMs) return GVIZ_CUDA_ERR_ARG;
+  if (!h->hasLayer) return GVIZ_CUDA_ERR_NOT_BEGUN;
+  GripGuard guard(h->device);
+  *totalMs = 0.f;
+  if (forcesMs) *forcesMs = 0.f;
+  if (!h->n || !rounds) return GVIZ_CUDA_OK;
+  std::vector<cudaEvent_t> ev(2 * (size_t)rounds + 2, nullptr);
+  int rc = GVIZ_CUDA_OK;
+  for (auto &e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) rc = GVIZ_CUDA_ERR_CUDA;
+  if (!rc) {
+    const GripArgs a = grip_args(h);
+    cudaEventRecord(ev[0], h->stream);
+    for (uint32_t r = 0; r < rounds; r++) {
+      cudaEventRecord(ev[2 + 2 * r], h->stream);
+      k_grip_pass1<<<grid_for(h->n), kThreads, 0, h->stream>>>(a);
+      cudaEventRecord(ev[3 + 2 * r], h->stream);
+      grip_after_forces(h, a);
+    }
+    cudaEventRecord(ev[1], h->stream);
+    if (cudaEventSynchronize(ev[1]) != cudaSuccess ||
+        cudaEventElapsedTime(totalMs, ev[0], ev[1]) != cudaSuccess)
+      rc = GVIZ_CUDA_ERR_CUDA;
+    float forces = 0.f;
+    for (uint32_t r = 0; r < rounds && !rc; r++) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, ev[2 + 2 * r], ev[3 + 2 * r]) != cudaSuccess)
+        rc = GVIZ_CUDA_ERR_CUDA;
+      forces += t;
+    }
+    if (forcesMs) *forcesMs = forces;
+  }
+  for (auto &e : ev)
+    if (e) cudaEventDestroy(e);
+  return rc;
+}
+
 int gvizCudaGripGetDecorators(gvizCudaGrip *h, double *heat, double *disp, double *oldCos) {
   if (!h || (h->V && (!heat || !disp || !oldCos))) return GVIZ_CUDA_ERR_ARG;
   GripGuard guard(h->device);
   if (!h->V) return GVIZ_CUDA_OK;
-  cudaMemcpyAsync(heat, h->d_heat, h->V * 8, cudaMemcpyDeviceToHost, h->stream);
-  cudaMemcpyAsync(disp, h->d_disp, h->V * 16, cudaMemcpyDeviceToHost, h->stream);
-  cudaMemcpyAsync(oldCos, h->d_oldCos, h->V * 8, cudaMemcpyDeviceToHost, h->stream);
+  std::vector<double> th(h->V), td(2 * h->V), tc(h->V);
+  cudaMemcpyAsync(th.data(), h->d_heat, h->V * 8, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(td.data(), h->d_disp, h->V * 16, cudaMemcpyDeviceToHost, h->stream);
+  cudaMemcpyAsync(tc.data(), h->d_oldCos, h->V * 8, cudaMemcpyDeviceToHost, h->stream);
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return GVIZ_CUDA_ERR_CUDA;
+  for (size_t n = 0; n < h->V; n++) {
+    const size_t o = h->perm[n];
+    heat[o] = th[n];
+    disp[2 * o] = td[2 * n];
+    disp[2 * o + 1] = td[2 * n + 1];
+    oldCos[o] = tc[n];
+  }
   return GVIZ_CUDA_OK;
 }
 

@@ -18,6 +18,26 @@ import numpy as np
 from . import _native as N
 
 
+def k_nearest(row_offsets, neighbors, sources, k, visible=None):
+    """GRIP's k-nearest lists (gvizCudaGripKNearest): (offsets over the
+    sources, vertices, graph distances)."""
+    L = N.lib()
+    row = np.ascontiguousarray(row_offsets, dtype=np.uint64)
+    col = np.ascontiguousarray(neighbors, dtype=np.uint32)
+    src = np.ascontiguousarray(sources, dtype=np.uint32)
+    vis = None if visible is None else np.ascontiguousarray(visible, dtype=np.uint8)
+    n = src.shape[0]
+    off = np.zeros(n + 1, np.uint64)
+    kv = np.zeros(max(1, n * int(k)), np.uint32)
+    kd = np.zeros(max(1, n * int(k)), np.uint32)
+    tot = L.gvizCudaGripKNearest(row.shape[0] - 1, N.ptr(row, C.c_uint64), N.ptr(col, C.c_uint32),
+                                 N.ptr(src, C.c_uint32), n, N.ptr(vis, C.c_uint8), int(k),
+                                 N.ptr(off, C.c_uint64), N.ptr(kv, C.c_uint32),
+                                 N.ptr(kd, C.c_uint32))
+    N.check(int(tot) if tot < 0 else 0, "gvizCudaGripKNearest")
+    return off, kv[:tot].copy(), kd[:tot].copy()
+
+
 class GripRefiner:
     def __init__(self, row_offsets, neighbors, device=0):
         self.L = N.lib()
@@ -63,6 +83,14 @@ class GripRefiner:
         st = N.GripRoundStats()
         N.check(self.L.gvizCudaGripRefineRound(self.h, C.byref(st)), "gvizCudaGripRefineRound")
         return np.array([st.maxDisplacement, st.meanDisplacement, st.meanForce, st.meanHeat])
+
+    def time_rounds(self, rounds):
+        """(total ms, force-kernel ms) of `rounds` device-resident rounds,
+        CUDA events on the handle's stream."""
+        tot, frc = C.c_float(), C.c_float()
+        N.check(self.L.gvizCudaGripTimeRounds(self.h, int(rounds), C.byref(tot), C.byref(frc)),
+                "gvizCudaGripTimeRounds")
+        return tot.value, frc.value
 
     def decorators(self):
         """Per vertex: heat, last displacement (2), previous cosine."""

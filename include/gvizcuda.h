@@ -350,8 +350,25 @@ int gvizCudaGripRefineRound(gvizCudaGrip *h, gvizCudaGripRoundStats *stats);
  * bit-identical to the reference's; 0 (default): chunked, deterministic. */
 int gvizCudaGripSetStrictReductions(gvizCudaGrip *h, int32_t strict);
 
+/* Runs `rounds` rounds on the device and times them with CUDA events on
+ * the handle's stream: all of them (totalMs) and the force kernel alone
+ * (forcesMs, may be NULL). Positions stay on the device. */
+int gvizCudaGripTimeRounds(gvizCudaGrip *h, uint32_t rounds, float *totalMs, float *forcesMs);
+
 /* Inspection: per vertex heat, last displacement (2) and previous cosine. */
 int gvizCudaGripGetDecorators(gvizCudaGrip *h, double *heat, double *disp, double *oldCos);
+
+/* GRIP's k-nearest lists for a layer (updateKNNs :970-1008 with
+ * gvizSearchKNearestScratch, src/algorithms/search/gvizKNearest.c:244-306),
+ * on all host threads: per source a breadth-first search over the whole
+ * graph in neighbour order recording the first k visible vertices reached
+ * (visible NULL: all) with their depth. Lists are packed in source order:
+ * offsets[sourceCount + 1]; vertices and distances need sourceCount * k
+ * entries. Returns the total entries or a negative code. */
+int64_t gvizCudaGripKNearest(size_t vertexCount, const uint64_t *rowOffsets,
+                             const uint32_t *neighbors, const uint32_t *sources,
+                             size_t sourceCount, const uint8_t *visible, uint32_t k,
+                             uint64_t *offsets, uint32_t *vertices, uint32_t *distances);
 
 /* ---- allocation-free speed update ------------------------------------- */
 

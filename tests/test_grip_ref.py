@@ -2,8 +2,10 @@
 src/embedders/gvizGRIPEmbedder.c compiled from its sources): layers nest,
 the finest layer holds every vertex, every k-nearest list names active
 vertices of the layer at graph distances >= 1, and rounds move the layout
-without NaNs (the reference's own invariant, :1322-1323)."""
+without NaNs (the reference's own invariant, :1322-1323). The library's own
+k-nearest search (gvizCudaGripKNearest) reproduces the reference's lists."""
 import numpy as np
+import pytest
 
 
 def test_reference_grip_layers_and_knn(ref):
@@ -30,4 +32,40 @@ def test_reference_grip_layers_and_knn(ref):
             break
         rg.next_stage()
     assert len(prev) == 100
+    rg.close()
+
+
+def _grip_graph(kind):
+    from grapher_b200 import graphs
+    if kind == "grid":
+        a, b = graphs.grid(12, 12)
+        return 144, a, b
+    if kind == "ba":
+        a, b = graphs.barabasi_albert(1500, 3, 5)
+        return 1500, a, b
+    a, b = graphs.random_connected(400, 0.02, 3)
+    return 400, np.asarray(a), np.asarray(b)
+
+
+@pytest.mark.parametrize("kind", ["grid", "ba", "random"])
+def test_k_nearest_matches_reference_on_every_layer(ref, kind):
+    """gvizCudaGripKNearest (host, all threads) gives the reference's
+    refinement lists (k = 128, the layer's vertices visible) entry for
+    entry on every layer."""
+    from grapher_b200 import graphs
+    from grapher_b200.grip import k_nearest
+    V, a, b = _grip_graph(kind)
+    row, col = graphs.to_csr(V, a, b)
+    rg = ref.create_grip(V, a, b)
+    rg.begin()
+    while True:
+        act = rg.active()
+        vis = np.zeros(V, np.uint8)
+        vis[act] = 1
+        off, kv, kd = rg.knn()
+        o2, v2, d2 = k_nearest(row, col, act, 128, vis)
+        assert np.array_equal(off, o2) and np.array_equal(kv, v2) and np.array_equal(kd, d2)
+        if rg.layer == 0:
+            break
+        rg.next_stage()
     rg.close()
