@@ -203,11 +203,22 @@ __global__ __launch_bounds__(kSumThreads) void k_grip_part1(GripArgs a) {
   block_partial<4>(acc, a.part, tmp);
 }
 
-__global__ void k_grip_final1(GripArgs a) {
+// the block partials, loaded by the whole block into shared memory so that
+// one thread can add them in order without waiting on each load
+__device__ __forceinline__ const double *stage_parts(const GripArgs &a, double *sp) {
+  for (uint32_t j = threadIdx.x; j < a.parts * 4; j += blockDim.x) sp[j] = a.part[j];
+  __syncthreads();
+  return sp;
+}
+
+__global__ __launch_bounds__(kPartThreads) void k_grip_final1(GripArgs a) {
+  __shared__ double sp[kMaxParts * 4];
+  const double *part = stage_parts(a, sp);
+  if (threadIdx.x) return;
   double acc[4];
-  for (int k = 0; k < 4; k++) acc[k] = a.part[k];
+  for (int k = 0; k < 4; k++) acc[k] = part[k];
   for (uint32_t b = 1; b < a.parts; b++)
-    for (int k = 0; k < 4; k++) acc[k] += a.part[b * 4 + k];
+    for (int k = 0; k < 4; k++) acc[k] += part[b * 4 + k];
   const double inv = 1.0 / (double)a.n;
   a.red[0] = acc[0] * inv;
   a.red[1] = acc[1] * inv;
@@ -236,11 +247,14 @@ __global__ __launch_bounds__(kSumThreads) void k_grip_part2(GripArgs a) {
   block_partial<2>(acc, a.part, tmp);
 }
 
-__global__ void k_grip_final2(GripArgs a) {
-  double L = a.part[0], I = a.part[1];
+__global__ __launch_bounds__(kPartThreads) void k_grip_final2(GripArgs a) {
+  __shared__ double sp[kMaxParts * 4];
+  const double *part = stage_parts(a, sp);
+  if (threadIdx.x) return;
+  double L = part[0], I = part[1];
   for (uint32_t b = 1; b < a.parts; b++) {
-    L += a.part[b * 2];
-    I += a.part[b * 2 + 1];
+    L += part[b * 2];
+    I += part[b * 2 + 1];
   }
   const bool rotate = a.n >= 3 && !(fabs(I) < kEps);
   a.red[4] = rotate ? L / I : 0.0;
@@ -292,11 +306,14 @@ __global__ __launch_bounds__(kSumThreads) void k_grip_part3(GripArgs a) {
   if (threadIdx.x == 0) a.part[blockIdx.x * 4] = mx;
 }
 
-__global__ void k_grip_final3(GripArgs a) {
-  double mx = a.part[0], acc[3] = {a.part[1], a.part[2], a.part[3]};
+__global__ __launch_bounds__(kPartThreads) void k_grip_final3(GripArgs a) {
+  __shared__ double sp[kMaxParts * 4];
+  const double *part = stage_parts(a, sp);
+  if (threadIdx.x) return;
+  double mx = part[0], acc[3] = {part[1], part[2], part[3]};
   for (uint32_t b = 1; b < a.parts; b++) {
-    mx = fmax(mx, a.part[b * 4]);
-    for (int k = 0; k < 3; k++) acc[k] += a.part[b * 4 + 1 + k];
+    mx = fmax(mx, part[b * 4]);
+    for (int k = 0; k < 3; k++) acc[k] += part[b * 4 + 1 + k];
   }
   a.red[6] = mx;
   a.red[7] = a.n ? acc[0] / a.n : 0.0;
@@ -640,12 +657,12 @@ int gvizCudaGripSetLayer(gvizCudaGrip *h, size_t layer, const uint32_t *active,
 void grip_after_forces(gvizCudaGrip *h, const GripArgs &a) {
   const uint32_t th = h->strict ? 1u : (uint32_t)kPartThreads;
   k_grip_part1<<<a.parts, th, 0, h->stream>>>(a);
-  k_grip_final1<<<1, 1, 0, h->stream>>>(a);
+  k_grip_final1<<<1, kPartThreads, 0, h->stream>>>(a);
   k_grip_part2<<<a.parts, th, 0, h->stream>>>(a);
-  k_grip_final2<<<1, 1, 0, h->stream>>>(a);
+  k_grip_final2<<<1, kPartThreads, 0, h->stream>>>(a);
   k_grip_apply<<<grid_for(h->n), kThreads, 0, h->stream>>>(a);
   k_grip_part3<<<a.parts, th, 0, h->stream>>>(a);
-  k_grip_final3<<<1, 1, 0, h->stream>>>(a);
+  k_grip_final3<<<1, kPartThreads, 0, h->stream>>>(a);
 }
 
 int gvizCudaGripRefineRound(gvizCudaGrip *h, gvizCudaGripRoundStats *stats) {
