@@ -216,12 +216,17 @@ int gvizCudaForceRepulsion(gvizCudaForce *h, double *out);
 int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
                                    uint64_t *warpNodeVisits);
 
-/* With the learned correction on: the MLP rows one force evaluation runs,
- * shared rows (one per warp and cell, evaluated at the centroid of the
- * warp's accepting targets) and per-target rows, and (laneRowCause[3], may
- * be NULL) why per-target rows were used: fewer than three targets accepted
- * the cell, their spread was too wide, or the cell fails the opening test
- * seen from their centroid. Zeros when the correction is off. */
+/* With the learned correction on: the MLP rows one force evaluation runs.
+ * Per-target walk (farCellGroups 0): shared rows (one per warp and cell,
+ * evaluated at the centroid of the warp's accepting targets) and per-target
+ * rows, and (laneRowCause[3], may be NULL) why per-target rows were used:
+ * fewer than two targets accepted the cell, their spread was too wide, or
+ * the cell fails the opening test seen from their centroid. Cell-group walk
+ * (farCellGroups 1): groupRows = one row per group and accepted cell,
+ * laneRows = 0, and laneRowCause = {node visits of the longest group walk,
+ * that group's target count << 32 | the FP32 bits of its bounding-box
+ * extent, targets walked over all groups}. Zeros when the correction is
+ * off. */
 int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows,
                               uint64_t *laneRows, uint64_t *laneRowCause);
 
