@@ -70,6 +70,7 @@ def _compile(src: str, extra: list[str], hdr: float, verbose: bool) -> str:
 
 
 ADAPTER_SRC = os.path.join(HERE, "gviz", "gvizCudaForceEmbedder.c")
+GRIP_ADAPTER_SRC = os.path.join(HERE, "gviz", "gvizCudaGripEmbedder.c")
 ADAPTER_LIB = os.path.join(LIBDIR, "libgvizcuda_gviz.so")
 
 
@@ -80,11 +81,13 @@ def build_gviz_adapter(gviz_include: str | None = None) -> str | None:
     if not os.path.isdir(inc):
         return None
     if os.path.exists(ADAPTER_LIB) and os.path.getmtime(ADAPTER_LIB) >= max(
-            os.path.getmtime(ADAPTER_SRC), os.path.getmtime(LIB),
-            os.path.getmtime(os.path.join(INCLUDE, "gvizCudaForceEmbedder.h"))):
+            os.path.getmtime(ADAPTER_SRC), os.path.getmtime(GRIP_ADAPTER_SRC),
+            os.path.getmtime(LIB),
+            os.path.getmtime(os.path.join(INCLUDE, "gvizCudaForceEmbedder.h")),
+            os.path.getmtime(os.path.join(INCLUDE, "gvizCudaGripEmbedder.h"))):
         return ADAPTER_LIB
     cmd = ["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-include", "stdint.h",
-           "-I" + INCLUDE, "-I" + inc, ADAPTER_SRC, "-o", ADAPTER_LIB,
+           "-I" + INCLUDE, "-I" + inc, ADAPTER_SRC, GRIP_ADAPTER_SRC, "-o", ADAPTER_LIB,
            "-L" + LIBDIR, "-lgvizcuda", "-Wl,-rpath,$ORIGIN"]
     out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:

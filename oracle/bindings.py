@@ -365,6 +365,21 @@ class RefGrip:
         self.L.ref_grip_get_decorators(self.h, _ptr(heat, D), _ptr(disp, D), _ptr(oc, D))
         return heat, disp, oc
 
+    def state_ptr(self):
+        self.L.ref_grip_state.restype = C.c_void_p
+        return self.L.ref_grip_state(self.h)
+
+    def invoke_refine(self):
+        """the "grip.refineRound" action by name (whatever handler holds it)"""
+        return int(self.L.ref_grip_invoke_refine(self.h))
+
+    def last_stats(self):
+        """(lastRoundStats as an array, currRound)"""
+        self.L.ref_grip_last_stats.restype = C.c_size_t
+        st = np.zeros(3)
+        r = int(self.L.ref_grip_last_stats(self.h, _ptr(st, D)))
+        return st, r
+
     def close(self):
         if self.h:
             self.L.ref_grip_release(self.h)

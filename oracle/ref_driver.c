@@ -578,3 +578,19 @@ void ref_grip_release(refGrip *r) {
   gvizGraphRelease(&r->g);
   free(r);
 }
+
+/* the state, for gviz-side glue that attaches to it */
+void *ref_grip_state(refGrip *r) { return &r->s; }
+
+/* "grip.refineRound" through the action registry, as a front-end invokes it */
+int ref_grip_invoke_refine(refGrip *r) {
+  return gvizEmbeddedGraphInvokeAction((gvizEmbeddedGraph *)&r->s, "grip.refineRound", NULL);
+}
+
+/* lastRoundStats {max, mean displacement, mean force} and currRound */
+size_t ref_grip_last_stats(refGrip *r, double *stats) {
+  stats[0] = r->s.lastRoundStats.maxDisplacement;
+  stats[1] = r->s.lastRoundStats.meanDisplacement;
+  stats[2] = r->s.lastRoundStats.meanForce;
+  return r->s.currRound;
+}

@@ -226,3 +226,24 @@ def test_run_batch_rejects_mixed_configurations(ref, glue):
     assert a[0].state()["iteration"] == 0
     for r in a + b:
         r.close()
+
+
+def test_grip_action_switch_bit_identical(ref, glue):
+    """gvizCudaGripAttach takes over "grip.refineRound": a GRIP state refined
+    through the action on the GPU (strict reductions) stays bit-identical to
+    a twin refined by the reference on the CPU, across every layer (gviz's
+    own NextStage places each layer and builds its k-nearest lists), with the
+    same lastRoundStats and round counter; after detach, CPU rounds on it
+    continue identically (the decorators were written back).
+
+    The check runs in a fresh process (tests/grip_glue_check.py): in a
+    process that has already run batched force Runs, two identical reference
+    GRIP states were seen to build different k-nearest lists in NextStage,
+    without the GPU involved and with no invalid access reported by
+    AddressSanitizer in the reference, the glue or this library's host code."""
+    import subprocess
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "grip_glue_check.py")],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.strip().splitlines()[-1] == "OK", out.stdout[-2000:]

@@ -28,6 +28,21 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_glue_library_exports_its_headers():
+    """The gviz-side glue (built only where gviz's headers are) exports every
+    entry point of include/gvizCudaForceEmbedder.h and gvizCudaGripEmbedder.h."""
+    import subprocess
+    glue = os.path.join(ROOT, "grapher_b200", "lib", "libgvizcuda_gviz.so")
+    if not os.path.exists(glue):
+        pytest.skip("gviz glue not built here")
+    out = subprocess.run(["nm", "-D", "--defined-only", glue], capture_output=True,
+                         text=True).stdout
+    defined = set(line.split()[-1] for line in out.splitlines() if line.strip())
+    for header in ("gvizCudaForceEmbedder.h", "gvizCudaGripEmbedder.h"):
+        missing = [n for n in _declared(header) if n not in defined]
+        assert not missing, (header, missing)
+
+
 def test_python_binding_covers_the_header():
     from grapher_b200 import _native
     names = set(_declared("gvizcuda.h"))
