@@ -194,11 +194,30 @@ void enqueue_step(gvizCudaForce *h) {
                   cudaMemcpyDeviceToDevice, st);
   const bool f64 = h->params.precision == GVIZ_CUDA_FP64;
   const bool bh = h->params.barnesHutEnabled != 0;
-  if (bh) enqueue_tree_build(h);
-  if (f64)
-    enqueue_attraction_f64(h);
-  else
-    enqueue_attraction_f32(h);
+  // attraction reads positions only and its forces are first read by the
+  // repulsion pass: with a tree to build it runs on the side stream,
+  // overlapping the build (in order while profiling, so that each kernel
+  // keeps its own time)
+  const bool overlap = bh && h->side && !h->profiling;
+  if (overlap) {
+    cudaEventRecord(h->evFork, st);
+    cudaStreamWaitEvent(h->side, h->evFork, 0);
+    h->stream = h->side;
+    if (f64)
+      enqueue_attraction_f64(h);
+    else
+      enqueue_attraction_f32(h);
+    h->stream = st;
+    cudaEventRecord(h->evJoin, h->side);
+    enqueue_tree_build(h);
+    cudaStreamWaitEvent(st, h->evJoin, 0);
+  } else {
+    if (bh) enqueue_tree_build(h);
+    if (f64)
+      enqueue_attraction_f64(h);
+    else
+      enqueue_attraction_f32(h);
+  }
   if (bh) {
     if (f64)
       enqueue_walk_f64(h);
@@ -483,6 +502,15 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
     return GVIZ_CUDA_ERR_CUDA;
   }
   h->ownStream = true;
+  if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming) != cudaSuccess) {
+    if (h->side) cudaStreamDestroy(h->side);
+    if (h->evFork) cudaEventDestroy(h->evFork);
+    h->side = nullptr;
+    h->evFork = nullptr;
+    h->evJoin = nullptr;  // without them the attraction runs in order
+  }
   const size_t Vs = V ? V : 1;
   const size_t C = h->nChunks ? h->nChunks : 1;
   h->maxNodes = 3 * Vs + 64;
@@ -646,6 +674,12 @@ void gvizCudaForceDestroy(gvizCudaForce *h) {
   free_all(h);
   mlp_free(h);
   far_side_free(h);
+  if (h->side) {
+    cudaStreamSynchronize(h->side);
+    cudaStreamDestroy(h->side);
+  }
+  if (h->evFork) cudaEventDestroy(h->evFork);
+  if (h->evJoin) cudaEventDestroy(h->evJoin);
   if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
   free(h->h_graphOff);
   free(h->h_meanDegPlusOne);

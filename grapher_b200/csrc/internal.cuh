@@ -80,6 +80,10 @@ struct ChunkStat {
 struct gvizCudaForce {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // attraction depends on positions only: it runs on `side`, forked from
+  // and joined back to `stream` around the tree build (null: in order)
+  cudaStream_t side = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   bool ownStream = false;
   int model = 0;
   size_t V = 0, E2 = 0, G = 1;
