@@ -497,7 +497,18 @@ refGrip *ref_grip_create(size_t V, const uint32_t *ea, const uint32_t *eb, size_
 }
 
 int ref_grip_init_result(refGrip *r) { return r->initRes; }
-void ref_grip_begin(refGrip *r) { gvizGRIPEmbedderBegin(&r->s); }
+/* gvizGRIPEmbedderInit allocates the BFS stamp array without clearing it
+ * (src/embedders/gvizGRIPEmbedder.c:253) and Begin's MIS filtration reads it
+ * (:511 gripPickFarCandidate, :603 verticesWithinRadius) as if every stamp
+ * were older than the first epoch, so leftover heap contents could mark
+ * vertices visited and two identical states could build different
+ * filtrations. Zeroed first, as the epoch scheme assumes (Begin clears it
+ * the same way when the epoch wraps, :605-607). */
+void ref_grip_begin(refGrip *r) {
+  if (r->s.radiusBfsStamp)
+    memset(r->s.radiusBfsStamp, 0, sizeof(size_t) * gvizGraphSize(&r->g));
+  gvizGRIPEmbedderBegin(&r->s);
+}
 void ref_grip_next_stage(refGrip *r) { gvizGRIPEmbedderNextStage(&r->s); }
 size_t ref_grip_layer(refGrip *r) { return r->s.currLayer; }
 size_t ref_grip_layer_count(refGrip *r) { return r->s.layerCount; }

@@ -236,11 +236,11 @@ def test_grip_action_switch_bit_identical(ref, glue):
     same lastRoundStats and round counter; after detach, CPU rounds on it
     continue identically (the decorators were written back).
 
-    The check runs in a fresh process (tests/grip_glue_check.py): in a
-    process that has already run batched force Runs, two identical reference
-    GRIP states were seen to build different k-nearest lists in NextStage,
-    without the GPU involved and with no invalid access reported by
-    AddressSanitizer in the reference, the glue or this library's host code."""
+    The check runs in a fresh process (tests/grip_glue_check.py), apart
+    from the glue's attach registry of the other tests. Both twins clear the
+    BFS stamps the reference allocates without clearing
+    (src/embedders/gvizGRIPEmbedder.c:253) before Begin, so they build the
+    same filtration (tests/test_grip_ref.py pins that)."""
     import subprocess
     import sys
     out = subprocess.run([sys.executable, os.path.join(ROOT, "tests", "grip_glue_check.py")],

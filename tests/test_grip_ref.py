@@ -69,3 +69,36 @@ def test_k_nearest_matches_reference_on_every_layer(ref, kind):
             break
         rg.next_stage()
     rg.close()
+
+
+def test_identical_states_stay_identical_after_heap_reuse(ref):
+    """Two GRIP states built from the same graph take the same filtration,
+    k-nearest lists and rounds on every layer, also after a released state
+    has left its BFS stamps on the heap: the driver clears the stamp array
+    the reference allocates without clearing
+    (src/embedders/gvizGRIPEmbedder.c:253) before Begin reads it."""
+    from grapher_b200 import graphs
+    a, b = graphs.barabasi_albert(600, 3, 5)
+    for _ in range(3):    # states whose freed stamps hold small epochs
+        old = ref.create_grip(600, a, b)
+        old.begin()
+        old.close()
+    s1, s2 = ref.create_grip(600, a, b), ref.create_grip(600, a, b)
+    s1.begin()
+    s2.begin()
+    layers = 0
+    while True:
+        assert np.array_equal(s1.active(), s2.active())
+        for x, y in zip(s1.knn(), s2.knn()):
+            assert np.array_equal(x, y)
+        for _ in range(2):
+            assert np.array_equal(s1.refine(), s2.refine())
+            assert np.array_equal(s1.positions(), s2.positions())
+        layers += 1
+        if s1.layer == 0:
+            break
+        s1.next_stage()
+        s2.next_stage()
+    assert layers >= 3
+    s1.close()
+    s2.close()
