@@ -16,7 +16,12 @@ normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
 The plain walk runs at theta = 0.5; the learned walk (the cell-group walk:
 one warp per group of <= 32 targets cut from the tree, one network row per
 accepted cell) at the largest theta of 1.3, 1.25, ..., 0.6 whose error is
-not above the plain walk's. ``value`` is the learned path's iterations/s;
+not above the plain walk's. It is judged twice: alone, and with hub targets
+(the V / 1024 heaviest vertices take the plain monopole walk at theta = 0.35,
+since LinLog's force on a vertex scales with its mass); each at its own
+largest qualifying theta, the faster of the two (10 timed steps each, from
+one saved state) is the learned configuration (--hub-targets fixes the
+count instead). ``value`` is the learned path's iterations/s;
 the plain path's are in ``plain``. Both are timed from the same saved
 layout state.
 rmat4m_learned: the same comparison on an R-MAT graph, scale 22 (4,194,304
@@ -347,8 +352,11 @@ def replica_value(ms_max, steps, world):
 LEARNED_THETAS = tuple(round(1.3 - 0.05 * i, 2) for i in range(15))  # 1.3 ... 0.6
 LEARNED_SPREAD = 1.0
 LEARNED_CELL_GROUPS = 1  # the cell-group walk: one warp per tree-cut group of <= 32 targets
+HUB_SHARE = 1024         # hub targets: the V / HUB_SHARE heaviest vertices
+HUB_THETA = 0.35         # their plain walk's opening threshold
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
 JUDGE_VERTICES = 65536
+CHOICE_STEPS = 10        # timed steps per candidate when choosing the learned config
 
 
 def force_error(lay, targets, exact):
@@ -361,10 +369,20 @@ def force_error(lay, targets, exact):
             float(np.sqrt(np.mean((d / np.maximum(n, 1e-300)) ** 2))))
 
 
-def learned_setup(lay, w):
+def learned_params(linfo):
+    """set_params arguments of the chosen learned configuration."""
+    return dict(theta=linfo["learned_theta"], farField=1, farGroupSpread=LEARNED_SPREAD,
+                farCellGroups=LEARNED_CELL_GROUPS, farHubTargets=linfo["hub_targets"],
+                farHubTheta=HUB_THETA)
+
+
+def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     """Trains the far-field MLP on this layout's own harvested pairs, judges
-    plain theta = 0.5 and the learned walk against exact FP64 repulsion on
-    the same positions and picks the learned theta (see the module text)."""
+    plain theta = 0.5 and the learned walk, without and with hub targets,
+    against exact FP64 repulsion on the same positions, and picks the
+    learned configuration (see the module text). `reduce` takes the maximum
+    of a time over ranks, so that every rank picks the same one;
+    `hub_targets` other than "auto" fixes the hub count instead."""
     from grapher_b200.farfield import FarFieldModel, harvest_training_set
     rng = np.random.default_rng(SEED)
     t0 = time.perf_counter()
@@ -385,18 +403,33 @@ def learned_setup(lay, w):
     lay.set_params(theta=w.spec["theta"], farField=0)
     e_plain, e_plain_pv = force_error(lay, targets, exact)
     model.attach(lay)
-    table = {}
-    chosen = None
-    for th in LEARNED_THETAS:
-        lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD,
-                       farCellGroups=LEARNED_CELL_GROUPS)
-        e, e_pv = force_error(lay, targets, exact)
-        table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
-        if chosen is None and e <= e_plain:
-            chosen = th
-    if chosen is None:
-        chosen = LEARNED_THETAS[-1]
-    lay.set_params(theta=w.spec["theta"], farField=0, farCellGroups=0)
+    fixed = hub_targets != "auto"
+    hubs = min(int(hub_targets), w.V) if fixed else w.V // HUB_SHARE
+    tables, picks = {}, {}
+    for k in sorted({0, hubs}):
+        table, pick = {}, None
+        for th in LEARNED_THETAS:
+            lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD,
+                           farCellGroups=LEARNED_CELL_GROUPS, farHubTargets=k,
+                           farHubTheta=HUB_THETA)
+            e, e_pv = force_error(lay, targets, exact)
+            table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
+            if pick is None and e <= e_plain:
+                pick = th
+        tables[k], picks[k] = table, (pick if pick is not None else LEARNED_THETAS[-1])
+    # the faster of the two qualifying configurations, from the same state
+    x_s, fa2_s = lay.positions(), lay.fa2_state()
+    times = {}
+    for k in sorted({0, hubs}):
+        lay.set_params(theta=picks[k], farField=1, farGroupSpread=LEARNED_SPREAD,
+                       farCellGroups=LEARNED_CELL_GROUPS, farHubTargets=k, farHubTheta=HUB_THETA)
+        lay.time_steps(3)
+        times[k] = reduce(lay.time_steps(CHOICE_STEPS)) / CHOICE_STEPS
+        lay.set_positions(x_s)
+        lay.set_fa2_state(*fa2_s)
+    k_best = hubs if (fixed or times[hubs] < times[0]) else 0
+    chosen, table = picks[k_best], tables[k_best]
+    lay.set_params(theta=w.spec["theta"], farField=0, farCellGroups=0, farHubTargets=0)
     plain_table = {}
     for th in (0.3, 0.4, 0.5, 0.6, 0.8, 1.0, 1.2):
         lay.set_params(theta=th)
@@ -407,7 +440,13 @@ def learned_setup(lay, w):
             "train_loss_first_last": [float(losses[0]), float(losses[-1])],
             "judge_vertices": int(len(targets)), "plain_rms_err": e_plain,
             "plain_rms_rel_err_per_vertex": e_plain_pv, "learned_theta": chosen,
+            "hub_targets": k_best, "hub_theta": HUB_THETA,
             "learned_errors": table, "plain_errors": plain_table,
+            "hub_choice": "fixed" if fixed else "auto",
+            "candidates": [{"hub_targets": k, "theta": picks[k], "ms_per_step": times[k],
+                            "rms_err": tables[k][str(picks[k])]["rms_err"]}
+                           for k in sorted({0, hubs})],
+            "learned_errors_by_hub_targets": {str(k): tables[k] for k in sorted({0, hubs})},
             "group_spread": LEARNED_SPREAD,
             "walk": "cell groups" if LEARNED_CELL_GROUPS else "per target"}
     return model, info
@@ -423,7 +462,8 @@ def error_trajectory(lay, w, linfo, chunks=5, every=20):
     for name, th, ff in (("learned", linfo["learned_theta"], 1), ("plain", w.spec["theta"], 0)):
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
-        lay.set_params(theta=th, farField=ff, farCellGroups=LEARNED_CELL_GROUPS if ff else 0)
+        lay.set_params(**(learned_params(linfo) if ff else
+                          dict(theta=th, farField=0, farCellGroups=0, farHubTargets=0)))
         errs = []
         for c in range(chunks):
             lay.time_steps(every)
@@ -431,7 +471,7 @@ def error_trajectory(lay, w, linfo, chunks=5, every=20):
             errs.append(force_error(lay, targets, exact)[0])
         out[name] = {"theta": th, "iterations": [every * (c + 1) for c in range(chunks)],
                      "rms_err": errs}
-    lay.set_params(theta=linfo["learned_theta"], farField=1, farCellGroups=LEARNED_CELL_GROUPS)
+    lay.set_params(**learned_params(linfo))
     return out
 
 
@@ -566,6 +606,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ba1m_learned", choices=sorted(SPECS) + ["grip_ba200k"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--hub-targets", default="auto",
+                    help="learned workloads: hub targets of the learned walk; 'auto' (default) "
+                         "times 0 and V/1024 at their own largest qualifying theta and keeps "
+                         "the faster, a number fixes the count")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == "grip_ba200k":
@@ -606,7 +650,7 @@ def main():
 
     model, linfo, plain_line = None, None, None
     if learned:
-        model, linfo = learned_setup(lay, w)
+        model, linfo = learned_setup(lay, w, max_over_ranks, args.hub_targets)
         x_s, (sf_s, sp_s, ef_s) = lay.positions(), lay.fa2_state()
         # plain theta = 0.5 from the saved state
         lay.set_params(theta=w.spec["theta"], farField=0)
@@ -623,8 +667,7 @@ def main():
         # then the learned walk from the same state
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
-        lay.set_params(theta=linfo["learned_theta"], farField=1, farGroupSpread=LEARNED_SPREAD,
-                       farCellGroups=LEARNED_CELL_GROUPS)
+        lay.set_params(**learned_params(linfo))
         lay.time_steps(args.warmup)
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
@@ -715,6 +758,7 @@ def main():
                                rms_err=linfo["learned_errors"][str(linfo["learned_theta"])]["rms_err"])
         line["plain"] = plain_line
         line["config"]["theta"] = {"plain": w.spec["theta"], "learned": linfo["learned_theta"]}
+        line["config"]["hub_targets"] = linfo["hub_targets"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

@@ -52,6 +52,8 @@ class ForceParams(C.Structure):
         ("farField", C.c_int32),
         ("farGroupSpread", C.c_double),
         ("farCellGroups", C.c_int32),
+        ("farHubTargets", C.c_int32),
+        ("farHubTheta", C.c_double),
     ]
 
 

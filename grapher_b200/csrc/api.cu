@@ -363,6 +363,8 @@ void gvizCudaForceDefaultParams(gvizCudaForceParams *p) {
   p->farField = 0;
   p->farGroupSpread = 1.0;
   p->farCellGroups = 0;
+  p->farHubTargets = 0;
+  p->farHubTheta = 0.35;
 }
 
 int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
@@ -680,10 +682,47 @@ void gvizCudaForceDestroy(gvizCudaForce *h) {
   }
   if (h->evFork) cudaEventDestroy(h->evFork);
   if (h->evJoin) cudaEventDestroy(h->evJoin);
+  cudaFree(h->d_farHubs);
+  cudaFree(h->d_farHubOut);
   if (h->ownStream && h->stream) cudaStreamDestroy(h->stream);
   free(h->h_graphOff);
   free(h->h_meanDegPlusOne);
   delete h;
+}
+
+// The `count` heaviest vertices (model mass; ties to the lower id), in id
+// order, as the learned walk's hub targets.
+static int select_hubs(gvizCudaForce *h, uint32_t count) {
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  cudaFree(h->d_farHubs);
+  cudaFree(h->d_farHubOut);
+  h->d_farHubs = nullptr;
+  h->d_farHubOut = nullptr;
+  h->nFarHubs = 0;
+  if (count == 0) return GVIZ_CUDA_OK;
+  std::vector<double> mass(h->V);
+  if (cudaMemcpy(mass.data(), h->d_mass, h->V * sizeof(double), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return GVIZ_CUDA_ERR_CUDA;
+  std::vector<uint32_t> ids(h->V);
+  for (size_t i = 0; i < h->V; i++) ids[i] = (uint32_t)i;
+  auto heavier = [&](uint32_t a, uint32_t b) {
+    return mass[a] > mass[b] || (mass[a] == mass[b] && a < b);
+  };
+  std::nth_element(ids.begin(), ids.begin() + (count - 1), ids.end(), heavier);
+  std::sort(ids.begin(), ids.begin() + count);
+  // the ids, then the walk's hub counter
+  if (cudaMalloc(&h->d_farHubs, (count + 1) * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&h->d_farHubOut, count * sizeof(double2)) != cudaSuccess) {
+    cudaFree(h->d_farHubs);
+    h->d_farHubs = nullptr;
+    return GVIZ_CUDA_ERR_ALLOC;
+  }
+  if (cudaMemcpy(h->d_farHubs, ids.data(), count * sizeof(uint32_t), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return GVIZ_CUDA_ERR_CUDA;
+  h->nFarHubs = count;
+  return GVIZ_CUDA_OK;
 }
 
 int gvizCudaForceSetParams(gvizCudaForce *h, const gvizCudaForceParams *p) {
@@ -697,9 +736,15 @@ int gvizCudaForceSetParams(gvizCudaForce *h, const gvizCudaForceParams *p) {
   if (p->farField && (!h->d_mlp || p->precision != GVIZ_CUDA_FP32 || !p->barnesHutEnabled))
     return set_err(h, GVIZ_CUDA_ERR_ARG);
   if (!(p->farGroupSpread >= 0.0 && p->farGroupSpread <= 1.0) ||
-      (p->farCellGroups != 0 && p->farCellGroups != 1))
+      (p->farCellGroups != 0 && p->farCellGroups != 1) || p->farHubTargets < 0 ||
+      (p->farHubTargets > 0 && !(p->farHubTheta > 0.0 && p->farHubTheta < INFINITY)))
     return set_err(h, GVIZ_CUDA_ERR_ARG);
   DeviceGuard guard(h->device);
+  const uint32_t hubs = (uint32_t)std::min<size_t>((size_t)p->farHubTargets, h->V);
+  if (hubs != h->nFarHubs) {
+    const int rc = select_hubs(h, hubs);
+    if (rc) return set_err(h, rc);
+  }
   const bool radiusChanged = p->preventOverlap != h->params.preventOverlap ||
                              p->radiusBase != h->params.radiusBase ||
                              p->radiusPerDegree != h->params.radiusPerDegree;

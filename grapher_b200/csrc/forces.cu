@@ -866,6 +866,183 @@ __global__ __launch_bounds__(kCellThreads, kCellBlocksPerSM) void k_walk_f32_cel
   }
 }
 
+// ---------------------------------------------------------------------------
+// Hub targets of the learned walk. LinLog's pair force scales with the
+// target's mass, so the heaviest targets carry most of the force and their
+// errors dominate the force-weighted RMS error. They are walked again with
+// the plain monopole method at a tighter opening threshold (farHubTheta) and
+// their learned results replaced. One warp walks one hub (hubs are drawn
+// from a counter) through a first-in first-out ring of preorder ranges
+// [lo, hi) of consecutive sibling subtrees in shared memory: a lane takes
+// kHubTake entries per round, loads their first nodes together, tests them
+// (leaf: pair term; cell: accepted, or opened) and yields at most two
+// entries for each, the opened cell's children [lo + 1, next) and the
+// remaining siblings [next, hi), appended in lane order after a warp scan.
+// An entry that finds the ring full is walked to its end by its lane. A
+// hub's sum depends only on the hub, so it is deterministic. The walk is
+// bound by the latency of the node loads along the ring, not by bandwidth.
+// ---------------------------------------------------------------------------
+constexpr int kHubThreads = 128;
+constexpr uint32_t kHubRing = 1024;  // ring entries per warp
+constexpr int kHubTake = 2;          // entries a lane takes per round
+
+struct FarHubArgs {
+  WalkArgs w;
+  const uint32_t *hubs;  // vertex ids
+  uint32_t *counter;     // hubs drawn so far (reset before every launch)
+  double2 *out;          // per hub: its plain repulsion
+  uint32_t nHubs;
+  float sizeScale;       // (theta / farHubTheta)^2: node sizes hold (2h/theta)^2
+};
+
+struct HubTarget {
+  uint32_t v;
+  float xh, xl, yh, yl, m, r;
+};
+
+struct HubNode {
+  float4 n0, n1;  // {x hi, y hi, x lo, y lo}, {mass, size, next, info}
+};
+
+__device__ __forceinline__ HubNode hub_load(const FarHubArgs &a, uint32_t cur) {
+  HubNode n;
+  n.n0 = __ldg(reinterpret_cast<const float4 *>(a.w.nodes + cur));
+  n.n1 = __ldg(reinterpret_cast<const float4 *>(a.w.nodes + cur) + 1);
+  return n;
+}
+
+// Tests node `cur` for the hub: adds its term when it is a leaf other than
+// the hub or an accepted cell; returns true when the cell is opened. `next`
+// is the node after its subtree.
+template <int MODEL, bool OVERLAP>
+__device__ __forceinline__ bool hub_visit(const FarHubArgs &a, const HubTarget &t, uint32_t cur,
+                                          const HubNode &n, Kahan &kx, Kahan &ky,
+                                          uint32_t &next) {
+  const float nmass = n.n1.x, nsize = n.n1.y;
+  const int32_t nnext = __float_as_int(n.n1.z), ninfo = __float_as_int(n.n1.w);
+  next = max((uint32_t)nnext, cur + 1u);
+  if (nmass == 0.0f) return false;
+  const float dx = (n.n0.x - t.xh) + (n.n0.z - t.xl);
+  const float dy = (n.n0.y - t.yh) + (n.n0.w - t.yl);
+  const float d2 = dx * dx + dy * dy;
+  const bool isLeaf = ninfo >= 0;
+  if (isLeaf ? (uint32_t)ninfo != t.v : nsize * a.sizeScale < d2) {
+    float fx, fy;
+    rep_term<MODEL, OVERLAP>(dx, dy, d2, t.m, nmass, t.r + (isLeaf ? nsize : 0.0f), a.w.num,
+                             a.w.overlapC, t.v, isLeaf ? (uint32_t)ninfo : t.v, fx, fy);
+    kx.add(fx);
+    ky.add(fy);
+    return false;
+  }
+  return !isLeaf;
+}
+
+// The stackless walk of [lo, hi) by one lane (every step moves forward).
+template <int MODEL, bool OVERLAP>
+__device__ __forceinline__ void hub_walk_range(const FarHubArgs &a, const HubTarget &t,
+                                               uint32_t lo, uint32_t hi, Kahan &kx, Kahan &ky) {
+  uint32_t cur = lo;
+  while (cur < hi) {
+    uint32_t next;
+    cur = hub_visit<MODEL, OVERLAP>(a, t, cur, hub_load(a, cur), kx, ky, next) ? cur + 1u : next;
+  }
+}
+
+template <int MODEL, bool OVERLAP>
+__global__ __launch_bounds__(kHubThreads) void k_walk_f32_hubs(FarHubArgs a) {
+  __shared__ uint2 ring[kHubThreads / 32][kHubRing];
+  const uint32_t lane = threadIdx.x & 31u;
+  uint2 *q = ring[threadIdx.x >> 5];
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0u) i = atomicAdd(a.counter, 1u);
+    i = __shfl_sync(0xffffffffu, i, 0);
+    if (i >= a.nHubs) return;
+    HubTarget t;
+    t.v = a.hubs[i];
+    const uint32_t g = a.w.gid ? a.w.gid[t.v] : 0u;
+    if (a.w.active && a.w.active[g] == 0u) continue;  // the whole warp
+    const uint32_t base = a.w.graphBase[g];
+    const uint32_t end = min(base + a.w.rootT[g], a.w.maxNodes);
+    const double2 p = a.w.pos[t.v];
+    ds_split(p.x, t.xh, t.xl);
+    ds_split(p.y, t.yh, t.yl);
+    t.m = a.w.massF[t.v];
+    t.r = OVERLAP ? a.w.radiusF[t.v] : 0.0f;
+    Kahan kx, ky;
+    // head, tail: entries taken and appended so far (warp-uniform)
+    uint32_t head = 0, tail = base < end ? 1u : 0u;
+    if (lane == 0u) q[0] = make_uint2(base, end);
+    __syncwarp();
+    while (head < tail) {
+      const uint32_t take = min(tail - head, 32u * kHubTake);
+      uint2 r[kHubTake];
+      HubNode n[kHubTake];
+#pragma unroll
+      for (int u = 0; u < kHubTake; u++) {
+        const uint32_t k = lane + 32u * u;
+        r[u] = k < take ? q[(head + k) % kHubRing] : make_uint2(0u, 0u);
+        if (k < take) n[u] = hub_load(a, r[u].x);
+      }
+      // each taken entry yields its children and / or its remaining siblings
+      uint2 e[2 * kHubTake];
+      uint32_t c = 0;
+#pragma unroll
+      for (int u = 0; u < kHubTake; u++) {
+        e[2 * u] = e[2 * u + 1] = make_uint2(0u, 0u);
+        if (lane + 32u * u < take) {
+          uint32_t next;
+          const bool open = hub_visit<MODEL, OVERLAP>(a, t, r[u].x, n[u], kx, ky, next);
+          const uint32_t childEnd = min(next, r[u].y);  // entries stay inside [base, end)
+          if (open && r[u].x + 1u < childEnd) e[2 * u] = make_uint2(r[u].x + 1u, childEnd);
+          if (next < r[u].y) e[2 * u + 1] = make_uint2(next, r[u].y);
+        }
+        c += (uint32_t)(e[2 * u].x < e[2 * u].y) + (uint32_t)(e[2 * u + 1].x < e[2 * u + 1].y);
+      }
+      __syncwarp();  // the slots just read are free from here on
+      head += take;
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+      const uint32_t room = kHubRing - (tail - head);
+      uint32_t slot = incl - c;
+#pragma unroll
+      for (int k = 0; k < 2 * kHubTake; k++) {
+        if (!(e[k].x < e[k].y)) continue;  // an empty range is no entry
+        if (slot < room) q[(tail + slot) % kHubRing] = e[k];
+        else hub_walk_range<MODEL, OVERLAP>(a, t, e[k].x, e[k].y, kx, ky);
+        slot++;
+      }
+      tail += min(total, room);
+      __syncwarp();
+    }
+    double sx = kx.value(), sy = ky.value();
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sx += __shfl_xor_sync(0xffffffffu, sx, o);
+      sy += __shfl_xor_sync(0xffffffffu, sy, o);
+    }
+    if (lane == 0u) a.out[i] = make_double2(sx, sy);
+  }
+}
+
+// The hubs' force epilogues with their plain repulsion, after the learned
+// walk wrote theirs.
+__global__ __launch_bounds__(256) void k_far_hub_epilogue(FarHubArgs a) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.nHubs) return;
+  const uint32_t v = a.hubs[i];
+  const uint32_t g = a.w.gid ? a.w.gid[v] : 0u;
+  if (a.w.active && a.w.active[g] == 0u) return;
+  const float2 at = a.w.attF[v];
+  const double2 r = a.out[i];
+  force_epilogue(a.w.epi, v, (double)at.x, (double)at.y, r.x, r.y);
+}
+
 struct ExactArgs {
   const double2 *pos;
   const float *massF, *radiusF;
@@ -1066,8 +1243,52 @@ void forces_set_smem_limits() {
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
 }
 
-// The learned walk (see k_walk_f32_far and k_walk_f32_cells).
+// The hub targets' plain walk, after the learned walk, on a grid that fills
+// the GPU; then their epilogues.
+template <int MODEL, bool OVERLAP>
+static void launch_far_hubs(gvizCudaForce *h, const FarHubArgs &ha) {
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_walk_f32_hubs<MODEL, OVERLAP>,
+                                                kHubThreads, 0);
+  const uint32_t fill = (uint32_t)((per > 0 ? per : 1) * (sms > 0 ? sms : 1));
+  const uint32_t need = blocks(h->nFarHubs, kHubThreads / 32);
+  cudaMemsetAsync(ha.counter, 0, sizeof(uint32_t), h->stream);
+  k_walk_f32_hubs<MODEL, OVERLAP><<<need < fill ? need : fill, kHubThreads, 0, h->stream>>>(ha);
+}
+
+static void enqueue_far_hubs(gvizCudaForce *h, const WalkArgs &a) {
+  FarHubArgs ha;
+  ha.w = a;
+  ha.hubs = h->d_farHubs;
+  ha.counter = h->d_farHubs + h->nFarHubs;
+  ha.out = h->d_farHubOut;
+  ha.nHubs = h->nFarHubs;
+  const double r = h->params.theta / h->params.farHubTheta;
+  ha.sizeScale = (float)(r * r);
+  const bool ov = h->params.preventOverlap != 0;
+  if (h->model == GVIZ_CUDA_MODEL_FR) {
+    if (ov) launch_far_hubs<GVIZ_CUDA_MODEL_FR, true>(h, ha);
+    else launch_far_hubs<GVIZ_CUDA_MODEL_FR, false>(h, ha);
+  } else {
+    if (ov) launch_far_hubs<GVIZ_CUDA_MODEL_LINLOG, true>(h, ha);
+    else launch_far_hubs<GVIZ_CUDA_MODEL_LINLOG, false>(h, ha);
+  }
+  prof_mark(h, "bh_walk_hubs");
+  k_far_hub_epilogue<<<blocks(h->nFarHubs, 256), 256, 0, h->stream>>>(ha);
+}
+
+static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters);
+
+// The learned walk (see k_walk_f32_far and k_walk_f32_cells), then the hub
+// targets' plain walk when params.farHubTargets asks for one.
 static void enqueue_far(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters) {
+  enqueue_far_walk(h, a, counters);
+  if (h->nFarHubs > 0 && h->d_farHubs) enqueue_far_hubs(h, a);
+}
+
+static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters) {
   FarArgs fa;
   fa.w = a;
   fa.cells = h->d_cells;

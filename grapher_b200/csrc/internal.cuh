@@ -190,6 +190,10 @@ struct gvizCudaForce {
   uint32_t *d_cellCnt = nullptr;    // per cell node: points below it
   uint4 *d_groups = nullptr;        // target groups: preorder [x, y), z points
   uint32_t *d_groupCount = nullptr; // [0] groups written, [1] walk queue
+  // hub targets of the learned walk (params.farHubTargets heaviest vertices)
+  uint32_t *d_farHubs = nullptr;  // nFarHubs ids, then the walk's hub counter
+  double2 *d_farHubOut = nullptr;
+  uint32_t nFarHubs = 0;
 
   // --- CUDA graph of one step ---
   cudaGraphExec_t stepExec = nullptr;

@@ -105,6 +105,14 @@ typedef struct gvizCudaForceParams {
                                one model evaluation at the group's centroid
                                corrects every target's monopole force;
                                0: the per-target walk above */
+  int32_t farHubTargets;    /* learned correction: the repulsion of this many
+                               heaviest vertices (model mass, ties to the
+                               lower id; at most vertexCount) comes from the
+                               plain monopole walk at farHubTheta instead, one
+                               block per vertex; 0 (default): none. LinLog's
+                               force on a vertex scales with its mass, so
+                               these carry most of the force-weighted error */
+  double farHubTheta;       /* their opening threshold (> 0; default 0.35) */
 } gvizCudaForceParams;
 
 /* One step's entries of the five stat series the embedder appends

@@ -295,6 +295,88 @@ def test_cell_group_steps_are_deterministic(trained):
     assert np.array_equal(outs[0], outs[1])
 
 
+def _heaviest(lay, k):
+    """The k heaviest vertices (LinLog mass deg + 1, ties to the lower id)."""
+    deg = np.diff(lay.row).astype(np.int64)
+    return np.sort(np.lexsort((np.arange(lay.V), -deg))[:k])
+
+
+def test_hub_targets_take_the_plain_walk(trained):
+    """farHubTargets: the heaviest vertices' repulsion is the plain monopole
+    walk's (at farHubTheta == theta the opening test is the same one; only
+    the order of the FP32 sums differs) and every other vertex keeps the
+    learned walk's result bit for bit."""
+    lay, m, _, _ = trained
+    m.attach(lay)
+    k = 300
+    hubs = _heaviest(lay, k)
+    lay.set_params(theta=1.2, farField=1, farCellGroups=1, farHubTargets=0)
+    learned = lay.repulsion()
+    lay.set_params(farField=0, farCellGroups=0)
+    plain = lay.repulsion()
+    lay.set_params(farField=1, farCellGroups=1, farHubTargets=k, farHubTheta=1.2)
+    mixed = lay.repulsion()
+    again = lay.repulsion()
+    lay.set_params(theta=1.0, farField=0, farCellGroups=0, farHubTargets=0)
+    rest = np.ones(lay.V, bool)
+    rest[hubs] = False
+    assert np.array_equal(mixed[rest], learned[rest])
+    d = np.linalg.norm(mixed[hubs] - plain[hubs], axis=1)
+    # both sums are Kahan-compensated FP32; the hubs' terms cancel heavily
+    assert np.all(d <= 1e-4 * np.linalg.norm(plain[hubs], axis=1)), d.max()
+    assert not np.array_equal(mixed[hubs], learned[hubs])
+    assert np.array_equal(mixed, again)   # deterministic sums
+
+
+def test_hub_walk_without_acceptance_is_exact(trained):
+    """At a tiny farHubTheta no cell is accepted: every hub sums the pair
+    terms of all other vertices, so its frontier outgrows the block's
+    shared memory and the entries beyond it are walked by their threads."""
+    lay, m, targets, exact = trained
+    m.attach(lay)
+    hubs = _heaviest(lay, 64)
+    ex = lay.exact_repulsion(hubs.astype(np.uint32))
+    lay.set_params(theta=1.2, farField=1, farCellGroups=1, farHubTargets=64,
+                   farHubTheta=1e-4)
+    rep = lay.repulsion()[hubs]
+    lay.set_params(theta=1.0, farField=0, farCellGroups=0, farHubTargets=0)
+    d = np.linalg.norm(rep - ex, axis=1)
+    n = np.linalg.norm(ex, axis=1)
+    assert np.sqrt(np.sum(d * d) / np.sum(n * n)) < 1e-4
+    assert np.all(d <= 1e-3 * n), (d / n).max()
+
+
+def test_hub_targets_cut_the_weighted_error(trained):
+    """The hubs carry most of LinLog's force, so a tight walk for the
+    heaviest 1/64 of the vertices lowers the force-weighted error of the
+    learned walk at theta = 1.2."""
+    lay, m, targets, exact = trained
+    m.attach(lay)
+    lay.set_params(theta=1.2, farField=1, farCellGroups=1, farHubTargets=0)
+    e0 = _nrms(lay, targets, exact)
+    lay.set_params(farHubTargets=lay.V // 64, farHubTheta=0.35)
+    e1 = _nrms(lay, targets, exact)
+    lay.set_params(theta=1.0, farField=0, farCellGroups=0, farHubTargets=0)
+    assert e1 < 0.9 * e0, (e1, e0)
+
+
+def test_hub_steps_are_deterministic(trained):
+    """Steps with the hub walk forked beside the learned walk in the
+    captured step graph give the same positions on every run."""
+    _, m, _, _ = trained
+    outs = []
+    for _ in range(2):
+        lay = _ba_layout(V=8192, steps=3)
+        m.attach(lay)
+        lay.set_params(theta=1.2, farField=1, farCellGroups=1, farHubTargets=128,
+                       farHubTheta=0.35)
+        for _ in range(5):
+            lay.step()
+        outs.append(lay.positions())
+    assert np.all(np.isfinite(outs[0]))
+    assert np.array_equal(outs[0], outs[1])
+
+
 def test_far_field_argument_checks(trained):
     from grapher_b200._native import GvizCudaError
     lay = _ba_layout(V=512, steps=1)
@@ -311,3 +393,12 @@ def test_far_field_argument_checks(trained):
     lay.set_params(farField=0, farGroupSpread=1.0)
     with pytest.raises(GvizCudaError):
         lay.set_params(farCellGroups=2)
+    lay.set_params(farCellGroups=0)
+    with pytest.raises(GvizCudaError):
+        lay.set_params(farHubTargets=-1)
+    lay.set_params(farHubTargets=0)
+    with pytest.raises(GvizCudaError):
+        lay.set_params(farHubTargets=8, farHubTheta=0.0)
+    lay.set_params(farHubTargets=0, farHubTheta=0.35)
+    lay.set_params(farHubTargets=1 << 30)   # more than the vertices: all of them
+    lay.set_params(farHubTargets=0)
