@@ -694,6 +694,7 @@ void gvizCudaForceDestroy(gvizCudaForce *h) {
 // order, as the learned walk's hub targets.
 static int select_hubs(gvizCudaForce *h, uint32_t count) {
   if (h->stream) cudaStreamSynchronize(h->stream);
+  h->graphDirty = true;  // the captured step holds the buffers freed here
   cudaFree(h->d_farHubs);
   cudaFree(h->d_farHubOut);
   h->d_farHubs = nullptr;

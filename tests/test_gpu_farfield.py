@@ -328,6 +328,43 @@ def test_hub_targets_take_the_plain_walk(trained):
     assert np.array_equal(mixed, again)   # deterministic sums
 
 
+def test_hub_targets_in_a_batch(trained):
+    """In a batch of layouts every hub walks its own graph's tree only: the
+    heaviest vertices over the batch take the plain walk's repulsion of
+    their own graph, the rest keep the learned walk's."""
+    from grapher_b200 import ForceLayout, graphs
+    _, m, _, _ = trained
+    parts, offs, n = [], [0], 0
+    for V, seed in ((3000, 11), (5000, 12)):
+        a, b = graphs.barabasi_albert(V, 4, seed)
+        parts.append((a + n, b + n))
+        n += V
+        offs.append(n)
+    a = np.concatenate([p[0] for p in parts])
+    b = np.concatenate([p[1] for p in parts])
+    row, col = graphs.to_csr(n, a, b)
+    lay = ForceLayout(row, col, model=1, graph_offsets=np.array(offs, np.uint64))
+    lay.set_params(theta=1.2, gravityK=1.0)
+    lay.begin(0, positions=graphs.randomize_positions(n, 1000.0, 7))
+    for _ in range(5):
+        lay.step()
+    m.attach(lay)
+    hubs = _heaviest(lay, 40)
+    assert hubs.min() < offs[1] <= hubs.max()   # hubs in both graphs
+    lay.set_params(farField=1, farCellGroups=1, farHubTargets=0)
+    learned = lay.repulsion()
+    lay.set_params(farField=0, farCellGroups=0)
+    plain = lay.repulsion()
+    lay.set_params(farField=1, farCellGroups=1, farHubTargets=40, farHubTheta=1.2)
+    mixed = lay.repulsion()
+    rest = np.ones(n, bool)
+    rest[hubs] = False
+    assert np.array_equal(mixed[rest], learned[rest])
+    d = np.linalg.norm(mixed[hubs] - plain[hubs], axis=1)
+    assert np.all(d <= 1e-4 * np.linalg.norm(plain[hubs], axis=1)), d.max()
+    lay.close()
+
+
 def test_hub_walk_without_acceptance_is_exact(trained):
     """At a tiny farHubTheta no cell is accepted: every hub sums the pair
     terms of all other vertices, so its frontier outgrows the block's
