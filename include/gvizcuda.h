@@ -109,9 +109,10 @@ typedef struct gvizCudaForceParams {
                                heaviest vertices (model mass, ties to the
                                lower id; at most vertexCount) comes from the
                                plain monopole walk at farHubTheta instead, one
-                               block per vertex; 0 (default): none. LinLog's
-                               force on a vertex scales with its mass, so
-                               these carry most of the force-weighted error */
+                               warp per vertex after the learned walk; 0
+                               (default): none. LinLog's force on a vertex
+                               scales with its mass, so these carry most of
+                               the force-weighted error */
   double farHubTheta;       /* their opening threshold (> 0; default 0.35) */
 } gvizCudaForceParams;
 
