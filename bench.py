@@ -12,14 +12,15 @@ trained on the GPU (40 epochs) from pairs harvested for 32,768 sampled
 vertices at theta = 1.2, 0.9 and 0.6 on three snapshots of this layout
 (untimed setup, reported as train_s). Force error is the
 normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
-65,536 sampled vertices, all configurations judged on the same positions.
+every vertex (on 65,536 sampled vertices for layouts above 2^20 vertices),
+all configurations judged on the same positions.
 The plain walk runs at theta = 0.5; the learned walk (the cell-group walk:
 one warp per group of <= 32 targets cut from the tree, one network row per
 accepted cell) at the largest theta of 1.3, 1.25, ..., 0.6 whose error is
-not above the plain walk's. It is judged twice: alone, and with hub targets
-(the V / 1024 heaviest vertices take the plain monopole walk at theta = 0.35,
-since LinLog's force on a vertex scales with its mass); each at its own
-largest qualifying theta, the faster of the two (10 timed steps each, from
+not above the plain walk's. It is judged alone and with hub targets (the
+V / 1024 or V / 256 heaviest vertices take the plain monopole walk at
+theta = 0.35, since LinLog's force on a vertex scales with its mass); each
+at its own largest qualifying theta, the fastest (10 timed steps each, from
 one saved state) is the learned configuration (--hub-targets fixes the
 count instead). ``value`` is the learned path's iterations/s;
 the plain path's are in ``plain``. Both are timed from the same saved
@@ -352,10 +353,12 @@ def replica_value(ms_max, steps, world):
 LEARNED_THETAS = tuple(round(1.3 - 0.05 * i, 2) for i in range(15))  # 1.3 ... 0.6
 LEARNED_SPREAD = 1.0
 LEARNED_CELL_GROUPS = 1  # the cell-group walk: one warp per tree-cut group of <= 32 targets
-HUB_SHARE = 1024         # hub targets: the V / HUB_SHARE heaviest vertices
+HUB_SHARES = (1024, 256)  # hub-target candidates: the V / share heaviest vertices
 HUB_THETA = 0.35         # their plain walk's opening threshold
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
 JUDGE_VERTICES = 65536
+JUDGE_ALL_MAX = 1 << 20  # layouts up to this size are judged on every vertex
+JUDGE_CHUNK = 262144     # targets per exact FP64 repulsion call
 CHOICE_STEPS = 10        # timed steps per candidate when choosing the learned config
 
 
@@ -398,15 +401,20 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     losses = model.train(np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws),
                          epochs=40, batch=4096, lr=2e-3, seed=SEED)
     train_s = time.perf_counter() - t0
-    targets = np.sort(rng.choice(w.V, min(JUDGE_VERTICES, w.V), replace=False)).astype(np.uint32)
-    exact = lay.exact_repulsion(targets)
+    if w.V <= JUDGE_ALL_MAX:
+        targets = np.arange(w.V, dtype=np.uint32)
+    else:
+        targets = np.sort(rng.choice(w.V, JUDGE_VERTICES, replace=False)).astype(np.uint32)
+    exact = np.concatenate([lay.exact_repulsion(targets[i:i + JUDGE_CHUNK])
+                            for i in range(0, len(targets), JUDGE_CHUNK)])
     lay.set_params(theta=w.spec["theta"], farField=0)
     e_plain, e_plain_pv = force_error(lay, targets, exact)
     model.attach(lay)
     fixed = hub_targets != "auto"
-    hubs = min(int(hub_targets), w.V) if fixed else w.V // HUB_SHARE
+    counts = sorted({0, min(int(hub_targets), w.V)} if fixed else
+                    {0} | {w.V // share for share in HUB_SHARES})
     tables, picks = {}, {}
-    for k in sorted({0, hubs}):
+    for k in counts:
         table, pick = {}, None
         for th in LEARNED_THETAS:
             lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD,
@@ -420,14 +428,14 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     # the faster of the two qualifying configurations, from the same state
     x_s, fa2_s = lay.positions(), lay.fa2_state()
     times = {}
-    for k in sorted({0, hubs}):
+    for k in counts:
         lay.set_params(theta=picks[k], farField=1, farGroupSpread=LEARNED_SPREAD,
                        farCellGroups=LEARNED_CELL_GROUPS, farHubTargets=k, farHubTheta=HUB_THETA)
         lay.time_steps(3)
         times[k] = reduce(lay.time_steps(CHOICE_STEPS)) / CHOICE_STEPS
         lay.set_positions(x_s)
         lay.set_fa2_state(*fa2_s)
-    k_best = hubs if (fixed or times[hubs] < times[0]) else 0
+    k_best = counts[-1] if fixed else min(counts, key=lambda k: times[k])
     chosen, table = picks[k_best], tables[k_best]
     lay.set_params(theta=w.spec["theta"], farField=0, farCellGroups=0, farHubTargets=0)
     plain_table = {}
@@ -444,9 +452,8 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
             "learned_errors": table, "plain_errors": plain_table,
             "hub_choice": "fixed" if fixed else "auto",
             "candidates": [{"hub_targets": k, "theta": picks[k], "ms_per_step": times[k],
-                            "rms_err": tables[k][str(picks[k])]["rms_err"]}
-                           for k in sorted({0, hubs})],
-            "learned_errors_by_hub_targets": {str(k): tables[k] for k in sorted({0, hubs})},
+                            "rms_err": tables[k][str(picks[k])]["rms_err"]} for k in counts],
+            "learned_errors_by_hub_targets": {str(k): tables[k] for k in counts},
             "group_spread": LEARNED_SPREAD,
             "walk": "cell groups" if LEARNED_CELL_GROUPS else "per target"}
     return model, info
@@ -608,8 +615,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--hub-targets", default="auto",
                     help="learned workloads: hub targets of the learned walk; 'auto' (default) "
-                         "times 0 and V/1024 at their own largest qualifying theta and keeps "
-                         "the faster, a number fixes the count")
+                         "times 0, V/1024 and V/256 at their own largest qualifying theta and "
+                         "keeps the fastest, a number fixes the count")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == "grip_ba200k":
