@@ -13,7 +13,9 @@ vertices at theta = 1.2, 0.9 and 0.6 on three snapshots of this layout
 (untimed setup, reported as train_s). Force error is the
 normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
 every vertex (on 65,536 sampled vertices for layouts above 2^20 vertices),
-all configurations judged on the same positions.
+all configurations judged on the same positions; the error tables also carry
+the RMS of the per-vertex relative errors and the largest per-vertex error
+over the RMS force.
 The plain walk runs at theta = 0.5; the learned walk (the cell-group walk:
 one warp per group of <= 32 targets cut from the tree, one network row per
 accepted cell) at the largest theta of 1.3, 1.25, ..., 0.6 whose error is
@@ -363,13 +365,20 @@ CHOICE_STEPS = 10        # timed steps per candidate when choosing the learned c
 
 
 def force_error(lay, targets, exact):
-    """Normalised RMS error of the current repulsion on the sampled targets,
-    and the RMS of the per-vertex relative errors."""
+    """Error of the current repulsion on the judged targets: the normalised
+    RMS (the metric's error), the RMS of the per-vertex relative errors and
+    the largest per-vertex error relative to the RMS force."""
     rep = lay.repulsion()[targets]
     d = np.linalg.norm(rep - exact, axis=1)
     n = np.linalg.norm(exact, axis=1)
+    rms_force = float(np.sqrt(np.mean(n * n)))
     return (float(np.sqrt(np.sum(d * d) / np.sum(n * n))),
-            float(np.sqrt(np.mean((d / np.maximum(n, 1e-300)) ** 2))))
+            float(np.sqrt(np.mean((d / np.maximum(n, 1e-300)) ** 2))),
+            float(np.max(d) / max(rms_force, 1e-300)))
+
+
+def error_entry(e):
+    return {"rms_err": e[0], "rms_rel_err_per_vertex": e[1], "max_err_over_rms_force": e[2]}
 
 
 def learned_params(linfo):
@@ -408,7 +417,7 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     exact = np.concatenate([lay.exact_repulsion(targets[i:i + JUDGE_CHUNK])
                             for i in range(0, len(targets), JUDGE_CHUNK)])
     lay.set_params(theta=w.spec["theta"], farField=0)
-    e_plain, e_plain_pv = force_error(lay, targets, exact)
+    e_plain, e_plain_pv, e_plain_max = force_error(lay, targets, exact)
     model.attach(lay)
     fixed = hub_targets != "auto"
     counts = sorted({0, min(int(hub_targets), w.V)} if fixed else
@@ -420,9 +429,9 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
             lay.set_params(theta=th, farField=1, farGroupSpread=LEARNED_SPREAD,
                            farCellGroups=LEARNED_CELL_GROUPS, farHubTargets=k,
                            farHubTheta=HUB_THETA)
-            e, e_pv = force_error(lay, targets, exact)
-            table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
-            if pick is None and e <= e_plain:
+            err = force_error(lay, targets, exact)
+            table[str(th)] = error_entry(err)
+            if pick is None and err[0] <= e_plain:
                 pick = th
         tables[k], picks[k] = table, (pick if pick is not None else LEARNED_THETAS[-1])
     # the faster of the two qualifying configurations, from the same state
@@ -441,13 +450,13 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     plain_table = {}
     for th in (0.3, 0.4, 0.5, 0.6, 0.8, 1.0, 1.2):
         lay.set_params(theta=th)
-        e, e_pv = force_error(lay, targets, exact)
-        plain_table[str(th)] = {"rms_err": e, "rms_rel_err_per_vertex": e_pv}
+        plain_table[str(th)] = error_entry(force_error(lay, targets, exact))
     lay.set_params(theta=w.spec["theta"])
     info = {"train_s": train_s, "train_pairs": int(sum(len(x) for x in Xs)),
             "train_loss_first_last": [float(losses[0]), float(losses[-1])],
             "judge_vertices": int(len(targets)), "plain_rms_err": e_plain,
-            "plain_rms_rel_err_per_vertex": e_plain_pv, "learned_theta": chosen,
+            "plain_rms_rel_err_per_vertex": e_plain_pv,
+            "plain_max_err_over_rms_force": e_plain_max, "learned_theta": chosen,
             "hub_targets": k_best, "hub_theta": HUB_THETA,
             "learned_errors": table, "plain_errors": plain_table,
             "hub_choice": "fixed" if fixed else "auto",

@@ -96,6 +96,8 @@ def test_candidates_take_their_largest_qualifying_theta(fake_training):
         ok = [float(t) for t, e in table.items() if e["rms_err"] <= plain]
         assert c["theta"] == max(ok)
         assert c["rms_err"] <= plain
+        assert set(table[str(c["theta"])]) == {"rms_err", "rms_rel_err_per_vertex",
+                                               "max_err_over_rms_force"}
 
 
 def test_fastest_candidate_wins(fake_training):
