@@ -79,7 +79,9 @@ static int32_t state_model(const gvizForceEmbedderState *s) {
 }
 
 /* Configuration is re-read before every step: the toggle action and the
- * Configure* setters may run between steps. */
+ * Configure* setters may run between steps. The learned far-field options
+ * have no embedder field; whatever the caller set on the handle
+ * (gvizCudaForceEmbedderHandle) is kept. */
 static int push_params(attached *a) {
   const gvizForceEmbedderState *s = a->state;
   gvizCudaForceParams p;
@@ -97,8 +99,14 @@ static int push_params(attached *a) {
   p.jitterTolerance = s->jitterTolerance;
   p.strictReductions = a->opt.strictReductions;
   gvizCudaForceParams cur;
-  if (gvizCudaForceGetParams(a->h, &cur) == GVIZ_CUDA_OK &&
-      memcmp(&cur, &p, sizeof(p)) == 0)
+  if (gvizCudaForceGetParams(a->h, &cur) != GVIZ_CUDA_OK)
+    return gvizCudaForceSetParams(a->h, &p);
+  p.farField = cur.farField;
+  p.farGroupSpread = cur.farGroupSpread;
+  p.farCellGroups = cur.farCellGroups;
+  p.farHubTargets = cur.farHubTargets;
+  p.farHubTheta = cur.farHubTheta;
+  if (memcmp(&cur, &p, sizeof(p)) == 0)
     return GVIZ_CUDA_OK;
   return gvizCudaForceSetParams(a->h, &p);
 }
@@ -369,6 +377,11 @@ void gvizCudaForceDetach(gvizForceEmbedderState *state) {
 int gvizCudaForceEmbedderLastError(const gvizForceEmbedderState *state) {
   const attached *a = find(state);
   return a ? a->lastError : GVIZ_CUDA_ERR_ARG;
+}
+
+gvizCudaForce *gvizCudaForceEmbedderHandle(const gvizForceEmbedderState *state) {
+  const attached *a = find(state);
+  return a ? a->h : NULL;
 }
 
 /* ---- batched Run over many embedders ------------------------------------ */

@@ -63,6 +63,14 @@ void gvizCudaForceDetach(gvizForceEmbedderState *state);
  * handler cannot return one. */
 int gvizCudaForceEmbedderLastError(const gvizForceEmbedderState *state);
 
+/* The library handle attached to this state (NULL when none), for options
+ * the embedder has no field for: the learned far field
+ * (gvizCudaForceSetFarFieldModel, then farField, farCellGroups,
+ * farHubTargets, ... through gvizCudaForceGetParams / SetParams). Steps
+ * through the action keep those options; every other field is re-read from
+ * the state before each step. The handle stays owned by the attachment. */
+gvizCudaForce *gvizCudaForceEmbedderHandle(const gvizForceEmbedderState *state);
+
 /* gvizForceEmbedderRun (src/embedders/gvizForceEmbedder.c:497-510) for n
  * independent begun embedders at once, all laid out by one GPU handle (one
  * quadtree per graph in one forest, per-graph FA2 speed, per-graph
