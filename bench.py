@@ -129,18 +129,61 @@ class Workload:
                 self.graphs.append((V, a, b, 0.5 * math.sqrt(V) * 10.0, 1000 + g))
             self.desc = "4096 graphs, V log-uniform [32, 8192], ER/random tree/grid"
         self.G = len(self.graphs)
-        if self.G == 1:
-            V, a, b, _, _ = self.graphs[0]
-            self.row, self.col = graphs.to_csr(V, a, b)
-            self.goff = None
-        else:
-            self.row, self.col, self.goff = graphs.batch([(V, a, b) for V, a, b, _, _ in self.graphs])
-        self.V = int(self.row.shape[0] - 1)
-        xs = []
-        for V, a, b, box, seed in self.graphs:
-            xs.append(graphs.unit_disk_positions(V, seed) if box is None
-                      else graphs.randomize_positions(V, box, seed))
-        self.x0 = np.concatenate(xs)
+        self.V = int(sum(g[0] for g in self.graphs))
+        self._csr = None
+        self._x0 = None
+
+    # The combined CSR and the initial positions come from libgvizcuda
+    # (gvizCudaEdgesToCsr, gvizCudaRandomizePositions): built on first use,
+    # so the reference arm, which never asks for them, does not load it.
+    def _build_csr(self):
+        from grapher_b200 import graphs
+        if self._csr is None:
+            if self.G == 1:
+                V, a, b, _, _ = self.graphs[0]
+                row, col = graphs.to_csr(V, a, b)
+                self._csr = (row, col, None)
+            else:
+                self._csr = graphs.batch([(V, a, b) for V, a, b, _, _ in self.graphs])
+        return self._csr
+
+    @property
+    def row(self):
+        return self._build_csr()[0]
+
+    @property
+    def col(self):
+        return self._build_csr()[1]
+
+    @property
+    def goff(self):
+        return self._build_csr()[2]
+
+    @property
+    def x0(self):
+        from grapher_b200 import graphs
+        if self._x0 is None:
+            self._x0 = np.concatenate(
+                [graphs.unit_disk_positions(V, seed) if box is None
+                 else graphs.randomize_positions(V, box, seed)
+                 for V, a, b, box, seed in self.graphs])
+        return self._x0
+
+    def unit_disk_start(self, g):
+        """Initial positions of graph g when it starts in the unit disk
+        (numpy only), else None (the reference's own Begin places it)."""
+        from grapher_b200 import graphs
+        V, _, _, box, seed = self.graphs[g]
+        return graphs.unit_disk_positions(V, seed) if box is None else None
+
+    def metric(self):
+        """The metric string, the same in both arms."""
+        if self.name == "ba1m_learned":
+            return "layout iters/sec, 1M-vertex BA graph: learned vs plain BH at equal force error"
+        if self.name == "rmat4m_learned":
+            return ("layout iters/sec, R-MAT scale-22 graph: learned vs plain BH at equal "
+                    "force error")
+        return f"layout iters/sec, {self.name}"
 
     def configure(self, lay):
         s = self.spec
@@ -237,9 +280,9 @@ def reference_graph(w, g):
     lay = ref.create_edges(V, a, b, w.spec["model"])
     lay.configure(w.oracle_params(), box if box else 0.0)
     lay.begin(seed)
-    if box is None:
-        s = 2 * int(sum(x[0] for x in w.graphs[:g]))
-        lay.set_positions(w.x0[s:s + 2 * V])
+    start = w.unit_disk_start(g)
+    if start is not None:
+        lay.set_positions(start)
     return ref, lay
 
 
@@ -277,25 +320,67 @@ def cpu_baseline(w):
     if Reference.available():
         t, cores, sample = reference_iteration_time(w)
         return {"value": 1.0 / t, "unit": "iters/s", "cores": cores, "kind": "reference",
-                "sample": sample}
+                "cpu_model": cpu_model(), "sample": sample}
     from oracle.bindings import Oracle
     o = Oracle()
-    V, a, b, _, _ = w.graphs[0]
-    row, col = w.row, w.col
+    V, a, b, box, seed = w.graphs[0]
+    row, col = csr_numpy(V, a, b)
     deg = np.diff(row).astype(np.uint64)
-    mass = np.ones(w.V) if w.spec["model"] == 0 else 1.0 + deg
-    pos, sf, ss = w.x0.copy(), np.zeros(2 * w.V), np.array([1.0, 1.0])
+    mass = np.ones(V) if w.spec["model"] == 0 else 1.0 + deg
+    start = w.unit_disk_start(0)
+    pos = start.copy() if start is not None else rand_r_positions(V, box, seed)
+    sf, ss = np.zeros(2 * V), np.array([1.0, 1.0])
     t0 = time.perf_counter()
     o.step((row, col), mass, deg, w.oracle_params(), pos, sf, ss)
-    return {"value": 1.0 / (time.perf_counter() - t0), "unit": "iters/s", "cores": 1,
-            "kind": "port", "sample": "1 step of the single-thread oracle (reference library absent)"}
+    t = (time.perf_counter() - t0) * w.V / V
+    return {"value": 1.0 / t, "unit": "iters/s", "cores": 1, "kind": "port",
+            "cpu_model": cpu_model(),
+            "sample": "1 step of the single-thread oracle on the first graph, scaled by vertex "
+                      "count (reference library absent)"}
+
+
+def csr_numpy(V, a, b):
+    """Adjacency as gvizGraphAddEdge builds it (edge (a,b) appends b to a's
+    list and a to b's, in edge order), with numpy alone."""
+    src = np.empty(2 * len(a), np.int64)
+    dst = np.empty(2 * len(a), np.uint32)
+    src[0::2], src[1::2] = a, b
+    dst[0::2], dst[1::2] = b, a
+    order = np.argsort(src, kind="stable")
+    row = np.zeros(V + 1, np.uint64)
+    np.cumsum(np.bincount(src, minlength=V), out=row[1:])
+    return row, np.ascontiguousarray(dst[order])
+
+
+def rand_r_positions(V, box, seed):
+    """The reference's Begin placement (libc rand_r, x then y per vertex),
+    through the C library directly."""
+    import ctypes
+    libc = ctypes.CDLL(None)
+    st = ctypes.c_uint(seed)
+    r = np.array([libc.rand_r(ctypes.byref(st)) for _ in range(2 * V)], np.float64)
+    return box * (2.0 * (r / (2147483647.0 + 1.0)) - 1.0)
+
+
+def cpu_model():
+    """The host CPU's model name and the logical CPUs online."""
+    name = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical CPUs"
 
 
 def run_reference_arm(args, w):
     if int(os.environ.get("RANK", "0")) != 0:
         return 0
     from oracle.bindings import Reference
-    line = {"impl": "reference", "metric": "layout iters/sec", "unit": "iters/s",
+    line = {"impl": "reference", "metric": w.metric(), "unit": "iters/s",
             "n_gpus": args.gpus, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": w.config(args)}
     if Reference.available() and w.G == 1:
@@ -307,6 +392,7 @@ def run_reference_arm(args, w):
         v = args.steps / float(t.sum())
         line.update(steps=args.steps, warmup=args.warmup, ms_per_step=1e3 * float(t.mean()))
         base = {"value": v, "unit": "iters/s", "cores": ref.pool_threads(), "kind": "reference",
+                "cpu_model": cpu_model(),
                 "sample": f"{args.steps} full reference steps after {args.warmup} warm-up steps"}
     else:
         base = cpu_baseline(w)
@@ -358,6 +444,13 @@ LEARNED_CELL_GROUPS = 1  # the cell-group walk: one warp per tree-cut group of <
 HUB_SHARES = (1024, 256)  # hub-target candidates: the V / share heaviest vertices
 HUB_THETA = 0.35         # their plain walk's opening threshold
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
+# The learned comparison starts from a fixed point of the layout, whatever
+# --warmup asks for: LEARNED_PRE_STEPS plain steps from the initial
+# positions, then the harvest snapshots HARVEST_GAP steps apart; the judged
+# and timed state is the one after the last snapshot. --warmup steps run
+# before each timed region, from that saved state.
+LEARNED_PRE_STEPS = 20
+HARVEST_GAP = 5
 JUDGE_VERTICES = 65536
 JUDGE_ALL_MAX = 1 << 20  # layouts up to this size are judged on every vertex
 JUDGE_CHUNK = 262144     # targets per exact FP64 repulsion call
@@ -401,7 +494,7 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     Xs, Ts, Ws = [], [], []
     for snap, th in enumerate((1.2, 0.9, 0.6)):  # cells of every angular size
         if snap:
-            for _ in range(5):
+            for _ in range(HARVEST_GAP):
                 lay.step()
         t = np.sort(rng.choice(w.V, HARVEST_TARGETS, replace=False)).astype(np.uint32)
         X, T, Wt = harvest_training_set(lay, th, t)
@@ -651,7 +744,7 @@ def main():
     lay = ForceLayout(w.row, w.col, model=w.spec["model"], graph_offsets=w.goff, device=local)
     w.configure(lay)
     lay.begin(0, positions=w.x0)
-    for _ in range(args.warmup):
+    for _ in range(LEARNED_PRE_STEPS if learned else args.warmup):
         lay.step()
     # the walk's launch shape for this layout (block size, static or
     # persistent schedule), timed on the warmed-up positions
@@ -751,7 +844,7 @@ def main():
                                                  "monopole/pair interactions per launch"}}
 
     line = {
-        "metric": "layout iters/sec", "value": value, "unit": "iters/s", "n_gpus": world,
+        "metric": w.metric(), "value": value, "unit": "iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": w.config(args), "clocks": clocks, "e2e": e2e,
@@ -767,9 +860,6 @@ def main():
         # the state after the timed steps (untimed)
         line["error_every_20"] = error_trajectory(lay, w, linfo)
     if learned:
-        line["metric"] = (("layout iters/sec, 1M-vertex BA graph" if args.workload == "ba1m_learned"
-                           else "layout iters/sec, R-MAT scale-22 graph")
-                          + ": learned vs plain BH at equal force error")
         line["learned"] = dict(linfo, value=value, theta=linfo["learned_theta"],
                                rms_err=linfo["learned_errors"][str(linfo["learned_theta"])]["rms_err"])
         line["plain"] = plain_line

@@ -170,14 +170,13 @@ _SIGS = {
     "gvizCudaForceHarvestFarField": (C.c_int64, [P, U32P, SZ, D, C.POINTER(C.c_float),
                                                  C.POINTER(C.c_float), C.POINTER(C.c_float),
                                                  U32P, SZ]),
-    "gvizCudaGenGrid": (SZ, [SZ, SZ, U32P, U32P]),
-    "gvizCudaGenRandomConnected": (SZ, [SZ, D, C.c_uint, U32P, U32P]),
-    "gvizCudaGenBarabasiAlbert": (SZ, [SZ, C.c_uint32, C.c_uint64, U32P, U32P]),
-    "gvizCudaGenErdosRenyi": (SZ, [SZ, SZ, C.c_uint64, U32P, U32P]),
-    "gvizCudaGenRmat": (SZ, [C.c_uint32, SZ, D, D, D, C.c_uint64, U32P, U32P]),
     "gvizCudaEdgesToCsr": (C.c_int, [SZ, U32P, U32P, SZ, U64P, U32P]),
     "gvizCudaForceAutotune": (C.c_int, [P, U32P, I32P, C.POINTER(C.c_float)]),
     "gvizCudaForceSetWalkShape": (C.c_int, [P, C.c_uint32, C.c_int32]),
+    "gvizCudaForceSetCellStackCap": (C.c_int, [P, C.c_uint32]),
+    "gvizCudaForceSetFarJudge": (C.c_int, [P, C.c_uint32, C.c_uint32, D, D, C.c_uint64]),
+    "gvizCudaForceJudgeFarField": (C.c_int, [P, DP, DP, I32P]),
+    "gvizCudaForceFarJudgeStatus": (C.c_int, [P, U64P, DP, DP, I32P]),
     "gvizCudaForceSaveCheckpoint": (C.c_int, [P, C.c_char_p, C.c_char_p]),
     "gvizCudaForceLoadCheckpoint": (C.c_int, [P, C.c_char_p, C.c_int, C.c_char_p, SZ]),
     "gvizCudaForceSaveEmbeddingText": (C.c_int, [P, C.c_char_p, C.c_char_p]),
@@ -207,6 +206,34 @@ def lib() -> C.CDLL:
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+# libgvizworkloads.so (include/gvizworkloads.h): synthetic graphs, host only
+WORKLOADS_PATH = os.path.join(HERE, "lib", "libgvizworkloads.so")
+_WSIGS = {
+    "gvizGenGrid": (SZ, [SZ, SZ, U32P, U32P]),
+    "gvizGenRandomConnected": (SZ, [SZ, D, C.c_uint, U32P, U32P]),
+    "gvizGenBarabasiAlbert": (SZ, [SZ, C.c_uint32, C.c_uint64, U32P, U32P]),
+    "gvizGenErdosRenyi": (SZ, [SZ, SZ, C.c_uint64, U32P, U32P]),
+    "gvizGenRmat": (SZ, [C.c_uint32, SZ, D, D, D, C.c_uint64, U32P, U32P]),
+}
+_wlib = None
+
+
+def workloads_lib() -> C.CDLL:
+    """Loads libgvizworkloads.so (it does not load libgvizcuda)."""
+    global _wlib
+    if _wlib is None:
+        if not os.path.exists(WORKLOADS_PATH):
+            raise RuntimeError(
+                f"{WORKLOADS_PATH} is missing: build it with `python -m grapher_b200.build`")
+        L = C.CDLL(WORKLOADS_PATH)
+        for name, (res, args) in _WSIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _wlib = L
+    return _wlib
 
 
 def check(code: int, what: str = "") -> int:

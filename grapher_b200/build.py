@@ -69,6 +69,24 @@ def _compile(src: str, extra: list[str], hdr: float, verbose: bool) -> str:
     return obj
 
 
+WORKLOADS_SRC = os.path.join(CSRC, "workloads.cpp")
+WORKLOADS_LIB = os.path.join(LIBDIR, "libgvizworkloads.so")
+
+
+def build_workloads() -> str:
+    """The synthetic-graph library, host C++ only (no CUDA)."""
+    hdr = os.path.join(INCLUDE, "gvizworkloads.h")
+    if os.path.exists(WORKLOADS_LIB) and os.path.getmtime(WORKLOADS_LIB) >= max(
+            os.path.getmtime(WORKLOADS_SRC), os.path.getmtime(hdr)):
+        return WORKLOADS_LIB
+    cmd = ["g++", "-O3", "-fPIC", "-shared", "-std=c++17", "-I" + INCLUDE, WORKLOADS_SRC,
+           "-o", WORKLOADS_LIB]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError(f"workloads build failed: {' '.join(cmd)}\n{out.stdout}{out.stderr}")
+    return WORKLOADS_LIB
+
+
 ADAPTER_SRC = os.path.join(HERE, "gviz", "gvizCudaForceEmbedder.c")
 GRIP_ADAPTER_SRC = os.path.join(HERE, "gviz", "gvizCudaGripEmbedder.c")
 ADAPTER_LIB = os.path.join(LIBDIR, "libgvizcuda_gviz.so")
@@ -108,6 +126,7 @@ def build(verbose: bool = False) -> str:
         out = subprocess.run(cmd, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{out.stdout}{out.stderr}")
+    build_workloads()
     build_gviz_adapter()
     return LIB
 

@@ -27,6 +27,8 @@ void enqueue_cell_dump(gvizCudaForce *h, int32_t *depth, uint64_t *hi,
                        uint64_t *lo, double *mass, double *cx, double *cy,
                        uint64_t *cnt);
 
+static int far_judge(gvizCudaForce *h);
+
 namespace {
 
 constexpr int kRunBatch = 8;
@@ -70,6 +72,10 @@ int upload_dir_table(gvizCudaForce *h) {
 }
 
 void free_all(gvizCudaForce *h) {
+  dfree(h->d_judgeIdx);
+  dfree(h->d_judgeExact);
+  dfree(h->d_judgeOut);
+  dfree(h->d_judgeRep);
   dfree(h->d_rowOff);
   dfree(h->d_cols);
   dfree(h->d_degree);
@@ -261,13 +267,27 @@ int ensure_graph(gvizCudaForce *h) {
   return GVIZ_CUDA_OK;
 }
 
+// Replays the captured step n times. With automatic checks of the learned
+// walk on (gvizCudaForceSetFarJudge), a check runs before every judgeEvery-th
+// step launched while the learned walk is on; a check that turns the walk
+// off makes the next replay capture the plain step.
 int launch_steps(gvizCudaForce *h, uint32_t n) {
   if (h->V == 0) return GVIZ_CUDA_OK;
   int rc = ensure_graph(h);
   if (rc) return rc;
-  for (uint32_t i = 0; i < n; i++)
+  for (uint32_t i = 0; i < n; i++) {
+    if (h->judgeEvery && h->params.farField && h->d_mlp &&
+        h->stepsLaunched >= h->judgeNextAt) {
+      rc = far_judge(h);
+      if (rc) return rc;
+      h->judgeNextAt = h->stepsLaunched + h->judgeEvery;
+      rc = ensure_graph(h);
+      if (rc) return rc;
+    }
     if (cudaGraphLaunch(h->stepExec, h->stream) != cudaSuccess)
       return set_err(h, GVIZ_CUDA_ERR_CUDA);
+    h->stepsLaunched++;
+  }
   return GVIZ_CUDA_OK;
 }
 
@@ -339,6 +359,114 @@ void prof_mark(gvizCudaForce *h, const char *name) {
   h->profName[h->nProf] = name;
   cudaEventRecord(h->profEv[h->nProf + 1], h->stream);
   h->nProf++;
+}
+
+// ---- judge of the learned walk ------------------------------------------
+
+__global__ void k_judge_gather(const double2 *__restrict__ rep, const uint32_t *__restrict__ idx,
+                               uint32_t n, double2 *out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = rep[idx[i]];
+}
+
+// The sampled vertices of the checks: `n` distinct ids drawn with a seeded
+// splitmix64 (Floyd's method), ascending.
+static std::vector<uint32_t> judge_sample(size_t V, size_t n, uint64_t seed) {
+  std::vector<uint32_t> out;
+  if (n >= V) {
+    out.resize(V);
+    for (size_t i = 0; i < V; i++) out[i] = (uint32_t)i;
+    return out;
+  }
+  uint64_t st = seed * 0x9e3779b97f4a7c15ULL + 0x7f4a7c159e3779b9ULL;
+  auto next = [&st]() {
+    uint64_t z = (st += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  };
+  std::vector<uint8_t> taken(V, 0);
+  for (size_t j = V - n; j < V; j++) {
+    const size_t t = (size_t)(next() % (uint64_t)(j + 1));
+    const size_t pick = taken[t] ? j : t;
+    taken[pick] = 1;
+  }
+  out.reserve(n);
+  for (size_t i = 0; i < V; i++)
+    if (taken[i]) out.push_back((uint32_t)i);
+  return out;
+}
+
+// One force-only evaluation of the current configuration; the sampled
+// vertices' repulsion goes to out (device).
+static void judge_eval(gvizCudaForce *h, double2 *out) {
+  h->forceOnly = true;
+  h->repVecOut = h->d_judgeRep;
+  enqueue_step(h);
+  h->forceOnly = false;
+  h->repVecOut = nullptr;
+  k_judge_gather<<<(h->judgeN + 255) / 256, 256, 0, h->stream>>>(h->d_judgeRep, h->d_judgeIdx,
+                                                                  h->judgeN, out);
+}
+
+// The learned walk judged by the plain one on sampled vertices: the
+// normalised RMS error of each against exact FP64 repulsion
+// (sqrt(sum |F - F_exact|^2 / sum |F_exact|^2) over the sample). When the
+// learned error is above judgeSlack times the plain walk's at judgeTheta,
+// the learned walk is turned off (farField = 0): the plain walk is its
+// fallback. The layout state is not touched.
+static int far_judge(gvizCudaForce *h) {
+  if (!h->params.farField || !h->d_mlp || h->V == 0) return GVIZ_CUDA_OK;
+  const uint32_t n = (uint32_t)std::min<size_t>(h->judgeSamples, h->V);
+  if (n != h->judgeN || !h->d_judgeIdx) {
+    dfree(h->d_judgeIdx);
+    dfree(h->d_judgeExact);
+    dfree(h->d_judgeOut);
+    h->judgeN = 0;
+    int rc = dalloc(h, &h->d_judgeIdx, n) | dalloc(h, &h->d_judgeExact, n) |
+             dalloc(h, &h->d_judgeOut, 2 * (size_t)n);
+    if (!h->d_judgeRep) rc |= dalloc(h, &h->d_judgeRep, h->V);
+    if (rc) return set_err(h, GVIZ_CUDA_ERR_ALLOC);
+    const std::vector<uint32_t> idx = judge_sample(h->V, n, h->judgeSeed);
+    if (cudaMemcpy(h->d_judgeIdx, idx.data(), n * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+      return set_err(h, GVIZ_CUDA_ERR_CUDA);
+    h->judgeN = n;
+  }
+  cudaMemsetAsync(h->d_status, 0, 4, h->stream);
+  enqueue_exact_judge(h, h->d_judgeIdx, n, h->d_judgeExact);
+  judge_eval(h, h->d_judgeOut);  // the learned walk as configured
+  const gvizCudaForceParams saved = h->params;
+  const bool savedSide = h->farSide;
+  h->params.farField = 0;
+  h->params.theta = h->judgeTheta;
+  h->farSide = false;
+  judge_eval(h, h->d_judgeOut + n);  // the plain walk
+  h->params = saved;
+  h->farSide = savedSide;
+  int rc = sync_and_check(h);
+  if (rc) return rc;
+  std::vector<double2> ex(n), got(2 * (size_t)n);
+  if (cudaMemcpy(ex.data(), h->d_judgeExact, n * 16, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(got.data(), h->d_judgeOut, 2 * (size_t)n * 16, cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  double den = 0.0, eL = 0.0, eP = 0.0;
+  for (uint32_t i = 0; i < n; i++) {
+    const double2 e = ex[i], l = got[i], p = got[n + i];
+    den += e.x * e.x + e.y * e.y;
+    eL += (l.x - e.x) * (l.x - e.x) + (l.y - e.y) * (l.y - e.y);
+    eP += (p.x - e.x) * (p.x - e.x) + (p.y - e.y) * (p.y - e.y);
+  }
+  h->judgeLearned = den > 0.0 ? sqrt(eL / den) : 0.0;
+  h->judgePlain = den > 0.0 ? sqrt(eP / den) : 0.0;
+  h->judgeChecks++;
+  if (!(h->judgeLearned <= h->judgeSlack * h->judgePlain)) {  // NaN falls back too
+    h->params.farField = 0;
+    h->farSide = false;
+    h->judgeFell = 1;
+  }
+  h->graphDirty = true;  // the checks ran other work on the step's buffers
+  return GVIZ_CUDA_OK;
 }
 
 // ---- C ABI ---------------------------------------------------------------
@@ -1511,6 +1639,52 @@ int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threadsOut, int32_t *persi
   return rc;
 }
 
+
+int gvizCudaForceSetFarJudge(gvizCudaForce *h, uint32_t every, uint32_t samples,
+                             double plainTheta, double slack, uint64_t seed) {
+  if (!h || samples == 0 || !(plainTheta > 0.0 && plainTheta < INFINITY) ||
+      !(slack > 0.0 && slack < INFINITY))
+    return GVIZ_CUDA_ERR_ARG;
+  if (samples != h->judgeSamples || seed != h->judgeSeed) h->judgeN = 0;  // new sample
+  h->judgeEvery = every;
+  h->judgeSamples = samples;
+  h->judgeTheta = plainTheta;
+  h->judgeSlack = slack;
+  h->judgeSeed = seed;
+  h->judgeNextAt = h->stepsLaunched;  // the next learned step is checked first
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceJudgeFarField(gvizCudaForce *h, double *learnedErr, double *plainErr,
+                               int32_t *fellBack) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  const int32_t was = h->params.farField;
+  h->judgeLearned = h->judgePlain = 0.0;
+  const int rc = far_judge(h);
+  if (learnedErr) *learnedErr = h->judgeLearned;
+  if (plainErr) *plainErr = h->judgePlain;
+  if (fellBack) *fellBack = (was && !h->params.farField) ? 1 : 0;
+  return rc;
+}
+
+int gvizCudaForceFarJudgeStatus(const gvizCudaForce *h, uint64_t *checks, double *learnedErr,
+                                double *plainErr, int32_t *fellBack) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (checks) *checks = h->judgeChecks;
+  if (learnedErr) *learnedErr = h->judgeLearned;
+  if (plainErr) *plainErr = h->judgePlain;
+  if (fellBack) *fellBack = h->judgeFell;
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceSetCellStackCap(gvizCudaForce *h, uint32_t entries) {
+  if (!h || (entries != 0 && (entries < 32 || entries > 512))) return GVIZ_CUDA_ERR_ARG;
+  h->cellStackCap = entries;
+  h->graphDirty = true;
+  return GVIZ_CUDA_OK;
+}
 
 int gvizCudaForceSetWalkShape(gvizCudaForce *h, uint32_t threads, int32_t persistent) {
   if (!h || threads < 32 || threads > 512 || threads % 32 != 0) return GVIZ_CUDA_ERR_ARG;

@@ -619,7 +619,7 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
 // (k_far_groups: a cell of <= 32 points, sibling cells packed), so the 32
 // targets of a warp always lie in one cell and its parent bounds them. The
 // warp walks the tree once for the whole group with warp-uniform decisions:
-//   leaf         - every target takes the pair term (self excluded);
+//   point        - every target takes the pair term (self excluded);
 //   cell         - opened when its preorder range meets the group's, or when
 //                  the opening test fails from the group's bounding box
 //                  (2h/theta against the distance from the box to the
@@ -628,40 +628,49 @@ __global__ __launch_bounds__(kFarThreads, 5) void k_walk_f32_far(FarArgs fa) {
 //                  monopole term, and one MLP row with the cell seen from
 //                  the group's centroid corrects them all (p1 F + p2
 //                  rot90(F) with each target's own F).
-// Rows are queued per warp and evaluated in 16-row mma.sync tiles, applied
-// in queue order; a group's forces depend only on the group, so the result
-// does not depend on which warp drew it.
+// Because the decisions do not depend on the target, the warp expands the
+// tree 32 cells at a time: each round every lane pops one pending node from
+// the warp's stack in shared memory, loads it (32 independent loads instead
+// of a chain of dependent ones) and classifies it; points go to a point
+// list, accepted cells to a cell list, opened cells push their children
+// (their slots come from the tree build's child records). Full lists are
+// then evaluated by all 32 lanes, each for its own target: 32 points per
+// pass, or 16 cells whose MLP rows form one 16-row mma.sync tile. A push
+// that would overflow the stack is walked in place by the warp with the
+// stackless preorder loop (same decisions, same lists). The order in which
+// terms are summed depends only on the group, so the result does not
+// depend on which warp drew it. Per-target sums are Kahan-compensated.
+// The lists are at most 63 points and 47 cells: a round adds at most 32 of
+// each, and a round runs only while fewer than 32 points and 16 cells wait.
 // ---------------------------------------------------------------------------
 
-// A plain FP32 running sum (the Kahan interface): the cell-group walk's
-// error is set by the far field, thousands of times the rounding of a
-// ~200-term FP32 sum, so it does not pay for compensation.
-struct SumF {
-  float s = 0.f;
-  __device__ __forceinline__ void add(float x) { s += x; }
-  __device__ __forceinline__ double value() const { return (double)s; }
-};
+constexpr int kCellRing = 64;     // point and cell list entries per warp (ring)
+constexpr int kCellStack = 512;   // pending nodes per warp
+constexpr int kCellThreads = 256; // one block of 8 warps shares the staged network
+constexpr int kCellBlocksPerSM = 3;
 
-// per warp: the accepted cells of the current tile (preorder index), each
-// lane's monopole force of each of them, and the tile's rows, which are
-// filled at flush time, one row per lane
+// per warp: the point and cell lists (double-single positions), the MLP
+// tile's rows and outputs, the group's targets and the pending nodes
 struct __align__(16) CellWarpSmem {
+  float4 pPos[kCellRing];  // point: x hi, y hi, x lo, y lo
+  float2 pMR[kCellRing];   // point: mass, radius
+  uint32_t pV[kCellRing];  // point: vertex
+  float4 cPos[kCellRing];  // cell: centre of mass, double-single
+  float2 cMN[kCellRing];   // cell: mass, preorder slot (bits)
   __nv_bfloat16 gx[kFarTile * MLP_XS];
-  float2 gF[kFarTile][32];
-  uint32_t cell[kFarTile];
   float2 out[kFarTile];
   uint32_t tgt[32];
+  uint32_t st[kCellStack];
 };
-
-constexpr int kCellThreads = 384;  // one block of 16 warps shares the staged network
-constexpr int kCellBlocksPerSM = 2;
 constexpr size_t kCellDyn = (kCellThreads / 32) * sizeof(CellWarpSmem);
 
 struct CellArgs {
   FarArgs f;
   const uint4 *groups;
+  const uint4 *kids;
   const uint32_t *nGroups;  // [0] groups written, [1] the walk's task counter
   uint32_t cap;
+  uint32_t stackCap;  // stack entries per warp in use (<= kCellStack)
 };
 
 __device__ __forceinline__ float warp_minf(float x) {
@@ -675,21 +684,78 @@ __device__ __forceinline__ float warp_maxf(float x) {
   return x;
 }
 
-// Evaluates the queued cells: lane r < rows builds row r (cell r seen from
-// the group's centroid), the tile runs on the tensor cores, and every lane
-// adds each row's correction of its own monopole force of that cell.
-__device__ __forceinline__ void cell_flush(const MlpSmem &W, CellWarpSmem &q, int rows,
-                                           const NodeF *__restrict__ nodes,
-                                           const FarCell *__restrict__ cells, float wxh,
-                                           float wxl, float wyh, float wyl, float wrv,
-                                           float &corrx, float &corry) {
-  const int lane = threadIdx.x & 31;
+// One group's walk state: this lane's target and sums, the group's centroid
+// and bounding box, and the warp-uniform list cursors.
+struct CellTarget {
+  uint32_t v;
+  bool has;
+  float vxh, vxl, vyh, vyl, mv, rv;
+};
+
+struct CellGroup {
+  float wxh, wxl, wyh, wyl, wrv;  // centroid (double-single) and mean radius
+  float bx0, bx1, by0, by1;       // bounding box of the targets (hi parts)
+  uint32_t gx, gy;                // the group's preorder range
+};
+
+struct CellSums {
+  Kahan kx, ky;
+  float corrx = 0.f, corry = 0.f;
+  uint32_t ph = 0, pn = 0, ch = 0, cn = 0;  // list heads and lengths
+  unsigned long long nInter = 0, nRows = 0;  // instrumentation only
+};
+
+// Every target takes the pair term of the first k listed points.
+template <int MODEL, bool OVERLAP, bool COUNT>
+__device__ __forceinline__ void cell_eval_points(const WalkArgs &a, CellWarpSmem &q,
+                                                 const CellTarget &t, CellSums &s, uint32_t k) {
   __syncwarp();
-  if (lane < rows) {
-    const uint32_t cc = q.cell[lane];
-    const float4 n0 = __ldg(reinterpret_cast<const float4 *>(nodes + cc));
-    const float4 c0 = __ldg(reinterpret_cast<const float4 *>(cells + cc));
-    const uint4 c1 = __ldg(reinterpret_cast<const uint4 *>(cells + cc) + 1);
+#pragma unroll 4
+  for (uint32_t j = 0; j < k; j++) {
+    const uint32_t e = (s.ph + j) & (kCellRing - 1);
+    const float4 p = q.pPos[e];
+    const float2 mr = q.pMR[e];
+    const uint32_t u = q.pV[e];
+    const float dx = (p.x - t.vxh) + (p.z - t.vxl);
+    const float dy = (p.y - t.vyh) + (p.w - t.vyl);
+    const float d2 = dx * dx + dy * dy;
+    const bool doForce = t.has && u != t.v;
+    float fx = 0.f, fy = 0.f;
+    if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {  // coincident points: rare
+      if (doForce)
+        rep_term<MODEL, OVERLAP>(dx, dy, d2, t.mv, mr.x, t.rv + mr.y, a.num, a.overlapC, t.v,
+                                 u, fx, fy);
+    } else if (doForce) {
+      rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, mr.x, t.rv + mr.y, a.num, a.overlapC,
+                                     fx, fy);
+    }
+    if (doForce) {
+      s.kx.add(fx);
+      s.ky.add(fy);
+      if (COUNT) s.nInter++;
+    }
+  }
+  s.ph = (s.ph + k) & (kCellRing - 1);
+  s.pn -= k;
+  __syncwarp();
+}
+
+// The first k <= 16 listed cells: lane r < k builds row r (cell r seen from
+// the group's centroid), the tile runs on the tensor cores, then every
+// target adds each cell's monopole term and the row's correction of it.
+template <int MODEL, bool OVERLAP, bool COUNT>
+__device__ __forceinline__ void cell_eval_cells(const WalkArgs &a, const FarCell *__restrict__ cells,
+                                                const MlpSmem &W, CellWarpSmem &q,
+                                                const CellTarget &t, const CellGroup &g,
+                                                CellSums &s, uint32_t k) {
+  const uint32_t lane = threadIdx.x & 31u;
+  __syncwarp();
+  if (lane < k) {
+    const uint32_t e = (s.ch + lane) & (kCellRing - 1);
+    const float4 p = q.cPos[e];
+    const uint32_t node = __float_as_uint(q.cMN[e].y);
+    const float4 c0 = __ldg(reinterpret_cast<const float4 *>(cells + node));
+    const uint4 c1 = __ldg(reinterpret_cast<const uint4 *>(cells + node) + 1);
     FarCell c;
     c.qa = c0.x;
     c.qb = c0.y;
@@ -699,18 +765,57 @@ __device__ __forceinline__ void cell_flush(const MlpSmem &W, CellWarpSmem &q, in
     c.oy = __uint_as_float(c1.y);
     c.s0 = c1.z;
     c.s1 = c1.w;
-    const float wdx = (n0.x - wxh) + (n0.z - wxl);
-    const float wdy = (n0.y - wyh) + (n0.w - wyl);
+    const float wdx = (p.x - g.wxh) + (p.z - g.wxl);
+    const float wdy = (p.y - g.wyh) + (p.w - g.wyl);
     const float wd2 = wdx * wdx + wdy * wdy;
     float f[MLP_IN], e1x, e1y;
-    far_features(wdx, wdy, wd2, c, wrv, f, e1x, e1y);
+    far_features(wdx, wdy, wd2, c, OVERLAP ? g.wrv : 0.f, f, e1x, e1y);
     far_put_row(q.gx + lane * MLP_XS, f);
   }
   __syncwarp();
   mlp_forward_tile<true>(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
   __syncwarp();
-  for (int r = 0; r < rows; r++) far_apply(q.out[r], q.gF[r][lane], corrx, corry);
+#pragma unroll 4
+  for (uint32_t r = 0; r < k; r++) {
+    const uint32_t e = (s.ch + r) & (kCellRing - 1);
+    const float4 p = q.cPos[e];
+    const float m = q.cMN[e].x;
+    const float dx = (p.x - t.vxh) + (p.z - t.vxl);
+    const float dy = (p.y - t.vyh) + (p.w - t.vyl);
+    const float d2 = dx * dx + dy * dy;
+    float fx = 0.f, fy = 0.f;
+    if (__any_sync(0xffffffffu, t.has && !(d2 > 0.0f))) {
+      if (t.has)
+        rep_term<MODEL, OVERLAP>(dx, dy, d2, t.mv, m, t.rv, a.num, a.overlapC, t.v, t.v, fx, fy);
+    } else if (t.has) {
+      rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, m, t.rv, a.num, a.overlapC, fx, fy);
+    }
+    if (t.has) {
+      s.kx.add(fx);
+      s.ky.add(fy);
+      far_apply(q.out[r], make_float2(fx, fy), s.corrx, s.corry);
+      if (COUNT) s.nInter++;
+    }
+  }
+  if (COUNT) s.nRows += k;
+  s.ch = (s.ch + k) & (kCellRing - 1);
+  s.cn -= k;
   __syncwarp();
+}
+
+// Classification of node `cur` (record n0, n1) for the group: 0 nothing
+// (empty), 1 point, 2 accepted cell, 3 opened cell.
+__device__ __forceinline__ int cell_classify(const CellGroup &g, uint32_t cur, float4 n0,
+                                             float4 n1) {
+  const float nmass = n1.x, nsize = n1.y;
+  const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
+  if (nmass == 0.0f) return 0;  // empty: skipped as the reference does
+  if (ninfo >= 0) return 1;
+  const uint32_t skip = max((uint32_t)nnext, cur + 1u);
+  if (cur < g.gy && skip > g.gx) return 3;  // holds targets of the group
+  const float ex = fmaxf(fmaxf(g.bx0 - n0.x, n0.x - g.bx1), 0.0f);
+  const float ey = fmaxf(fmaxf(g.by0 - n0.y, n0.y - g.by1), 0.0f);
+  return nsize < ex * ex + ey * ey ? 2 : 3;
 }
 
 template <int MODEL, bool OVERLAP, bool COUNT>
@@ -721,14 +826,16 @@ __global__ __launch_bounds__(kCellThreads, kCellBlocksPerSM) void k_walk_f32_cel
   mlp_stage(W, ca.f.mlp);
   const WalkArgs &a = ca.f.w;
   const FarCell *__restrict__ cells = ca.f.cells;
+  const uint4 *__restrict__ kids = ca.kids;
   CellWarpSmem &q = Q[threadIdx.x >> 5];
-  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t below = (1u << lane) - 1u;
   for (int e = lane; e < kFarTile * MLP_XS / 8; e += 32)
     reinterpret_cast<uint4 *>(q.gx)[e] = make_uint4(0u, 0u, 0u, 0u);
   __syncthreads();
   const uint32_t nGroups = min(ca.nGroups[0], ca.cap);
   uint32_t *queue = const_cast<uint32_t *>(ca.nGroups) + 1;
-  unsigned long long nInter = 0, nVisit = 0, nRows = 0, nGrp = 0;
+  unsigned long long nInter = 0, nVisit = 0, nRows = 0, nGrp = 0, nSerial = 0;
   for (;;) {
     uint32_t gi = 0;
     if (lane == 0) gi = atomicAdd(queue, 1u);
@@ -741,119 +848,191 @@ __global__ __launch_bounds__(kCellThreads, kCellBlocksPerSM) void k_walk_f32_cel
       const uint32_t j = b + lane;
       const int32_t info = j < G.y ? __ldg(reinterpret_cast<const int4 *>(a.nodes + j) + 1).w : -1;
       const uint32_t ball = __ballot_sync(0xffffffffu, info >= 0);
-      const uint32_t r = found + __popc(ball & ((1u << lane) - 1u));
+      const uint32_t r = found + __popc(ball & below);
       if (info >= 0 && r < 32u) q.tgt[r] = (uint32_t)info;
       found += __popc(ball);
     }
     __syncwarp();
     const uint32_t nT = min(found, 32u);
-    const bool has = lane < nT;
-    const uint32_t v = has ? q.tgt[lane] : 0u;
+    CellTarget t;
+    t.has = lane < nT;
+    t.v = t.has ? q.tgt[lane] : 0u;
     __syncwarp();
     if (nT == 0) continue;
-    const uint32_t v0 = __shfl_sync(0xffffffffu, v, 0);
-    const uint32_t g = a.gid ? a.gid[v0] : 0u;
-    if (a.active && a.active[g] == 0u) continue;
-    const uint32_t root = a.graphBase[g];
-    const uint32_t end = min(root + a.rootT[g], a.maxNodes);
-    float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
+    const uint32_t v0 = __shfl_sync(0xffffffffu, t.v, 0);
+    const uint32_t gr = a.gid ? a.gid[v0] : 0u;
+    if (a.active && a.active[gr] == 0u) continue;
+    const uint32_t root = a.graphBase[gr];
+    const uint32_t end = min(root + a.rootT[gr], a.maxNodes);
+    t.vxh = t.vxl = t.vyh = t.vyl = t.mv = t.rv = 0.f;
     double2 pv = make_double2(0.0, 0.0);
-    if (has) {
-      pv = a.pos[v];
-      ds_split(pv.x, vxh, vxl);
-      ds_split(pv.y, vyh, vyl);
-      mv = a.massF[v];
-      if (OVERLAP) rv = a.radiusF[v];
+    if (t.has) {
+      pv = a.pos[t.v];
+      ds_split(pv.x, t.vxh, t.vxl);
+      ds_split(pv.y, t.vyh, t.vyl);
+      t.mv = a.massF[t.v];
+      if (OVERLAP) t.rv = a.radiusF[t.v];
     }
-    float wxh, wxl, wyh, wyl, wr2, wrv;
-    group_centroid<32, OVERLAP>(has, pv, vxh, vxl, vyh, vyl, rv, wxh, wxl, wyh, wyl, wr2, wrv);
-    const float bx0 = warp_minf(has ? vxh : INFINITY), bx1 = warp_maxf(has ? vxh : -INFINITY);
-    const float by0 = warp_minf(has ? vyh : INFINITY), by1 = warp_maxf(has ? vyh : -INFINITY);
-    SumF kx, ky;
-    float corrx = 0.f, corry = 0.f;
-    int qg = 0;
+    CellGroup g;
+    float wr2;
+    group_centroid<32, OVERLAP>(t.has, pv, t.vxh, t.vxl, t.vyh, t.vyl, t.rv, g.wxh, g.wxl,
+                                g.wyh, g.wyl, wr2, g.wrv);
+    g.bx0 = warp_minf(t.has ? t.vxh : INFINITY);
+    g.bx1 = warp_maxf(t.has ? t.vxh : -INFINITY);
+    g.by0 = warp_minf(t.has ? t.vyh : INFINITY);
+    g.by1 = warp_maxf(t.has ? t.vyh : -INFINITY);
+    g.gx = G.x;
+    g.gy = G.y;
+    CellSums s;
     const unsigned long long visit0 = nVisit;
     if (COUNT) nGrp++;
-    for (uint32_t cur = root; cur < end;) {
-      const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
-      const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
-      const float nmass = n1.x, nsize = n1.y;
-      const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
-      const uint32_t skip = max((uint32_t)nnext, cur + 1u);
-      if (COUNT) nVisit++;
-      if (nmass == 0.0f) {  // empty: skipped as the reference does
-        cur = skip;
+    // pending nodes (stack), the in-place walk of a subtree that did not
+    // fit the stack [serCur, serEnd), and the lanes whose subtrees wait for
+    // it (each holds its range in sLo, sHi); all warp-uniform but sLo/sHi
+    uint32_t top = 0, serCur = 0, serEnd = 0, pendS = 0, sLo = 0, sHi = 0;
+    if (root < end) {
+      if (lane == 0) q.st[0] = root;
+      top = 1;
+    }
+    __syncwarp();
+    // Each pass either evaluates a full list (or, once nothing is left to
+    // expand, what remains) or expands more of the tree.
+    for (;;) {
+      const bool more = serCur < serEnd || pendS != 0u || top > 0u;
+      if (s.pn >= 32u || (!more && s.pn > 0u)) {
+        cell_eval_points<MODEL, OVERLAP, COUNT>(a, q, t, s, min(s.pn, 32u));
         continue;
       }
-      const float dx = (n0.x - vxh) + (n0.z - vxl);
-      const float dy = (n0.y - vyh) + (n0.w - vyl);
-      const float d2 = dx * dx + dy * dy;
-      if (ninfo >= 0) {  // a point: pair term for every other target
-        const bool doForce = has && (uint32_t)ninfo != v;
-        float fx = 0.f, fy = 0.f;
-        if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {
-          if (doForce) {
-            rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + nsize, a.num, a.overlapC, v,
-                                     (uint32_t)ninfo, fx, fy);
-            kx.add(fx);
-            ky.add(fy);
+      if (s.cn >= (uint32_t)kFarTile || (!more && s.cn > 0u)) {
+        cell_eval_cells<MODEL, OVERLAP, COUNT>(a, cells, W, q, t, g, s,
+                                               min(s.cn, (uint32_t)kFarTile));
+        continue;
+      }
+      if (!more) break;
+      if (serCur < serEnd) {
+        // the stackless preorder walk, one node at a time, until a list fills
+        while (serCur < serEnd && s.pn < 32u && s.cn < (uint32_t)kFarTile) {
+          const uint32_t cur = serCur;
+          const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
+          const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+          const uint32_t skip = min(max((uint32_t)__float_as_int(n1.z), cur + 1u), serEnd);
+          if (COUNT) nVisit++;
+          const int kind = cell_classify(g, cur, n0, n1);
+          if (kind == 1 && lane == 0) {
+            const uint32_t e = (s.ph + s.pn) & (kCellRing - 1);
+            q.pPos[e] = n0;
+            q.pMR[e] = make_float2(n1.x, n1.y);
+            q.pV[e] = (uint32_t)__float_as_int(n1.w);
           }
-        } else if (doForce) {
-          rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + nsize, a.num, a.overlapC,
-                                         fx, fy);
-          kx.add(fx);
-          ky.add(fy);
+          if (kind == 2 && lane == 0) {
+            const uint32_t e = (s.ch + s.cn) & (kCellRing - 1);
+            q.cPos[e] = n0;
+            q.cMN[e] = make_float2(n1.x, __uint_as_float(cur));
+          }
+          s.pn += kind == 1 ? 1u : 0u;
+          s.cn += kind == 2 ? 1u : 0u;
+          serCur = kind == 3 ? cur + 1u : skip;
         }
-        if (COUNT && doForce) nInter++;
-        cur = cur + 1u;
         continue;
       }
-      bool accept = false;
-      if (!(cur < G.y && skip > G.x)) {  // outside the group
-        const float ex = fmaxf(fmaxf(bx0 - n0.x, n0.x - bx1), 0.0f);
-        const float ey = fmaxf(fmaxf(by0 - n0.y, n0.y - by1), 0.0f);
-        accept = nsize < ex * ex + ey * ey;
-      }
-      if (!accept) {
-        cur = cur + 1u;
+      if (pendS) {
+        const int l = __ffs(pendS) - 1;
+        pendS &= pendS - 1u;
+        serCur = __shfl_sync(0xffffffffu, sLo, l);
+        serEnd = __shfl_sync(0xffffffffu, sHi, l);
+        if (COUNT) nSerial++;
         continue;
       }
-      float fx = 0.f, fy = 0.f;
-      if (__any_sync(0xffffffffu, has && !(d2 > 0.0f))) {
-        if (has) rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv, a.num, a.overlapC, v, v, fx, fy);
-      } else if (has) {
-        rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv, a.num, a.overlapC, fx, fy);
+      // one expansion round: up to 32 pending nodes, one per lane
+      const uint32_t n = min(top, 32u);
+      const bool mine = lane < n;
+      const uint32_t cur = mine ? q.st[top - n + lane] : 0u;
+      top -= n;
+      __syncwarp();  // popped before the pushes below reuse the slots
+      float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
+      uint4 kd = make_uint4(GVIZ_NONE, GVIZ_NONE, GVIZ_NONE, GVIZ_NONE);
+      if (mine) {
+        n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
+        n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+        kd = __ldg(kids + cur);  // read for every node; used only when it is opened
       }
-      if (has) {
-        kx.add(fx);
-        ky.add(fy);
+      if (COUNT) nVisit += n;
+      const int kind = mine ? cell_classify(g, cur, n0, n1) : 0;
+      // children inside (cur, end) only: a child record never sends the
+      // walk outside the graph's subtree
+      uint32_t nk = 0;
+      if (kind == 3) {
+        if (kd.y == GVIZ_KIDS_RUN) {
+          nk = (kd.x > cur && kd.x < end) ? min(kd.z, end - kd.x) : 0u;
+          nk = min(nk, (uint32_t)kCellStack + 1u);  // a longer run never fits
+          kd.w = 0u;
+        } else {
+          kd.x = (kd.x > cur && kd.x < end) ? kd.x : GVIZ_NONE;
+          kd.y = (kd.y > cur && kd.y < end) ? kd.y : GVIZ_NONE;
+          kd.z = (kd.z > cur && kd.z < end) ? kd.z : GVIZ_NONE;
+          kd.w = (kd.w > cur && kd.w < end) ? kd.w : GVIZ_NONE;
+          nk = (uint32_t)(kd.x != GVIZ_NONE) + (uint32_t)(kd.y != GVIZ_NONE) +
+               (uint32_t)(kd.z != GVIZ_NONE) + (uint32_t)(kd.w != GVIZ_NONE);
+        }
       }
-      if (COUNT && has) nInter++;
-      q.gF[qg][lane] = make_float2(fx, fy);  // zero for lanes without a target
-      if (lane == 0) q.cell[qg] = cur;
-      if (COUNT) nRows++;
-      if (++qg == kFarTile) {
-        cell_flush(W, q, kFarTile, a.nodes, cells, wxh, wxl, wyh, wyl, OVERLAP ? wrv : 0.f,
-                   corrx, corry);
-        qg = 0;
+      // points and accepted cells join their lists in lane order
+      const uint32_t bP = __ballot_sync(0xffffffffu, kind == 1);
+      if (kind == 1) {
+        const uint32_t e = (s.ph + s.pn + __popc(bP & below)) & (kCellRing - 1);
+        q.pPos[e] = n0;
+        q.pMR[e] = make_float2(n1.x, n1.y);
+        q.pV[e] = (uint32_t)__float_as_int(n1.w);
       }
-      cur = skip;
+      s.pn += __popc(bP);
+      const uint32_t bC = __ballot_sync(0xffffffffu, kind == 2);
+      if (kind == 2) {
+        const uint32_t e = (s.ch + s.cn + __popc(bC & below)) & (kCellRing - 1);
+        q.cPos[e] = n0;
+        q.cMN[e] = make_float2(n1.x, __uint_as_float(cur));
+      }
+      s.cn += __popc(bC);
+      // opened cells push their children (lane order) while they fit; the
+      // rest wait for the in-place walk
+      uint32_t incl = nk;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += y;
+      }
+      const bool fits = top + incl <= ca.stackCap;
+      if (kind == 3 && fits) {
+        const uint32_t base = top + incl - nk;
+        if (kd.y == GVIZ_KIDS_RUN) {
+          for (uint32_t i = 0; i < nk; i++) q.st[base + i] = kd.x + i;
+        } else {
+          uint32_t w = base;
+          if (kd.x != GVIZ_NONE) q.st[w++] = kd.x;
+          if (kd.y != GVIZ_NONE) q.st[w++] = kd.y;
+          if (kd.z != GVIZ_NONE) q.st[w++] = kd.z;
+          if (kd.w != GVIZ_NONE) q.st[w++] = kd.w;
+        }
+      }
+      top += __reduce_max_sync(0xffffffffu, fits ? incl : 0u);
+      pendS = __ballot_sync(0xffffffffu, kind == 3 && !fits);
+      if (kind == 3 && !fits) {
+        sLo = cur + 1u;
+        sHi = min(max((uint32_t)__float_as_int(n1.z), cur + 1u), end);
+      }
+      __syncwarp();
     }
-    if (qg > 0)
-      cell_flush(W, q, qg, a.nodes, cells, wxh, wxl, wyh, wyl, OVERLAP ? wrv : 0.f, corrx,
-                 corry);
-    if (COUNT && lane == 0) {  // the longest group walk and its group
-      const unsigned long long len = nVisit - visit0;
-      const float ext = fmaxf(bx1 - bx0, by1 - by0);
-      if (atomicMax(a.counters + 4, len) < len) {
-        atomicExch(a.counters + 5, ((unsigned long long)nT << 32) | __float_as_uint(ext));
+    if (COUNT) {
+      nInter += s.nInter;
+      if (lane == 0) {
+        nRows += s.nRows;
+        const unsigned long long len = nVisit - visit0;
+        atomicMax(a.counters + 4, len);  // the longest group walk
+        atomicAdd(a.counters + 6, (unsigned long long)nT);
       }
-      atomicAdd(a.counters + 6, (unsigned long long)nT);
     }
-    if (has) {
-      const float2 at = a.attF[v];
-      force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value() + (double)corrx,
-                     ky.value() + (double)corry);
+    if (t.has) {
+      const float2 at = a.attF[t.v];
+      force_epilogue(a.epi, t.v, (double)at.x, (double)at.y, s.kx.value() + (double)s.corrx,
+                     s.ky.value() + (double)s.corry);
     }
   }
   if (COUNT) {
@@ -861,11 +1040,11 @@ __global__ __launch_bounds__(kCellThreads, kCellBlocksPerSM) void k_walk_f32_cel
     if (lane == 0) {
       atomicAdd(a.counters + 1, nVisit);
       atomicAdd(a.counters + 2, nRows);
+      atomicAdd(a.counters + 5, nSerial);
       atomicAdd(a.counters + 7, nGrp);
     }
   }
 }
-
 // ---------------------------------------------------------------------------
 // Hub targets of the learned walk. LinLog's pair force scales with the
 // target's mass, so the heaviest targets carry most of the force and their
@@ -1301,6 +1480,9 @@ static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *coun
     CellArgs ca;
     ca.f = fa;
     ca.groups = h->d_groups;
+    ca.kids = h->d_kids;
+    ca.stackCap = (h->cellStackCap >= 32 && h->cellStackCap <= (uint32_t)kCellStack)
+                      ? h->cellStackCap : (uint32_t)kCellStack;
     ca.nGroups = h->d_groupCount;
     ca.cap = (uint32_t)(h->V ? h->V : 1);
     if (h->model == GVIZ_CUDA_MODEL_FR) {

@@ -7,6 +7,7 @@
 #include "gvizcuda.h"
 
 #define GVIZ_NONE 0xFFFFFFFFu
+#define GVIZ_KIDS_RUN 0xFFFFFFFEu  // child record of a cell whose children are a run of points
 #define GVIZ_LEAF_BIT 0x80000000u
 #define GVIZ_MAX_NODES_PER_CELL 256
 #define GVIZ_CHUNK 2048          // vertices per reduction chunk
@@ -145,6 +146,7 @@ struct gvizCudaForce {
   uint32_t walkThreads = 0;
   bool walkPersistent = false;
   uint32_t walkResident = 0;
+  uint32_t cellStackCap = 0;  // learned cell-group walk: stack entries per warp (0: all)
   ChunkStat *d_chunkStat = nullptr;
   uint32_t *d_status = nullptr;
 
@@ -189,11 +191,26 @@ struct gvizCudaForce {
   uint32_t *d_leafPre = nullptr;    // per vertex: preorder index of its leaf
   uint32_t *d_cellCnt = nullptr;    // per cell node: points below it
   uint4 *d_groups = nullptr;        // target groups: preorder [x, y), z points
+  uint4 *d_kids = nullptr;          // per cell: children's preorder slots (tree.cu)
   uint32_t *d_groupCount = nullptr; // [0] groups written, [1] walk queue
   // hub targets of the learned walk (params.farHubTargets heaviest vertices)
   uint32_t *d_farHubs = nullptr;  // nFarHubs ids, then the walk's hub counter
   double2 *d_farHubOut = nullptr;
   uint32_t nFarHubs = 0;
+
+  // --- judge of the learned walk (api.cu far_judge) ---
+  uint32_t judgeEvery = 0;       // steps between automatic checks (0: none)
+  uint32_t judgeSamples = 4096;  // sampled target vertices per check
+  double judgeTheta = 0.5;       // the plain walk's opening threshold
+  double judgeSlack = 1.0;       // learned error may be this times the plain one
+  uint64_t judgeSeed = 1;
+  uint64_t judgeChecks = 0, judgeNextAt = 0, stepsLaunched = 0;
+  double judgeLearned = 0.0, judgePlain = 0.0;
+  int32_t judgeFell = 0;
+  uint32_t judgeN = 0;             // samples the buffers below hold
+  uint32_t *d_judgeIdx = nullptr;  // sampled vertices, ascending
+  double2 *d_judgeExact = nullptr, *d_judgeOut = nullptr;  // n; 2n (learned, plain)
+  double2 *d_judgeRep = nullptr;   // V: repulsion of one evaluation
 
   // --- CUDA graph of one step ---
   cudaGraphExec_t stepExec = nullptr;

@@ -17,9 +17,14 @@
 // GVIZ_NOALLOC_MAX_CHUNKS * 2 doubles (64 KiB), which every GPU that loads the
 // library holds until the process exits.
 //
-// Compiled with --fmad=false like precise.cu, so the results are bit-identical
-// to the handle-based step for the same inputs.
+// Compiled with --fmad=false like precise.cu, and the partial sums are added
+// in the same order as the handle-based step's (per chunk a strided loop and
+// a block reduction, then over the chunks a strided loop and a block
+// reduction), so for one layout the results are bit-identical to the
+// handle-based FP64 step for the same inputs.
 #include <math.h>
+
+#include <atomic>
 
 #include "internal.cuh"
 
@@ -75,15 +80,20 @@ __global__ __launch_bounds__(kThreads) void k_na_swing(
   }
 }
 
-// updateGlobalSpeed on the chunk partials, in chunk order.
-__global__ void k_na_speed(const double *scratch, uint32_t nChunks, uint32_t n,
-                           double jitterTolerance, double *state) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// updateGlobalSpeed on the chunk partials: one block, thread t adds chunks
+// t, t + kThreads, ..., then the block reduction (the order of k_fa2_speed).
+__global__ __launch_bounds__(kThreads) void k_na_speed(const double *scratch, uint32_t nChunks,
+                                                        uint32_t n, double jitterTolerance,
+                                                        double *state) {
+  __shared__ double sh[kThreads / 32];
   double totalSwing = 0.0, totalTraction = 0.0;
-  for (uint32_t c = 0; c < nChunks; c++) {
+  for (uint32_t c = threadIdx.x; c < nChunks; c += kThreads) {
     totalSwing += scratch[2 * c];
     totalTraction += scratch[2 * c + 1];
   }
+  totalSwing = block_sum_na(totalSwing, sh);
+  totalTraction = block_sum_na(totalTraction, sh);
+  if (threadIdx.x != 0) return;
   if (totalTraction < 1e-7) return;
   double speed = state[0], eff = state[1];
   const double nn = (double)n;
@@ -113,9 +123,11 @@ __global__ void k_na_speed(const double *scratch, uint32_t nChunks, uint32_t n,
 }
 
 // Device address of g_speedScratch per device ordinal, looked up once with
-// that device current. The name g_speedScratch in host code is only a
-// host-side stand-in and must never be passed to a kernel.
-double *g_scratchAddr[64] = {nullptr};
+// that device current and kept for the life of the process (atomics: first
+// calls from several host threads may race to store it; they store the same
+// value). The name g_speedScratch in host code is only a host-side stand-in
+// and must never be passed to a kernel.
+std::atomic<double *> g_scratchAddr[64];
 
 }  // namespace
 
@@ -130,20 +142,21 @@ extern "C" int gvizCudaFa2SpeedUpdateNoAlloc(
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
     return GVIZ_CUDA_ERR_NO_DEVICE;
-  if (!g_scratchAddr[dev]) {
+  double *scratch = g_scratchAddr[dev].load(std::memory_order_acquire);
+  if (!scratch) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_speedScratch) != cudaSuccess || !p)
       return GVIZ_CUDA_ERR_CUDA;
-    g_scratchAddr[dev] = static_cast<double *>(p);
+    scratch = static_cast<double *>(p);
+    g_scratchAddr[dev].store(scratch, std::memory_order_release);
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (nChunks)
     k_na_swing<<<(unsigned)nChunks, kThreads, 0, st>>>(
         reinterpret_cast<const double2 *>(d_structForce),
         reinterpret_cast<const double2 *>(d_oldStructForce), d_mass,
-        (uint32_t)vertexCount, d_swing, g_scratchAddr[dev]);
-  k_na_speed<<<1, 32, 0, st>>>(g_scratchAddr[dev], (uint32_t)nChunks,
-                               (uint32_t)vertexCount, jitterTolerance,
-                               d_speedState);
+        (uint32_t)vertexCount, d_swing, scratch);
+  k_na_speed<<<1, kThreads, 0, st>>>(scratch, (uint32_t)nChunks, (uint32_t)vertexCount,
+                                     jitterTolerance, d_speedState);
   return cudaGetLastError() == cudaSuccess ? GVIZ_CUDA_OK : GVIZ_CUDA_ERR_CUDA;
 }

@@ -602,7 +602,7 @@ __device__ __forceinline__ void walk_up(uint2 u, const uint2 *__restrict__ upInt
 
 struct EM {
   const uint32_t *idx, *bStart, *bGid, *bCnt, *counts, *nFirst, *nLast, *nFlag,
-      *nT, *nCnt, *graphBase;
+      *nT, *nCnt, *graphBase, *nLeft, *nRight;
   const int32_t *nDelta;
   const uint2 *upInt, *upLeaf;
   const double *bM, *bSX, *bSY, *nM, *nSX, *nSY, *mass, *radius;
@@ -619,6 +619,7 @@ struct EM {
   FarCell *cells;
   uint32_t *leafPre;
   uint32_t *cellCnt;  // per cell: points below it (null unless requested)
+  uint4 *kids;        // per cell: its children's preorder slots (null unless requested)
 };
 
 __device__ __forceinline__ void put_count(const EM &a, uint32_t at, uint32_t c) {
@@ -752,6 +753,46 @@ __device__ void put_leaf(const EM &a, uint32_t at, uint32_t v) {
   }
 }
 
+// Children of a cell for walks that expand several cells at once (a cell's
+// first child is the next preorder slot, the others sit behind their elder
+// siblings' subtrees): up to four preorder slots in quadrant order,
+// GVIZ_NONE where a quadrant is empty; a cell whose children are a run of
+// more than four points (a leaf bucket or a capacity leaf) stores
+// {first slot, GVIZ_KIDS_RUN, count}.
+__device__ __forceinline__ uint32_t link_weight(const EM &a, uint32_t c) {
+  const uint2 u = (c & GVIZ_LEAF_BIT) ? a.upLeaf[c & ~GVIZ_LEAF_BIT] : a.upInt[c];
+  return u.y & 0x7fffffffu;
+}
+
+__device__ void put_kids_run(const EM &a, uint32_t at, uint32_t c) {
+  if (!a.kids || at >= a.maxNodes) return;
+  a.kids[at] = c <= 4u ? make_uint4(at + 1u, c > 1u ? at + 2u : GVIZ_NONE,
+                                    c > 2u ? at + 3u : GVIZ_NONE, c > 3u ? at + 4u : GVIZ_NONE)
+                       : make_uint4(at + 1u, GVIZ_KIDS_RUN, c, 0u);
+}
+
+// A quadtree node p: its binary children, or their children where a child
+// was absorbed into p's level (two path bits per quadtree level), each at p's
+// slot plus the weights of the links down to it.
+__device__ void put_kids_quad(const EM &a, uint32_t at, uint32_t p) {
+  if (!a.kids || at >= a.maxNodes) return;
+  uint32_t out[4] = {GVIZ_NONE, GVIZ_NONE, GVIZ_NONE, GVIZ_NONE};
+  int n = 0;
+  const uint32_t ch[2] = {a.nLeft[p], a.nRight[p]};
+  for (int i = 0; i < 2; i++) {
+    const uint32_t c = ch[i];
+    const uint32_t wc = at + link_weight(a, c);
+    if (!(c & GVIZ_LEAF_BIT) && (a.nFlag[c] & 1u)) {
+      const uint32_t g0 = a.nLeft[c], g1 = a.nRight[c];
+      if (n < 4) out[n++] = wc + link_weight(a, g0);
+      if (n < 4) out[n++] = wc + link_weight(a, g1);
+    } else if (n < 4) {
+      out[n++] = wc;
+    }
+  }
+  a.kids[at] = make_uint4(out[0], out[1], out[2], out[3]);
+}
+
 // depth of the nearest quadtree ancestor of a node whose binary parent is p
 __device__ __forceinline__ int quad_parent_depth(const EM &a, uint32_t p) {
   if (p != GVIZ_NONE && (a.nFlag[p] & 1u)) p = a.upInt[p].x;
@@ -779,6 +820,7 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
       put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], INFINITY,
                pre + a.nT[p]);
       put_count(a, pre, s1 - s0);
+      put_kids_run(a, pre, s1 - s0);
       uint32_t ids[GVIZ_MAX_NODES_PER_CELL];
       uint32_t c = s1 - s0;
       for (uint32_t j = 0; j < c; j++) {
@@ -796,6 +838,7 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
     const int q = (a.nDelta[p] - 32) >> 1;
     put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], ldexp(R.h0, -q),
              pre + a.nT[p]);
+    put_kids_quad(a, pre, p);
     if (a.cells) {
       const uint32_t lb = a.nLast[p];
       const uint32_t s0 = a.bStart[fb];
@@ -826,6 +869,7 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
   const double h = testable ? ldexp(R.h0, -(R.D - 1)) : (double)INFINITY;
   put_cell(a, pre, a.bM[b], a.bSX[b], a.bSY[b], h, pre + 1 + c);
   put_count(a, pre, c);
+  put_kids_run(a, pre, c);
   if (a.cells && testable)
     put_far(a, pre, R, b, R.D - 1, h, a.bQ[b], a.bM[b], a.bSX[b], a.bSY[b], s0,
             s0 + c);
@@ -1062,6 +1106,9 @@ EM make_em(gvizCudaForce *h) {
   a.cells = h->farSide ? h->d_cells : nullptr;
   a.leafPre = h->farSide ? h->d_leafPre : nullptr;
   a.cellCnt = (h->farSide && h->params.farCellGroups) ? h->d_cellCnt : nullptr;
+  a.nLeft = h->d_nLeft;
+  a.nRight = h->d_nRight;
+  a.kids = (h->farSide && h->params.farCellGroups && !a.f64) ? h->d_kids : nullptr;
   return a;
 }
 

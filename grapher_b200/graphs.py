@@ -1,7 +1,9 @@
-"""Workload graphs as numpy arrays, generated by libgvizcuda's host helpers.
+"""Workload graphs as numpy arrays.
 
-Edge lists are ordered (a[i], b[i]) pairs; ``to_csr`` builds adjacency the
-way gvizGraphAddEdge does (src/ds/gvizGraph.c:163-172).
+The generators come from libgvizworkloads (host only; importing them does
+not load libgvizcuda). Edge lists are ordered (a[i], b[i]) pairs;
+``to_csr`` (libgvizcuda) builds adjacency the way gvizGraphAddEdge does
+(src/ds/gvizGraph.c:163-172).
 """
 from __future__ import annotations
 
@@ -13,7 +15,7 @@ from . import _native as N
 
 
 def _gen(fn, *args):
-    L = N.lib()
+    L = N.workloads_lib()
     f = getattr(L, fn)
     E = int(f(*args, None, None))
     a = np.zeros(E, np.uint32)
@@ -24,24 +26,24 @@ def _gen(fn, *args):
 
 def grid(rows, cols):
     """build_rect_mesh (src/utils/graphs.c:285-316)"""
-    return _gen("gvizCudaGenGrid", rows, cols)
+    return _gen("gvizGenGrid", rows, cols)
 
 
 def random_connected(n, density, seed):
     """build_random_connected_graph (src/utils/graphs.c:598-639)"""
-    return _gen("gvizCudaGenRandomConnected", n, float(density), seed)
+    return _gen("gvizGenRandomConnected", n, float(density), seed)
 
 
 def barabasi_albert(n, m, seed):
-    return _gen("gvizCudaGenBarabasiAlbert", n, m, seed)
+    return _gen("gvizGenBarabasiAlbert", n, m, seed)
 
 
 def erdos_renyi(n, m, seed):
-    return _gen("gvizCudaGenErdosRenyi", n, m, seed)
+    return _gen("gvizGenErdosRenyi", n, m, seed)
 
 
 def rmat(scale, draws, a=0.57, b=0.19, c=0.19, seed=1):
-    return _gen("gvizCudaGenRmat", scale, draws, a, b, c, seed)
+    return _gen("gvizGenRmat", scale, draws, a, b, c, seed)
 
 
 def to_csr(V, a, b):

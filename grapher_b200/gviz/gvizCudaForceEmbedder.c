@@ -25,6 +25,8 @@ typedef struct attached {
   double *xy;              /* compact positions, 2V */
   size_t lastIteration;    /* state->iteration after our last step */
   int lastError;
+  int farWanted;           /* the caller turned the learned walk on (handle) */
+  int farPushed;           /* farField as this glue last pushed it */
   struct attached *next;
 } attached;
 
@@ -81,7 +83,14 @@ static int32_t state_model(const gvizForceEmbedderState *s) {
 /* Configuration is re-read before every step: the toggle action and the
  * Configure* setters may run between steps. The learned far-field options
  * have no embedder field; whatever the caller set on the handle
- * (gvizCudaForceEmbedderHandle) is kept. */
+ * (gvizCudaForceEmbedderHandle) is kept, except that the learned walk
+ * (FP32 Barnes-Hut only) is held off while the embedder has Barnes-Hut
+ * off (gvizForceEmbedderSetBarnesHutEnabled,
+ * src/embedders/gvizForceEmbedder.c:381) or the glue runs FP64: the step then
+ * takes the exact or the FP64 walk, as the reference would, and the learned
+ * walk comes back with Barnes-Hut. When something else turns it off (the
+ * caller, or the handle's judge falling back to the plain walk), it stays
+ * off. */
 static int push_params(attached *a) {
   const gvizForceEmbedderState *s = a->state;
   gvizCudaForceParams p;
@@ -101,7 +110,12 @@ static int push_params(attached *a) {
   gvizCudaForceParams cur;
   if (gvizCudaForceGetParams(a->h, &cur) != GVIZ_CUDA_OK)
     return gvizCudaForceSetParams(a->h, &p);
-  p.farField = cur.farField;
+  if (cur.farField)
+    a->farWanted = 1;
+  else if (a->farPushed)
+    a->farWanted = 0; /* turned off since our last push */
+  p.farField = (a->farWanted && p.barnesHutEnabled && p.precision == GVIZ_CUDA_FP32) ? 1 : 0;
+  a->farPushed = p.farField;
   p.farGroupSpread = cur.farGroupSpread;
   p.farCellGroups = cur.farCellGroups;
   p.farHubTargets = cur.farHubTargets;

@@ -295,6 +295,38 @@ class ForceLayout:
                 "gvizCudaForceAutotune")
         return int(t.value), bool(p.value), float(ms.value)
 
+    def set_far_judge(self, every=0, samples=4096, plain_theta=0.5, slack=1.0, seed=1):
+        """The learned walk's judge (gvizCudaForceSetFarJudge): checks every
+        `every` steps (0: on request) against the plain walk at plain_theta
+        on `samples` vertices; a learned error above slack times the plain
+        one turns the learned walk off."""
+        N.check(self.L.gvizCudaForceSetFarJudge(self.h, every, samples, float(plain_theta),
+                                                 float(slack), seed),
+                "gvizCudaForceSetFarJudge")
+
+    def judge_far_field(self):
+        """One check now: (learned error, plain error, fell back)."""
+        le, pe, fb = C.c_double(), C.c_double(), C.c_int32()
+        N.check(self.L.gvizCudaForceJudgeFarField(self.h, C.byref(le), C.byref(pe),
+                                                   C.byref(fb)),
+                "gvizCudaForceJudgeFarField")
+        return le.value, pe.value, bool(fb.value)
+
+    def far_judge_status(self):
+        """(checks run, last learned error, last plain error, fell back)."""
+        n, le, pe, fb = C.c_uint64(), C.c_double(), C.c_double(), C.c_int32()
+        N.check(self.L.gvizCudaForceFarJudgeStatus(self.h, C.byref(n), C.byref(le),
+                                                    C.byref(pe), C.byref(fb)),
+                "gvizCudaForceFarJudgeStatus")
+        return n.value, le.value, pe.value, bool(fb.value)
+
+    def set_cell_stack_cap(self, entries):
+        """Stack entries per warp of the learned cell-group walk (32..512; 0
+        restores 512): a tuning and test knob, forces agree up to the order
+        of the per-target sums."""
+        N.check(self.L.gvizCudaForceSetCellStackCap(self.h, entries),
+                "gvizCudaForceSetCellStackCap")
+
     def set_walk_shape(self, threads, persistent):
         N.check(self.L.gvizCudaForceSetWalkShape(self.h, threads, int(persistent)),
                 "gvizCudaForceSetWalkShape")

@@ -233,9 +233,9 @@ int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
  * the cell fails the opening test seen from their centroid. Cell-group walk
  * (farCellGroups 1): groupRows = one row per group and accepted cell,
  * laneRows = 0, and laneRowCause = {node visits of the longest group walk,
- * that group's target count << 32 | the FP32 bits of its bounding-box
- * extent, targets walked over all groups}. Zeros when the correction is
- * off. */
+ * subtrees walked in place because the stack was full
+ * (gvizCudaForceSetCellStackCap), targets walked over all groups}. Zeros
+ * when the correction is off. */
 int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows,
                               uint64_t *laneRows, uint64_t *laneRowCause);
 
@@ -401,9 +401,14 @@ int64_t gvizCudaGripKNearest(size_t vertexCount, const uint64_t *rowOffsets,
  * which every GPU that loads the library holds until the process exits.
  * Limit: vertexCount <= 4096 * 2048 (8,388,608); larger counts return
  * GVIZ_CUDA_ERR_LIMIT. The first call on each device looks up that array's
- * device address with the device current; make that first call before any
- * stream capture. All calls share the array, so calls that overlap on the
- * GPU (different streams without ordering between them) race. */
+ * device address with the device current and keeps it for the life of the
+ * process; make that first call before any stream capture, and do not call
+ * this entry point on a device after cudaDeviceReset of that device (the
+ * kept address belonged to the context the reset destroyed). All calls
+ * share the array, so calls that overlap on the GPU (different streams
+ * without ordering between them) race. Host threads may make first calls
+ * concurrently. For one layout the results are bit-identical to the FP64
+ * handle-based step's (the same sums in the same order). */
 int gvizCudaFa2SpeedUpdateNoAlloc(const double *d_structForce,
                                   const double *d_oldStructForce,
                                   const double *d_mass, size_t vertexCount,
@@ -423,6 +428,41 @@ int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threads,
 /* Sets the FP32 walk's launch shape directly: threads per block (a multiple
  * of 32, at most 512) and the persistent schedule (1) or the static one. */
 int gvizCudaForceSetWalkShape(gvizCudaForce *h, uint32_t threads, int32_t persistent);
+
+/* The judge of the learned walk (no reference counterpart): the plain
+ * Barnes-Hut walk stays both the learned walk's fallback and the judge of
+ * its error. A check evaluates, on the current positions, the learned walk
+ * as configured and the plain walk at plainTheta, and compares each with
+ * exact FP64 all-pairs repulsion on `samples` vertices (a seeded sample,
+ * drawn once): error = sqrt(sum |F - F_exact|^2 / sum |F_exact|^2) over the
+ * sample. When the learned error is above slack times the plain walk's, the
+ * handle turns the learned walk off (farField = 0; GetParams shows it) and
+ * later steps take the plain walk. The layout state is not changed.
+ * With every > 0 a check runs before every `every`-th step replayed while
+ * the learned walk is on (Step, StepHost, EnqueueSteps, Run, TimeSteps;
+ * the first one before the next such step); every = 0 checks only on
+ * request. Defaults: every 0, samples 4096, plainTheta 0.5, slack 1, seed 1. */
+int gvizCudaForceSetFarJudge(gvizCudaForce *h, uint32_t every, uint32_t samples,
+                             double plainTheta, double slack, uint64_t seed);
+
+/* One check now (see above); each output may be NULL. fellBack = 1 when this
+ * check turned the learned walk off. Errors are 0 when the learned walk is
+ * off. Synchronous. */
+int gvizCudaForceJudgeFarField(gvizCudaForce *h, double *learnedErr, double *plainErr,
+                               int32_t *fellBack);
+
+/* Checks run so far, the last check's errors, and whether any check turned
+ * the learned walk off. */
+int gvizCudaForceFarJudgeStatus(const gvizCudaForce *h, uint64_t *checks, double *learnedErr,
+                                double *plainErr, int32_t *fellBack);
+
+/* The learned cell-group walk expands the tree 32 cells at a time through a
+ * per-warp stack of pending nodes in shared memory (512 entries); a subtree
+ * whose children do not fit is walked in place instead. Sets the stack
+ * entries the walk may use, 32 to 512 (0 restores 512); forces agree up to
+ * the order of the per-target sums. A tuning and test knob. No reference
+ * counterpart. */
+int gvizCudaForceSetCellStackCap(gvizCudaForce *h, uint32_t entries);
 
 /* ---- checkpoints ------------------------------------------------------ */
 
@@ -487,27 +527,7 @@ int gvizCudaLoadObjFile(const char *path, gvizCudaCsr *out);
 
 void gvizCudaCsrFree(gvizCudaCsr *csr);
 
-/* ---- host helpers: workloads and initial placement ------------------- */
-
-/* Ordered undirected edge lists. Each returns the edge count; pass NULL
- * buffers to query it first. */
-/* build_rect_mesh (src/utils/graphs.c:285-316) */
-size_t gvizCudaGenGrid(size_t rows, size_t cols, uint32_t *ea, uint32_t *eb);
-/* build_random_connected_graph (src/utils/graphs.c:598-639), same rand_r
- * stream, same edge order */
-size_t gvizCudaGenRandomConnected(size_t n, double density, unsigned seed,
-                                  uint32_t *ea, uint32_t *eb);
-/* Barabasi-Albert: K_{m+1} seed, then each new vertex attaches m distinct
- * targets chosen proportionally to degree; 4n - 10 edges for m = 4 */
-size_t gvizCudaGenBarabasiAlbert(size_t n, uint32_t m, uint64_t seed,
-                                 uint32_t *ea, uint32_t *eb);
-/* Erdos-Renyi G(n, m): m distinct non-loop edges */
-size_t gvizCudaGenErdosRenyi(size_t n, size_t m, uint64_t seed, uint32_t *ea,
-                             uint32_t *eb);
-/* R-MAT with (a, b, c, 1-a-b-c): `draws` edge draws, self-loops dropped,
- * duplicates (either orientation) removed, first occurrence kept */
-size_t gvizCudaGenRmat(uint32_t scale, size_t draws, double a, double b,
-                       double c, uint64_t seed, uint32_t *ea, uint32_t *eb);
+/* ---- host helpers: adjacency and initial placement ------------------- */
 
 /* CSR exactly as gvizGraphAddEdge builds adjacency lists for an undirected
  * graph (src/ds/gvizGraph.c:163-172): edge (a,b) appends b to a's list and

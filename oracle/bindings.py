@@ -406,6 +406,10 @@ class RefLayout:
     def set_prevent_overlap(self, on):
         self.L.ref_set_prevent_overlap(self.h, C.c_int(1 if on else 0))
 
+    def set_barnes_hut(self, on):
+        """gvizForceEmbedderSetBarnesHutEnabled (a live toggle)."""
+        self.L.ref_set_barnes_hut(self.h, C.c_int(1 if on else 0))
+
     def begin(self, seed):
         return self.L.ref_begin(self.h, C.c_uint(seed))
 

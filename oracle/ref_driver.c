@@ -106,6 +106,9 @@ void ref_configure(refLayout *r, const refParams *p, double boxExtent) {
 void ref_set_prevent_overlap(refLayout *r, int on) {
   gvizForceEmbedderSetPreventOverlapEnabled(&r->s, on);
 }
+void ref_set_barnes_hut(refLayout *r, int on) {
+  gvizForceEmbedderSetBarnesHutEnabled(&r->s, on);
+}
 
 int ref_begin(refLayout *r, unsigned seed) {
   return gvizForceEmbedderBegin(&r->s, seed);

@@ -4,6 +4,8 @@ BF16 rounding emulated where the kernels store BF16), the harvested training
 targets against the analytic quadrupole term, and what the trained network
 gains over the same walk without it, judged against exact FP64 all-pairs
 repulsion."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -295,6 +297,33 @@ def test_cell_group_steps_are_deterministic(trained):
     assert np.array_equal(outs[0], outs[1])
 
 
+@pytest.mark.parametrize("theta", [1.0, 1e-4])
+def test_cell_walk_in_place_subtrees_agree(trained, theta):
+    """The expanding cell-group walk with a stack too small for its pushes
+    walks those subtrees in place: the same decisions and the same terms, so
+    the forces agree up to the order of the compensated FP32 sums, and the
+    fallback really ran."""
+    lay, m, targets, exact = trained
+    m.attach(lay)
+    lay.set_params(theta=theta, farField=1, farCellGroups=1)
+    lay.set_cell_stack_cap(0)
+    full = lay.repulsion()
+    _, _, why_full = lay.count_far_rows(causes=True)
+    lay.set_cell_stack_cap(32)
+    try:
+        small = lay.repulsion()
+        g, _, why_small = lay.count_far_rows(causes=True)
+    finally:
+        lay.set_cell_stack_cap(0)
+        lay.set_params(theta=1.0, farField=0, farCellGroups=0)
+    assert why_small[1] > 0 and why_small[2] == lay.V and why_full[2] == lay.V
+    d = np.linalg.norm(small - full, axis=1)
+    n = np.linalg.norm(full, axis=1)
+    assert np.all(np.isfinite(small))
+    assert float(np.sqrt(np.sum(d * d) / np.sum(n * n))) < 1e-6
+    assert float(np.max(d / np.maximum(n, 1e-30))) < 1e-4
+
+
 def _heaviest(lay, k):
     """The k heaviest vertices (LinLog mass deg + 1, ties to the lower id)."""
     deg = np.diff(lay.row).astype(np.int64)
@@ -439,3 +468,62 @@ def test_far_field_argument_checks(trained):
     lay.set_params(farHubTargets=0, farHubTheta=0.35)
     lay.set_params(farHubTargets=1 << 30)   # more than the vertices: all of them
     lay.set_params(farHubTargets=0)
+
+
+# ------------------------------------------------------------ the judge
+def test_judge_keeps_a_good_network_and_drops_a_bad_one(trained):
+    """gvizCudaForceJudgeFarField: the learned walk is judged against the
+    plain walk on sampled vertices, both against exact FP64 repulsion. The
+    trained network at theta = 1.0 beats the plain walk at the same theta and
+    stays on; a network with large random weights does not and the handle
+    falls back to the plain walk (farField 0, later steps plain)."""
+    from grapher_b200 import _native as N
+    lay, m, targets, exact = trained
+    m.attach(lay)
+    lay.set_params(theta=1.0, farField=1, farCellGroups=1)
+    lay.set_far_judge(every=0, samples=2048, plain_theta=1.0, slack=1.0, seed=5)
+    le, pe, fell = lay.judge_far_field()
+    assert not fell and 0 < le < pe, (le, pe)
+    p = N.ForceParams()
+    lay.L.gvizCudaForceGetParams(lay.h, C.byref(p))
+    assert p.farField == 1
+    bad = _model(9)
+    bad.set_weights(np.random.default_rng(1).normal(0, 3.0, bad.nparams).astype(np.float32))
+    bad.attach(lay)
+    le2, pe2, fell2 = lay.judge_far_field()
+    lay.L.gvizCudaForceGetParams(lay.h, C.byref(p))
+    n, l_last, p_last, fell_any = lay.far_judge_status()
+    lay.set_far_judge()
+    lay.set_params(theta=1.0, farField=0, farCellGroups=0)
+    assert fell2 and le2 > pe2 and p.farField == 0
+    assert n >= 2 and fell_any and l_last == le2 and p_last == pe2
+    assert abs(pe2 - pe) <= 1e-12 * pe   # the plain walk's error does not depend on the model
+
+
+def test_judge_every_n_steps_falls_back_to_the_plain_walk(trained):
+    """Automatic checks: with every = 3 the first learned step is checked;
+    a bad network is dropped there, and the steps that follow are exactly
+    the plain walk's steps from the same state."""
+    lay, _, _, _ = trained
+    x_s, (sf, sp, ef) = lay.positions(), lay.fa2_state()
+    bad = _model(11)
+    bad.set_weights(np.random.default_rng(2).normal(0, 3.0, bad.nparams).astype(np.float32))
+    bad.attach(lay)
+    lay.set_params(theta=0.5, farField=1, farCellGroups=1)
+    lay.set_far_judge(every=3, samples=1024, plain_theta=0.5, slack=1.0, seed=3)
+    for _ in range(4):
+        lay.step()
+    judged = lay.positions()
+    n, _, _, fell = lay.far_judge_status()
+    lay.set_far_judge()
+    lay.set_positions(x_s)
+    lay.set_fa2_state(sf, sp, ef)
+    lay.set_params(theta=0.5, farField=0, farCellGroups=0)
+    for _ in range(4):
+        lay.step()
+    plain = lay.positions()
+    lay.set_positions(x_s)
+    lay.set_fa2_state(sf, sp, ef)
+    lay.set_params(theta=1.0)
+    assert fell and n >= 1
+    assert np.array_equal(judged, plain)

@@ -247,3 +247,69 @@ def test_grip_action_switch_bit_identical(ref, glue):
                          capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     assert out.stdout.strip().splitlines()[-1] == "OK", out.stdout[-2000:]
+
+
+def test_learned_walk_through_the_action(ref, glue):
+    """The learned walk behind the drop-in switch: the caller turns it on
+    through the attached handle and "forceEmbedder.step" runs it; the
+    embedder's own Barnes-Hut toggle (gvizForceEmbedderSetBarnesHutEnabled)
+    holds it off while Barnes-Hut is off (an exact step, no error) and it
+    comes back with Barnes-Hut; once the handle's judge falls back to the
+    plain walk, it stays off."""
+    from oracle.bindings import make_params
+
+    from grapher_b200 import _native as N
+    from grapher_b200.farfield import FarFieldModel
+    L = N.lib()
+    glue.gvizCudaForceEmbedderHandle.restype = C.c_void_p
+    glue.gvizCudaForceEmbedderHandle.argtypes = [C.c_void_p]
+    p = make_params(model=1, theta=1.0, gravity=1.0)
+    lrn, pln = twins(ref, 1, p, 100.0, 3, n=3000)
+    opt = Options(0, 0, 0, 0)
+    assert glue.gvizCudaForceAttach(lrn.state_ptr(), C.byref(opt)) == 0
+    assert glue.gvizCudaForceAttach(pln.state_ptr(), C.byref(opt)) == 0
+    h = C.c_void_p(glue.gvizCudaForceEmbedderHandle(lrn.state_ptr()))
+    model = FarFieldModel(seed=4)
+    model.set_weights(np.random.default_rng(6).normal(0, 0.05, model.nparams).astype(np.float32))
+    assert L.gvizCudaForceSetFarFieldModel(h, model.h) == 0
+
+    def far_field():
+        q = N.ForceParams()
+        assert L.gvizCudaForceGetParams(h, C.byref(q)) == 0
+        return q
+
+    q = far_field()
+    q.farField, q.farCellGroups = 1, 1
+    assert L.gvizCudaForceSetParams(h, C.byref(q)) == 0
+    x0 = lrn.positions()
+    lrn.invoke_step_action()
+    pln.invoke_step_action()
+    d_l = (lrn.positions() - x0).reshape(-1, 2)
+    d_p = (pln.positions() - x0).reshape(-1, 2)
+    e = np.linalg.norm(d_l - d_p, axis=1) / np.linalg.norm(d_p, axis=1)
+    assert np.all(np.isfinite(d_l)) and glue.gvizCudaForceEmbedderLastError(lrn.state_ptr()) == 0
+    assert far_field().farField == 1 and lrn.state()["iteration"] == 1
+    assert 0.0 < np.median(e) < 0.05, np.median(e)   # the learned walk ran, close to plain
+    lrn.set_barnes_hut(False)
+    before = lrn.positions()
+    lrn.invoke_step_action()
+    assert glue.gvizCudaForceEmbedderLastError(lrn.state_ptr()) == 0
+    assert far_field().farField == 0 and np.any(lrn.positions() != before)
+    lrn.set_barnes_hut(True)
+    lrn.invoke_step_action()
+    assert far_field().farField == 1
+    # a judge that no network can satisfy sends the layout back to the plain walk
+    assert L.gvizCudaForceSetFarJudge(h, 1, 256, 1.0, 1e-9, 1) == 0
+    lrn.invoke_step_action()
+    assert far_field().farField == 0
+    lrn.set_barnes_hut(False)
+    lrn.invoke_step_action()
+    lrn.set_barnes_hut(True)
+    lrn.invoke_step_action()
+    assert far_field().farField == 0 and glue.gvizCudaForceEmbedderLastError(lrn.state_ptr()) == 0
+    assert lrn.state()["iteration"] == 6
+    for r in (lrn, pln):
+        glue.gvizCudaForceDetach(r.state_ptr())
+    model.close()
+    lrn.close()
+    pln.close()

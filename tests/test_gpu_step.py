@@ -184,3 +184,57 @@ def test_hub_attraction_split_across_warps(model):
         s = d / 10.0 if model == 0 else np.log1p(d) / d
         want = np.linalg.norm((s[:, None] * q).sum(0))
         assert abs(att[v] - want) <= 1e-5 * want, (v, att[v], want)
+
+
+@pytest.mark.parametrize("name", ["traj_grid32_fr_theta05", "traj_rc300_linlog_theta08_grav_overlap",
+                                  "traj_rc500_linlog_theta12_k3"])
+def test_fp32_free_run_tracks_reference_golden(name):
+    """The FP32 path run freely (each step from its own previous state, not
+    the reference's) along the reference's golden trajectory: after every
+    step the positions stay within a small fraction of the distance the
+    reference moved them since the start."""
+    g = golden(name)
+    c = golden_cfg(g)
+    c.update(precision="fp32")
+    V = int(g["V"])
+    row, col = csr_of(V, g["ea"], g["eb"])
+    lay = make_layout(row, col, c)
+    lay.begin(0, positions=g["x0"])
+    x0 = g["x0"]
+    for s in range(g["pos"].shape[0]):
+        lay.step()
+        p = lay.positions()
+        moved = np.linalg.norm((g["pos"][s] - x0).reshape(-1, 2), axis=1)
+        scale = float(np.sqrt(np.mean(moved * moved)))
+        d = np.linalg.norm((p - g["pos"][s]).reshape(-1, 2), axis=1) / scale
+        assert np.median(d) <= 1e-4 and np.quantile(d, 0.99) <= 1e-2, (
+            s, float(np.median(d)), float(np.quantile(d, 0.99)), float(d.max()))
+    lay.close()
+
+
+def test_fp32_free_run_tracks_oracle_as_a_layout(oracle):
+    """100 free FP32 steps of the 32x32 grid (FR, theta = 0.5) against 100 FP64
+    oracle steps from the same start: threshold flips and FP32 rounding make
+    the trajectories drift apart vertex by vertex, but the two layouts agree
+    as layouts (mean edge length and the spread of the vertices)."""
+    from grapher_b200 import graphs
+    a, b = graphs.grid(32, 32)
+    row, col = csr_of(1024, a, b)
+    deg, mass = degree_mass(row, 0)
+    c = cfg(model=0, theta=0.5, precision="fp32")
+    x0 = graphs.randomize_positions(1024, 1.0, 7)
+    pos_o, sf_o, ss_o = x0.copy(), np.zeros(2048), np.array([1.0, 1.0])
+    lay = make_layout(row, col, c)
+    lay.begin(0, positions=x0)
+    for _ in range(100):
+        oracle.step((row, col), mass, deg, oracle_params(c), pos_o, sf_o, ss_o)
+        lay.step()
+    p = lay.positions().reshape(-1, 2)
+    q = pos_o.reshape(-1, 2)
+    e_gpu = np.linalg.norm(p[a] - p[b], axis=1).mean()
+    e_ref = np.linalg.norm(q[a] - q[b], axis=1).mean()
+    r_gpu = np.linalg.norm(p - p.mean(0), axis=1).mean()
+    r_ref = np.linalg.norm(q - q.mean(0), axis=1).mean()
+    assert abs(e_gpu - e_ref) <= 1e-2 * e_ref, (e_gpu, e_ref)
+    assert abs(r_gpu - r_ref) <= 1e-2 * r_ref, (r_gpu, r_ref)
+    lay.close()

@@ -28,6 +28,25 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_workloads_library_exports_its_header_and_stays_apart():
+    """libgvizworkloads exports include/gvizworkloads.h, and it does not pull
+    in libgvizcuda (the CPU reference timing builds its graphs with it)."""
+    import subprocess
+    from grapher_b200 import _native
+    lib = _native.workloads_lib()
+    names = [n for n in re.findall(r"\b(gvizGen\w+)\s*\(",
+                                   re.sub(r"/\*.*?\*/", "",
+                                          open(os.path.join(ROOT, "include",
+                                                            "gvizworkloads.h")).read(),
+                                          flags=re.S))]
+    assert len(names) == 5
+    assert all(hasattr(lib, n) for n in names)
+    assert set(names) <= set(_native._WSIGS)
+    deps = subprocess.run(["ldd", _native.WORKLOADS_PATH], capture_output=True,
+                          text=True).stdout
+    assert "gvizcuda" not in deps and "libcuda" not in deps and "cudart" not in deps
+
+
 def test_glue_library_exports_its_headers():
     """The gviz-side glue (built only where gviz's headers are) exports every
     entry point of include/gvizCudaForceEmbedder.h and gvizCudaGripEmbedder.h."""

@@ -5,10 +5,10 @@ It serves callers that must not allocate device memory while they run, e.g.
 a render loop stepping the layout every frame, or a program whose GPU memory
 belongs to another allocator. The handle-based step sums swing and traction
 in a buffer it allocated; this entry point keeps those partial sums in an
-array built into the library. Same inputs, same arithmetic, same order, so
-the results must agree to the FP64 tolerance the step tests use (1e-12
-relative here; they are expected bit-identical), on two calls in a row
-(the second call reuses the array the first one left behind).
+array built into the library. Same inputs, same arithmetic, same order of
+the sums, so the results must be bit-identical to the FP64 step's, on two
+calls in a row (the second call reuses the array the first one left
+behind).
 This file is named to be collected last."""
 import ctypes as C
 
@@ -58,8 +58,8 @@ def test_speed_update_without_allocation_matches_step():
         assert rc == 0, N.lib().gvizCudaErrorString(rc)
         torch.cuda.synchronize()
         got = d_state.cpu().numpy()
-        np.testing.assert_allclose(got, [speed1[0], eff1[0]], rtol=1e-12, atol=0)
-        np.testing.assert_allclose(d_swing.cpu().numpy(), swing_ref, rtol=1e-12, atol=0)
+        assert got[0] == speed1[0] and got[1] == eff1[0], (call, got, speed1, eff1)
+        assert np.array_equal(d_swing.cpu().numpy(), swing_ref), call
 
 
 def test_speed_update_without_allocation_rejects_oversize():
