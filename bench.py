@@ -584,6 +584,151 @@ def error_trajectory(lay, w, linfo, chunks=5, every=20):
     return out
 
 
+# ----------------------------------------------------------- precision reports
+STRESS_SOURCES = 16
+JUDGE_SAMPLE = 65536
+
+
+def layout_stress(row, col, xy, sources=STRESS_SOURCES, seed=SEED):
+    """Normalised stress of a layout at its best scale, over the pairs
+    (source, vertex) of `sources` seeded breadth-first sources:
+    min_s mean((s |x_i - x_j| - d_ij)^2 / d_ij^2) = 1 - A1^2 / (n A2) with
+    A1 = sum e/d, A2 = sum (e/d)^2 over the n reachable pairs."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import shortest_path
+    V = len(row) - 1
+    A = sp.csr_matrix((np.ones(len(col), np.float32), np.asarray(col, np.int64),
+                       np.asarray(row, np.int64)), shape=(V, V))
+    rng = np.random.default_rng(seed)
+    src = rng.choice(V, min(sources, V), replace=False)
+    D = shortest_path(A, method="D", unweighted=True, indices=src)
+    p = np.asarray(xy).reshape(-1, 2)
+    a1 = a2 = 0.0
+    n = 0
+    for i, s0 in enumerate(src):
+        d = D[i]
+        m = np.isfinite(d) & (d > 0)
+        r = np.linalg.norm(p[m] - p[s0], axis=1) / d[m]
+        a1 += float(r.sum())
+        a2 += float((r * r).sum())
+        n += int(m.sum())
+    return float(1.0 - a1 * a1 / (n * a2)) if n and a2 > 0 else None
+
+
+def vector_error(a, b):
+    """Error of per-vertex vectors a against b: normalised RMS over all
+    vertices, RMS and maximum of the per-vertex relative errors."""
+    a = np.asarray(a).reshape(-1, 2)
+    b = np.asarray(b).reshape(-1, 2)
+    d = np.linalg.norm(a - b, axis=1)
+    n = np.linalg.norm(b, axis=1)
+    rel = d / np.maximum(n, 1e-300)
+    return {"rms_err": float(np.sqrt(np.sum(d * d) / max(np.sum(n * n), 1e-300))),
+            "rms_rel_err_per_vertex": float(np.sqrt(np.mean(rel * rel))),
+            "max_rel_err_per_vertex": float(rel.max())}
+
+
+def run_from(lay, x0, steps, precision, strict=0):
+    """Positions after `steps` steps from x0 (FA2 state reset, as Begin),
+    and the device time of the steps."""
+    lay.set_params(precision=precision, strictReductions=strict)
+    lay.set_positions(x0)
+    lay.set_fa2_state(np.zeros(2 * lay.V), 1.0, 1.0)
+    ms = lay.time_steps(steps) if steps else 0.0
+    return lay.positions(), ms
+
+
+def precision_report(lay, w, args):
+    """FP32 GPU against FP64 GPU (and the reference's CPU step where the CPU
+    baseline leg runs) on this workload: per-vertex force errors, free-run
+    drift and final-layout stress. Untimed; the layout is left at its state."""
+    x_s, (sf_s, sp_s, ef_s) = lay.positions(), lay.fa2_state()
+    rng = np.random.default_rng(SEED + 2)
+    out = {}
+    if w.name == "ba1m":
+        t = np.sort(rng.choice(w.V, min(JUDGE_SAMPLE, w.V), replace=False)).astype(np.uint32)
+        exact = lay.exact_repulsion(t)
+        lay.set_params(precision=0)
+        r32 = lay.repulsion()[t]
+        lay.set_params(precision=1)
+        r64 = lay.repulsion()[t]
+        out["forces"] = {"sample": f"{len(t)} seeded vertices, at the timed state",
+                         "fp32_bh_vs_fp64_bh": vector_error(r32, r64),
+                         "fp32_bh_vs_exact_fp64": vector_error(r32, exact),
+                         "fp64_bh_vs_exact_fp64": vector_error(r64, exact)}
+        iters = 200
+    elif w.name == "er65k_exact":
+        lay.set_params(precision=0)
+        r32 = lay.repulsion()
+        lay.set_params(precision=1)
+        r64 = lay.repulsion()
+        out["forces"] = {"sample": f"all {w.V} vertices, at the timed state",
+                         "fp32_kahan_exact_vs_fp64_exact": vector_error(r32, r64)}
+        iters = 100
+    else:  # grid32
+        iters = 500
+    x0 = w.x0
+    xy32, ms32 = run_from(lay, x0, iters, 0)
+    xy64, ms64 = run_from(lay, x0, iters, 1, strict=1 if w.name == "grid32" else 0)
+    ext = float(np.abs(xy64).max())
+    dr = np.linalg.norm((xy32 - xy64).reshape(-1, 2), axis=1) / max(ext, 1e-300)
+    out["free_run"] = {
+        "iterations": iters, "from": "the initial positions",
+        "fp32_vs_fp64_drift_over_extent": {"median": float(np.median(dr)),
+                                           "max": float(dr.max())},
+        "fp64_ms_per_step": ms64 / iters, "fp32_ms_per_step": ms32 / iters,
+        "stress": {"initial": layout_stress(w.row, w.col, x0),
+                   "fp32": layout_stress(w.row, w.col, xy32),
+                   "fp64": layout_stress(w.row, w.col, xy64),
+                   "sources": STRESS_SOURCES}}
+    if not args.no_cpu_baseline:
+        out["reference"] = reference_comparison(lay, w, iters)
+    lay.set_params(precision=0, strictReductions=0)
+    lay.set_positions(x_s)
+    lay.set_fa2_state(sf_s, sp_s, ef_s)
+    return out
+
+
+def reference_comparison(lay, w, iters):
+    """The reference's own CPU step (oracle/_ref, the CPU baseline's
+    library) against the GPU paths, free-running from the same Begin: every
+    iteration of the 32x32 grid; for larger layouts the first steps only
+    (the CPU step takes seconds there)."""
+    from oracle.bindings import Reference
+    if not Reference.available():
+        return None
+    ref, rl = reference_graph(w, 0)
+    x0 = rl.positions()
+    n = iters if w.V <= 4096 else 2
+    marks = sorted({1, 2, 10, 50, 100, 200, 500} & set(range(1, n + 1)))
+    res = {"steps": n, "threads": ref.pool_threads(), "at": marks}
+    refpos = {}
+    for s in range(1, n + 1):
+        rl.step()
+        if s in marks:
+            refpos[s] = rl.positions()
+    rl.close()
+    for name, prec, strict in (("fp64", 1, 1), ("fp32", 0, 0)):
+        lay.set_params(precision=prec, strictReductions=strict)
+        lay.set_positions(x0)
+        lay.set_fa2_state(np.zeros(2 * lay.V), 1.0, 1.0)
+        drift = []
+        for s in range(1, n + 1):
+            lay.step()
+            if s in marks:
+                p, q = lay.positions(), refpos[s]
+                ext = max(float(np.abs(q).max()), 1e-300)
+                d = np.linalg.norm((p - q).reshape(-1, 2), axis=1) / ext
+                drift.append({"iteration": s, "median": float(np.median(d)),
+                              "max": float(d.max())})
+        res[name] = drift
+        if n == iters:
+            res[name + "_stress"] = layout_stress(w.row, w.col, lay.positions())
+    if n == iters:
+        res["reference_stress"] = layout_stress(w.row, w.col, refpos[n])
+    return res
+
+
 # ---------------------------------------------------------------------- GRIP
 GRIP_V, GRIP_M, GRIP_K = 200_000, 3, 128
 
@@ -865,6 +1010,8 @@ def main():
         line["plain"] = plain_line
         line["config"]["theta"] = {"plain": w.spec["theta"], "learned": linfo["learned_theta"]}
         line["config"]["hub_targets"] = linfo["hub_targets"]
+    if rank == 0 and world == 1 and w.name in ("ba1m", "er65k_exact", "grid32"):
+        line["precision"] = precision_report(lay, w, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(w)
     if rank == 0:

@@ -165,9 +165,11 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_rootT);
   dfree(h->d_graphBase);
   dfree(h->d_nodes);
+  dfree(h->d_kids);
   dfree(h->d_leafDepth);
   dfree(h->d_counters);
   dfree(h->d_walkQueue);
+  dfree(h->d_walkTasks);
 }
 
 int upload_radius(gvizCudaForce *h) {
@@ -736,9 +738,19 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_rootT, G);
   rc |= dalloc(h, &h->d_graphBase, G);
   rc |= dalloc(h, &h->d_nodes, h->maxNodes * sizeof(NodeD));
+  rc |= dalloc(h, &h->d_kids, h->maxNodes);
   rc |= dalloc(h, &h->d_leafDepth, Vs);
   rc |= dalloc(h, &h->d_counters, 8);
   rc |= dalloc(h, &h->d_walkQueue, 1);
+  // walk tasks: 32 consecutive path-sorted targets of one graph each, cut
+  // from every graph's first sorted position, so that a graph's tasks are
+  // the same alone and in a forest
+  std::vector<uint2> tasks;
+  for (size_t gg = 0; gg < G; gg++)
+    for (uint64_t s0 = goff[gg]; s0 < goff[gg + 1]; s0 += 32)
+      tasks.push_back(make_uint2((uint32_t)s0, (uint32_t)std::min<uint64_t>(32, goff[gg + 1] - s0)));
+  h->nWalkTasks = (uint32_t)tasks.size();
+  rc |= dalloc(h, &h->d_walkTasks, std::max<size_t>(tasks.size(), 1));
   if (rc) {
     gvizCudaForceDestroy(h);
     return GVIZ_CUDA_ERR_ALLOC;
@@ -754,6 +766,7 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   up(h->d_massF, massF.data(), V * 4);
   if (G > 1) up(h->d_gid, gid.data(), V * 4);
   up(h->d_graphOff, goff.data(), (G + 1) * 8);
+  up(h->d_walkTasks, tasks.data(), tasks.size() * sizeof(uint2));
   up(h->d_meanDegPlusOne, mdp.data(), G * 8);
   up(h->d_chunkBegin, cb.data(), cb.size() * 4);
   up(h->d_chunkEnd, ce.data(), ce.size() * 4);
@@ -1679,9 +1692,9 @@ int gvizCudaForceFarJudgeStatus(const gvizCudaForce *h, uint64_t *checks, double
   return GVIZ_CUDA_OK;
 }
 
-int gvizCudaForceSetCellStackCap(gvizCudaForce *h, uint32_t entries) {
+int gvizCudaForceSetWalkStackCap(gvizCudaForce *h, uint32_t entries) {
   if (!h || (entries != 0 && (entries < 32 || entries > 512))) return GVIZ_CUDA_ERR_ARG;
-  h->cellStackCap = entries;
+  h->walkStackCap = entries;
   h->graphDirty = true;
   return GVIZ_CUDA_OK;
 }

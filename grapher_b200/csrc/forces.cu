@@ -31,6 +31,8 @@ constexpr int kWalkMaxThreads = 512;  // largest block size the autotuner tries
 constexpr int kAttrThreads = 256;
 constexpr int kExactThreads = 256;
 constexpr int kExactTile = 256;
+constexpr int kExactTpt = 4;     // exact mode: targets per thread
+constexpr int kExactChunk = 32;  // exact mode: sources per plain partial sum
 constexpr uint32_t kInf = 0xffffffffu;
 
 struct Kahan {
@@ -168,6 +170,7 @@ __global__ __launch_bounds__(kAttrThreads) void k_attr_hub_sum(HubArgs a) {
 
 struct WalkArgs {
   const NodeF *nodes;
+  const uint4 *kids;  // per cell: children's preorder slots (tree build)
   const uint32_t *idx, *gid, *active, *graphBase, *rootT;
   const double2 *pos;
   const float *massF, *radiusF;
@@ -179,6 +182,9 @@ struct WalkArgs {
   uint32_t V;
   unsigned long long *counters;  // [0] interactions, [1] warp node visits
   uint32_t *queue;               // next task of the persistent schedule
+  uint32_t stackCap;             // stack entries per warp in use
+  const uint2 *tasks;            // plain walk tasks: first sorted position, targets
+  uint32_t nTasks;
 };
 
 // One pair or pseudo-body term of FR / LinLog repulsion
@@ -238,85 +244,225 @@ __device__ __forceinline__ void rep_term_apart(float dx, float dy, float d2, flo
 }
 
 // One walk task: the 32 path-sorted targets starting at sorted position
-// 32 * task, one per lane.
-template <int MODEL, bool OVERLAP, bool COUNT>
-__device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task) {
-  const unsigned lane = threadIdx.x & 31u;
-  const uint32_t s = task * 32u + lane;
-  const bool valid = s < a.V;
-  const uint32_t v = valid ? a.idx[s] : 0u;
-  const uint32_t g = (valid && a.gid) ? a.gid[v] : 0u;
-  const bool act = valid && (a.active == nullptr || a.active[g] != 0u);
-  uint32_t resume = 0, myEnd = 0;
-  if (act) {
-    resume = a.graphBase[g];
-    myEnd = min(resume + a.rootT[g], a.maxNodes);
-  }
-  float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
-  if (act) {
-    const double2 p = a.pos[v];
-    ds_split(p.x, vxh, vxl);
-    ds_split(p.y, vyh, vyl);
-    mv = a.massF[v];
-    if (OVERLAP) rv = a.radiusF[v];
-  }
-  Kahan kx, ky;
-  unsigned long long nInter = 0, nVisit = 0;
-  uint32_t nxt = resume < myEnd ? resume : kInf;
-  uint32_t cur = __reduce_min_sync(0xffffffffu, nxt);
-  while (cur != kInf) {
-    const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
-    const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
-    const float nmass = n1.x, nsize = n1.y;
-    const int32_t nnext = __float_as_int(n1.z), ninfo = __float_as_int(n1.w);
-    const bool active = cur >= resume && cur < myEnd;
-    const float dx = (n0.x - vxh) + (n0.z - vxl);
-    const float dy = (n0.y - vyh) + (n0.w - vyl);
-    const float d2 = dx * dx + dy * dy;
-    const bool isLeaf = ninfo >= 0;
-    const bool massOk = nmass != 0.0f;
-    const bool accept = !isLeaf && nsize < d2;
-    const bool doForce =
-        active && massOk && (isLeaf ? ((uint32_t)ninfo != v) : accept);
-    const bool open = active && massOk && !isLeaf && !accept;
-    // coincident points are rare: one vote keeps their branch off the
-    // common path, which stays straight-line
-    if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {
-      if (doForce) {
-        float fx, fy;
-        rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, nmass,
-                                 rv + (isLeaf ? nsize : 0.0f), a.num,
-                                 a.overlapC, v, isLeaf ? (uint32_t)ninfo : v,
-                                 fx, fy);
-        kx.add(fx);
-        ky.add(fy);
-      }
-    } else if (doForce) {
+// 32 * task, one per lane, each making the reference's own decisions
+// (bhAccumulateRepulsion, src/embedders/gvizForceEmbedder.c:35-74): empty
+// node skipped; point: pair term unless it is the target; cell: accepted
+// when 2h/|com - v| < theta, else opened. The warp expands the union of
+// the nodes its lanes need 32 at a time: a pending entry is a node and the
+// lanes whose walks reach it (they opened every ancestor); each round every
+// lane pops one entry and loads its node (32 independent loads), the
+// records go to shared memory, and then every lane tests each of the round's
+// nodes for its own target if it is among that node's lanes. An opened node
+// pushes its children (slots from the tree build's child records) with the
+// lanes that opened it. A push that would overflow the stack is walked in
+// place with the stackless union walk below (the same decisions).
+constexpr int kPlainStack = 512;  // pending (node, lanes) entries per warp
+
+struct __align__(16) PlainWarpSmem {
+  float4 rec[32][2];      // the round's node records
+  uint2 st[kPlainStack];  // pending entries: node, lanes
+};
+
+struct PlainTarget {
+  uint32_t v;
+  bool act;
+  float vxh, vxl, vyh, vyl, mv, rv;
+};
+
+// The reference's decision for one node and this lane's target: adds the
+// term of a point or an accepted cell; returns true when the cell is opened.
+template <int MODEL, bool OVERLAP>
+__device__ __forceinline__ bool plain_visit(const WalkArgs &a, const PlainTarget &t, bool in,
+                                            float4 n0, float4 n1, Kahan &kx, Kahan &ky,
+                                            unsigned long long &nInter) {
+  const float nmass = n1.x, nsize = n1.y;
+  const int32_t ninfo = __float_as_int(n1.w);
+  const float dx = (n0.x - t.vxh) + (n0.z - t.vxl);
+  const float dy = (n0.y - t.vyh) + (n0.w - t.vyl);
+  const float d2 = dx * dx + dy * dy;
+  const bool isLeaf = ninfo >= 0;
+  const bool massOk = nmass != 0.0f;
+  const bool accept = !isLeaf && nsize < d2;
+  const bool doForce = in && massOk && (isLeaf ? ((uint32_t)ninfo != t.v) : accept);
+  // coincident points are rare: one vote keeps their branch off the
+  // common path, which stays straight-line
+  if (__any_sync(0xffffffffu, doForce && !(d2 > 0.0f))) {
+    if (doForce) {
       float fx, fy;
-      rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, mv, nmass, rv + (isLeaf ? nsize : 0.0f),
-                                     a.num, a.overlapC, fx, fy);
+      rep_term<MODEL, OVERLAP>(dx, dy, d2, t.mv, nmass, t.rv + (isLeaf ? nsize : 0.0f), a.num,
+                               a.overlapC, t.v, isLeaf ? (uint32_t)ninfo : t.v, fx, fy);
       kx.add(fx);
       ky.add(fy);
     }
-    if (COUNT && doForce) nInter++;
-    if (active) resume = open ? cur + 1u : max((uint32_t)nnext, cur + 1u);
-    nxt = resume < myEnd ? resume : kInf;
-    if (COUNT) nVisit++;
-    cur = __reduce_min_sync(0xffffffffu, nxt);
+  } else if (doForce) {
+    float fx, fy;
+    rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, nmass, t.rv + (isLeaf ? nsize : 0.0f),
+                                   a.num, a.overlapC, fx, fy);
+    kx.add(fx);
+    ky.add(fy);
+  }
+  nInter += doForce ? 1ull : 0ull;
+  return in && massOk && !isLeaf && !accept;
+}
+
+// The stackless union walk of the preorder range [lo, hi) for the lanes in
+// `lanes`: the warp steps through the union of the nodes they need, each
+// lane's next node is cur + 1 (opened) or the node's skip pointer, the warp
+// moves to the minimum.
+template <int MODEL, bool OVERLAP>
+__device__ void plain_walk_range(const WalkArgs &a, const PlainTarget &t, uint32_t lanes,
+                                 uint32_t lo, uint32_t hi, Kahan &kx, Kahan &ky,
+                                 unsigned long long &nInter, unsigned long long &nVisit) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const bool mine = (lanes >> lane) & 1u;
+  uint32_t resume = mine ? lo : kInf;
+  uint32_t cur = __reduce_min_sync(0xffffffffu, resume < hi ? resume : kInf);
+  while (cur != kInf) {
+    const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
+    const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
+    const bool in = mine && cur == resume;
+    const bool open = plain_visit<MODEL, OVERLAP>(a, t, in, n0, n1, kx, ky, nInter);
+    if (in) resume = open ? cur + 1u : max((uint32_t)__float_as_int(n1.z), cur + 1u);
+    nVisit++;
+    cur = __reduce_min_sync(0xffffffffu, resume < hi ? resume : kInf);
+  }
+}
+
+template <int MODEL, bool OVERLAP, bool COUNT>
+__device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, PlainWarpSmem &q) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t below = (1u << lane) - 1u;
+  // a task's targets all belong to one graph (tasks are cut per graph): the
+  // order of each target's sums depends only on its graph's layout
+  const uint2 tk = a.tasks[task];
+  const uint32_t s = tk.x + lane;
+  const bool valid = lane < tk.y && s < a.V;
+  PlainTarget t;
+  t.v = valid ? a.idx[s] : 0u;
+  const uint32_t g = (valid && a.gid) ? a.gid[t.v] : 0u;
+  t.act = valid && (a.active == nullptr || a.active[g] != 0u);
+  uint32_t root = 0, myEnd = 0;
+  if (t.act) {
+    root = a.graphBase[g];
+    myEnd = min(root + a.rootT[g], a.maxNodes);
+  }
+  t.vxh = t.vxl = t.vyh = t.vyl = t.mv = t.rv = 0.f;
+  if (t.act) {
+    const double2 p = a.pos[t.v];
+    ds_split(p.x, t.vxh, t.vxl);
+    ds_split(p.y, t.vyh, t.vyl);
+    t.mv = a.massF[t.v];
+    if (OVERLAP) t.rv = a.radiusF[t.v];
+  }
+  Kahan kx, ky;
+  unsigned long long nInter = 0, nVisit = 0, nSerial = 0;
+  // the first entries: each distinct root among the lanes, with its lanes
+  const uint32_t key = (t.act && root < myEnd) ? root : kInf;
+  const uint32_t same = __match_any_sync(0xffffffffu, key);
+  const bool leader = key != kInf && (uint32_t)(__ffs(same) - 1) == lane;
+  const uint32_t bl = __ballot_sync(0xffffffffu, leader);
+  if (leader) q.st[__popc(bl & below)] = make_uint2(root, same);
+  uint32_t top = __popc(bl);
+  __syncwarp();
+  while (top > 0u) {
+    const uint32_t n = min(top, 32u);
+    const bool mine = lane < n;
+    const uint2 e = mine ? q.st[top - n + lane] : make_uint2(0u, 0u);
+    top -= n;
+    float4 n0 = make_float4(0.f, 0.f, 0.f, 0.f), n1 = n0;
+    uint4 kd = make_uint4(GVIZ_NONE, GVIZ_NONE, GVIZ_NONE, GVIZ_NONE);
+    if (mine) {
+      n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + e.x));
+      n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + e.x) + 1);
+      kd = __ldg(a.kids + e.x);  // read for every node; used only when it is opened
+    }
+    // the graph's end for the entry's lanes (they share one graph)
+    const uint32_t entryEnd = __shfl_sync(0xffffffffu, myEnd, mine ? __ffs(e.y) - 1 : 0);
+    __syncwarp();  // popped, and last round's records read, before the writes below
+    if (mine) {
+      q.rec[lane][0] = n0;
+      q.rec[lane][1] = n1;
+    }
+    __syncwarp();
+    if (COUNT) nVisit += n;
+    uint32_t myOpen = 0;
+    for (uint32_t j = 0; j < n; j++) {
+      const uint32_t lanes = __shfl_sync(0xffffffffu, e.y, j);
+      const bool open = plain_visit<MODEL, OVERLAP>(a, t, (lanes >> lane) & 1u, q.rec[j][0],
+                                                    q.rec[j][1], kx, ky, nInter);
+      const uint32_t ob = __ballot_sync(0xffffffffu, open);
+      if (lane == j) myOpen = ob;
+    }
+    // opened nodes push their children (inside the graph's subtree) with the
+    // lanes that opened them, in lane order, while they fit
+    uint32_t nk = 0;
+    if (myOpen) {
+      if (kd.y == GVIZ_KIDS_RUN) {
+        nk = (kd.x > e.x && kd.x < entryEnd) ? min(kd.z, entryEnd - kd.x) : 0u;
+        nk = min(nk, (uint32_t)kPlainStack + 1u);  // a longer run never fits
+      } else {
+        kd.x = (kd.x > e.x && kd.x < entryEnd) ? kd.x : GVIZ_NONE;
+        kd.y = (kd.y > e.x && kd.y < entryEnd) ? kd.y : GVIZ_NONE;
+        kd.z = (kd.z > e.x && kd.z < entryEnd) ? kd.z : GVIZ_NONE;
+        kd.w = (kd.w > e.x && kd.w < entryEnd) ? kd.w : GVIZ_NONE;
+        nk = (uint32_t)(kd.x != GVIZ_NONE) + (uint32_t)(kd.y != GVIZ_NONE) +
+             (uint32_t)(kd.z != GVIZ_NONE) + (uint32_t)(kd.w != GVIZ_NONE);
+      }
+    }
+    uint32_t incl = nk;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    const bool fits = top + incl <= a.stackCap;
+    if (myOpen && fits) {
+      const uint32_t base = top + incl - nk;
+      if (kd.y == GVIZ_KIDS_RUN) {
+        for (uint32_t i = 0; i < nk; i++) q.st[base + i] = make_uint2(kd.x + i, myOpen);
+      } else {
+        uint32_t w = base;
+        if (kd.x != GVIZ_NONE) q.st[w++] = make_uint2(kd.x, myOpen);
+        if (kd.y != GVIZ_NONE) q.st[w++] = make_uint2(kd.y, myOpen);
+        if (kd.z != GVIZ_NONE) q.st[w++] = make_uint2(kd.z, myOpen);
+        if (kd.w != GVIZ_NONE) q.st[w++] = make_uint2(kd.w, myOpen);
+      }
+    }
+    top += __reduce_max_sync(0xffffffffu, fits ? incl : 0u);
+    // subtrees that did not fit, walked in place
+    uint32_t bS = __ballot_sync(0xffffffffu, myOpen != 0u && !fits);
+    if (COUNT) nSerial += __popc(bS);
+    while (bS) {
+      const int l = __ffs(bS) - 1;
+      bS &= bS - 1u;
+      const uint32_t lanes = __shfl_sync(0xffffffffu, myOpen, l);
+      const uint32_t lo = __shfl_sync(0xffffffffu, e.x, l) + 1u;
+      const uint32_t hi = __shfl_sync(
+          0xffffffffu, min(max((uint32_t)__float_as_int(n1.z), e.x + 1u), entryEnd), l);
+      plain_walk_range<MODEL, OVERLAP>(a, t, lanes, lo, hi, kx, ky, nInter, nVisit);
+    }
+    __syncwarp();
   }
   if (COUNT) {
     atomicAdd(a.counters, nInter);
-    if (lane == 0) atomicAdd(a.counters + 1, nVisit);
+    if (lane == 0) {
+      atomicAdd(a.counters + 1, nVisit);
+      atomicAdd(a.counters + 5, nSerial);
+    }
   }
-  if (!act) return;
-  const float2 at = a.attF[v];
-  force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value(), ky.value());
+  if (!t.act) return;
+  const float2 at = a.attF[t.v];
+  force_epilogue(a.epi, t.v, (double)at.x, (double)at.y, kx.value(), ky.value());
 }
 
 // Static schedule: warp w of the grid takes task w.
 template <int MODEL, bool OVERLAP, bool COUNT>
 __global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32(WalkArgs a) {
-  walk_task<MODEL, OVERLAP, COUNT>(a, (blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  extern __shared__ __align__(16) unsigned char plainDyn[];
+  PlainWarpSmem &q = reinterpret_cast<PlainWarpSmem *>(plainDyn)[threadIdx.x >> 5];
+  const uint32_t task = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (task >= a.nTasks) return;  // the whole warp
+  walk_task<MODEL, OVERLAP, COUNT>(a, task, q);
 }
 
 // Persistent schedule: a grid sized to fill the GPU once; each warp takes
@@ -324,13 +470,14 @@ __global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32(WalkArgs a) {
 // the queue is empty, so warps that drew cheap tasks take more of them.
 template <int MODEL, bool OVERLAP, bool COUNT>
 __global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32_queue(WalkArgs a) {
-  const uint32_t tasks = (a.V + 31u) / 32u;
+  extern __shared__ __align__(16) unsigned char plainDyn[];
+  PlainWarpSmem &q = reinterpret_cast<PlainWarpSmem *>(plainDyn)[threadIdx.x >> 5];
   for (;;) {
     uint32_t t = 0;
     if ((threadIdx.x & 31u) == 0u) t = atomicAdd(a.queue, 1u);
     t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= tasks) return;
-    walk_task<MODEL, OVERLAP, COUNT>(a, t);
+    if (t >= a.nTasks) return;
+    walk_task<MODEL, OVERLAP, COUNT>(a, t, q);
   }
 }
 
@@ -1233,76 +1380,128 @@ struct ExactArgs {
   uint32_t V;
 };
 
+// Exact all-pairs repulsion (src/embedders/gvizForceEmbedder.c:104-115) as
+// a tiled N-body: a block holds kExactThreads * kExactTpt targets, each
+// thread kExactTpt of them (kExactThreads apart), and the sources stream
+// through shared memory in tiles of kExactTile; every source read from
+// shared memory serves kExactTpt targets. Per target the terms of each run
+// of kExactChunk sources are added in plain FP32 and that partial joins a
+// Kahan-compensated running sum (cascade summation: the rounding of a
+// V-term sum stays at a chunk's). The pair term runs straight-line; a source
+// that coincides with a target (the target itself, or a duplicate point,
+// d2 == 0) sends the warp through the guarded path for that source, which
+// skips the self pair and applies the coincident direction. Tiles that
+// straddle a graph boundary of a forest take the guarded path too.
 template <int MODEL, bool OVERLAP>
 __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
   __shared__ float4 sp[kExactTile];
   __shared__ float2 sm[kExactTile];
   __shared__ uint32_t sRange[2];
-  const uint32_t v = blockIdx.x * kExactThreads + threadIdx.x;
-  const bool valid = v < a.V;
-  const uint32_t g = (valid && a.gid) ? a.gid[v] : 0u;
-  const bool act = valid && (a.active == nullptr || a.active[g] != 0u);
-  uint32_t gb = 0, ge = 0;
-  if (act) {
-    gb = (uint32_t)a.graphOff[g];
-    ge = (uint32_t)a.graphOff[g + 1];
-  }
+  uint32_t v[kExactTpt], gb[kExactTpt], ge[kExactTpt];
+  bool act[kExactTpt];
+  float vxh[kExactTpt], vxl[kExactTpt], vyh[kExactTpt], vyl[kExactTpt], mv[kExactTpt],
+      rv[kExactTpt];
+  Kahan kx[kExactTpt], ky[kExactTpt];
   if (threadIdx.x == 0) {
     sRange[0] = kInf;
     sRange[1] = 0;
   }
   __syncthreads();
-  if (act) {
-    atomicMin(&sRange[0], gb);
-    atomicMax(&sRange[1], ge);
+#pragma unroll
+  for (int k = 0; k < kExactTpt; k++) {
+    v[k] = blockIdx.x * (kExactThreads * kExactTpt) + k * kExactThreads + threadIdx.x;
+    const bool valid = v[k] < a.V;
+    const uint32_t g = (valid && a.gid) ? a.gid[v[k]] : 0u;
+    act[k] = valid && (a.active == nullptr || a.active[g] != 0u);
+    gb[k] = ge[k] = 0;
+    // an idle slot sits at NaN: its terms are never used and never vote
+    vxh[k] = vxl[k] = vyh[k] = vyl[k] = __int_as_float(0x7fc00000);
+    mv[k] = rv[k] = 0.f;
+    if (act[k]) {
+      gb[k] = (uint32_t)a.graphOff[g];
+      ge[k] = (uint32_t)a.graphOff[g + 1];
+      atomicMin(&sRange[0], gb[k]);
+      atomicMax(&sRange[1], ge[k]);
+      const double2 p = a.pos[v[k]];
+      ds_split(p.x, vxh[k], vxl[k]);
+      ds_split(p.y, vyh[k], vyl[k]);
+      mv[k] = a.massF[v[k]];
+      if (OVERLAP) rv[k] = a.radiusF[v[k]];
+    }
   }
   __syncthreads();
   const uint32_t lo = sRange[0], hi = sRange[1];
-  float vxh = 0.f, vxl = 0.f, vyh = 0.f, vyl = 0.f, mv = 0.f, rv = 0.f;
-  if (act) {
-    const double2 p = a.pos[v];
-    ds_split(p.x, vxh, vxl);
-    ds_split(p.y, vyh, vyl);
-    mv = a.massF[v];
-    if (OVERLAP) rv = a.radiusF[v];
-  }
-  Kahan kx, ky;
   for (uint32_t t0 = lo; t0 < hi; t0 += kExactTile) {
     __syncthreads();
     const uint32_t j = t0 + threadIdx.x;
-    if (threadIdx.x < kExactTile) {
-      if (j < hi) {
-        const double2 q = a.pos[j];
-        float4 f;
-        ds_split(q.x, f.x, f.z);
-        ds_split(q.y, f.y, f.w);
-        sp[threadIdx.x] = f;
-        sm[threadIdx.x] = make_float2(a.massF[j], OVERLAP ? a.radiusF[j] : 0.f);
-      }
+    if (threadIdx.x < kExactTile && j < hi) {
+      const double2 q = a.pos[j];
+      float4 f;
+      ds_split(q.x, f.x, f.z);
+      ds_split(q.y, f.y, f.w);
+      sp[threadIdx.x] = f;
+      sm[threadIdx.x] = make_float2(a.massF[j], OVERLAP ? a.radiusF[j] : 0.f);
     }
     __syncthreads();
     const uint32_t cnt = min((uint32_t)kExactTile, hi - t0);
-    if (act) {
+    bool inside = true;  // the whole tile lies in every target's graph
+#pragma unroll
+    for (int k = 0; k < kExactTpt; k++)
+      inside = inside && (!act[k] || (gb[k] <= t0 && t0 + cnt <= ge[k]));
+    const bool fastTile = __all_sync(0xffffffffu, inside);
+    for (uint32_t c0 = 0; c0 < cnt; c0 += kExactChunk) {
+      const uint32_t c1 = min(c0 + (uint32_t)kExactChunk, cnt);
+      float px[kExactTpt], py[kExactTpt];
+#pragma unroll
+      for (int k = 0; k < kExactTpt; k++) px[k] = py[k] = 0.f;
 #pragma unroll 4
-      for (uint32_t q = 0; q < cnt; q++) {
-        const uint32_t jj = t0 + q;
-        if (jj == v || jj < gb || jj >= ge) continue;
+      for (uint32_t q = c0; q < c1; q++) {
         const float4 f = sp[q];
         const float2 m = sm[q];
-        const float dx = (f.x - vxh) + (f.z - vxl);
-        const float dy = (f.y - vyh) + (f.w - vyl);
-        const float d2 = dx * dx + dy * dy;
-        float fx, fy;
-        rep_term<MODEL, OVERLAP>(dx, dy, d2, mv, m.x, rv + m.y, a.num,
-                                 a.overlapC, v, jj, fx, fy);
-        kx.add(fx);
-        ky.add(fy);
+        float dx[kExactTpt], dy[kExactTpt], d2[kExactTpt];
+        bool zero = false;
+#pragma unroll
+        for (int k = 0; k < kExactTpt; k++) {
+          dx[k] = (f.x - vxh[k]) + (f.z - vxl[k]);
+          dy[k] = (f.y - vyh[k]) + (f.w - vyl[k]);
+          d2[k] = dx[k] * dx[k] + dy[k] * dy[k];
+          zero = zero || d2[k] == 0.0f;
+        }
+        if (fastTile && !__any_sync(0xffffffffu, zero)) {
+#pragma unroll
+          for (int k = 0; k < kExactTpt; k++) {
+            float fx, fy;
+            rep_term_apart<MODEL, OVERLAP>(dx[k], dy[k], d2[k], mv[k], m.x, rv[k] + m.y, a.num,
+                                           a.overlapC, fx, fy);
+            px[k] += fx;
+            py[k] += fy;
+          }
+        } else {
+          const uint32_t jj = t0 + q;
+#pragma unroll
+          for (int k = 0; k < kExactTpt; k++) {
+            if (!act[k] || jj == v[k] || jj < gb[k] || jj >= ge[k]) continue;
+            float fx, fy;
+            rep_term<MODEL, OVERLAP>(dx[k], dy[k], d2[k], mv[k], m.x, rv[k] + m.y, a.num,
+                                     a.overlapC, v[k], jj, fx, fy);
+            px[k] += fx;
+            py[k] += fy;
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kExactTpt; k++) {
+        kx[k].add(px[k]);
+        ky[k].add(py[k]);
       }
     }
   }
-  if (!act) return;
-  const float2 at = a.attF[v];
-  force_epilogue(a.epi, v, (double)at.x, (double)at.y, kx.value(), ky.value());
+#pragma unroll
+  for (int k = 0; k < kExactTpt; k++) {
+    if (!act[k]) continue;
+    const float2 at = a.attF[v[k]];
+    force_epilogue(a.epi, v[k], (double)at.x, (double)at.y, kx[k].value(), ky[k].value());
+  }
 }
 
 inline uint32_t blocks(size_t n, int t) { return (uint32_t)((n + t - 1) / t); }
@@ -1358,19 +1557,23 @@ void enqueue_attraction_f32(gvizCudaForce *h) {
   prof_mark(h, "attraction_f32");
 }
 
+// dynamic shared memory of the plain walk: one PlainWarpSmem per warp
+static size_t plain_smem(uint32_t threads) { return (threads / 32) * sizeof(PlainWarpSmem); }
+
 template <int MODEL, bool OVERLAP, bool COUNT>
 static void launch_walk(gvizCudaForce *h, const WalkArgs &a) {
   const uint32_t threads = h->walkThreads ? h->walkThreads : kWalkThreads;
-  const uint32_t warps = (uint32_t)((h->V + 31) / 32);
+  const uint32_t warps = h->nWalkTasks;
+  if (warps == 0) return;
   if (h->walkPersistent && h->walkResident) {
     cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), h->stream);
     const uint32_t need = blocks((size_t)warps * 32, threads);
     const uint32_t grid = need < h->walkResident ? need : h->walkResident;
-    k_walk_f32_queue<MODEL, OVERLAP, COUNT><<<grid, threads, 0, h->stream>>>(a);
+    k_walk_f32_queue<MODEL, OVERLAP, COUNT><<<grid, threads, plain_smem(threads), h->stream>>>(a);
     return;
   }
-  k_walk_f32<MODEL, OVERLAP, COUNT><<<blocks((size_t)warps * 32, threads), threads, 0,
-                                      h->stream>>>(a);
+  k_walk_f32<MODEL, OVERLAP, COUNT><<<blocks((size_t)warps * 32, threads), threads,
+                                      plain_smem(threads), h->stream>>>(a);
 }
 
 template <int MODEL, bool OVERLAP>
@@ -1403,7 +1606,23 @@ static void launch_cells(gvizCudaForce *h, const CellArgs &ca, bool count) {
 
 // The cell-group walk's per-warp queues exceed the default dynamic shared
 // memory of a block; opted in once per process for every instance.
+template <int MODEL, bool OVERLAP, bool COUNT>
+static void plain_smem_limits() {
+  cudaFuncSetAttribute(k_walk_f32<MODEL, OVERLAP, COUNT>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plain_smem(kWalkMaxThreads));
+  cudaFuncSetAttribute(k_walk_f32_queue<MODEL, OVERLAP, COUNT>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plain_smem(kWalkMaxThreads));
+}
+
 void forces_set_smem_limits() {
+  plain_smem_limits<GVIZ_CUDA_MODEL_FR, false, false>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_FR, false, true>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_FR, true, false>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_FR, true, true>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_LINLOG, false, false>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_LINLOG, false, true>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_LINLOG, true, false>();
+  plain_smem_limits<GVIZ_CUDA_MODEL_LINLOG, true, true>();
   cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_FR, false, false>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCellDyn);
   cudaFuncSetAttribute(k_walk_f32_cells<GVIZ_CUDA_MODEL_FR, false, true>,
@@ -1481,8 +1700,8 @@ static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *coun
     ca.f = fa;
     ca.groups = h->d_groups;
     ca.kids = h->d_kids;
-    ca.stackCap = (h->cellStackCap >= 32 && h->cellStackCap <= (uint32_t)kCellStack)
-                      ? h->cellStackCap : (uint32_t)kCellStack;
+    ca.stackCap = (h->walkStackCap >= 32 && h->walkStackCap <= (uint32_t)kCellStack)
+                      ? h->walkStackCap : (uint32_t)kCellStack;
     ca.nGroups = h->d_groupCount;
     ca.cap = (uint32_t)(h->V ? h->V : 1);
     if (h->model == GVIZ_CUDA_MODEL_FR) {
@@ -1516,14 +1735,14 @@ uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads) {
   cudaError_t e;
   if (fr) {
     e = ov ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, true, false>, threads, 0)
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, true, false>, threads, plain_smem(threads))
            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, false, false>, threads, 0);
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, false, false>, threads, plain_smem(threads));
   } else {
     e = ov ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, true, false>, threads, 0)
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, true, false>, threads, plain_smem(threads))
            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, false, false>, threads, 0);
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, false, false>, threads, plain_smem(threads));
   }
   if (e != cudaSuccess || per <= 0 || sms <= 0) return 0;
   return (uint32_t)(per * sms);
@@ -1548,6 +1767,11 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   a.counters = reinterpret_cast<unsigned long long *>(counters);
   a.queue = h->d_walkQueue;
   a.maxNodes = (uint32_t)h->maxNodes;
+  a.kids = h->d_kids;
+  a.tasks = h->d_walkTasks;
+  a.nTasks = h->nWalkTasks;
+  a.stackCap = (h->walkStackCap >= 32 && h->walkStackCap <= (uint32_t)kPlainStack)
+                   ? h->walkStackCap : (uint32_t)kPlainStack;
   const bool ov = h->params.preventOverlap != 0;
   const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
   if (h->params.farField && h->d_mlp) {
@@ -1587,7 +1811,7 @@ void enqueue_exact_f32(gvizCudaForce *h) {
   a.num = (float)(h->params.edgeLength * h->params.edgeLength);
   a.overlapC = (float)h->params.overlapConstant;
   a.V = (uint32_t)h->V;
-  const uint32_t grid = blocks(h->V, kExactThreads);
+  const uint32_t grid = blocks(h->V, kExactThreads * kExactTpt);
   const bool ov = h->params.preventOverlap != 0;
   if (h->model == GVIZ_CUDA_MODEL_FR) {
     if (ov) k_exact_f32<GVIZ_CUDA_MODEL_FR, true><<<grid, kExactThreads, 0, h->stream>>>(a);

@@ -141,12 +141,14 @@ struct gvizCudaForce {
   double *d_lastStats = nullptr;    // [G][5], the latest row per graph
   uint64_t *d_counters = nullptr;   // instrumentation counters
   uint32_t *d_walkQueue = nullptr;  // task counter of the persistent walk
+  uint2 *d_walkTasks = nullptr;     // walk tasks: first sorted position, targets
+  uint32_t nWalkTasks = 0;
   // walk launch shape (gvizCudaForceAutotune): block size, persistent
   // work-queue schedule, and the resident grid for it (0: not measured)
   uint32_t walkThreads = 0;
   bool walkPersistent = false;
   uint32_t walkResident = 0;
-  uint32_t cellStackCap = 0;  // learned cell-group walk: stack entries per warp (0: all)
+  uint32_t walkStackCap = 0;  // FP32 walks: stack entries per warp (0: all)
   ChunkStat *d_chunkStat = nullptr;
   uint32_t *d_status = nullptr;
 
@@ -176,6 +178,7 @@ struct gvizCudaForce {
   uint32_t *d_bCnt = nullptr, *d_bT = nullptr;
   uint32_t *d_rootNode = nullptr, *d_rootT = nullptr, *d_graphBase = nullptr;
   void *d_nodes = nullptr;  // NodeF or NodeD, maxNodes records
+  uint4 *d_kids = nullptr;  // per cell: children's preorder slots (FP32 builds)
   uint32_t *d_leafDepth = nullptr;  // per vertex (inspection only)
 
   // forces-only evaluation (no FA2 history update): structForce goes to
@@ -191,7 +194,6 @@ struct gvizCudaForce {
   uint32_t *d_leafPre = nullptr;    // per vertex: preorder index of its leaf
   uint32_t *d_cellCnt = nullptr;    // per cell node: points below it
   uint4 *d_groups = nullptr;        // target groups: preorder [x, y), z points
-  uint4 *d_kids = nullptr;          // per cell: children's preorder slots (tree.cu)
   uint32_t *d_groupCount = nullptr; // [0] groups written, [1] walk queue
   // hub targets of the learned walk (params.farHubTargets heaviest vertices)
   uint32_t *d_farHubs = nullptr;  // nFarHubs ids, then the walk's hub counter

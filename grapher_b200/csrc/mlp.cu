@@ -496,7 +496,6 @@ int far_side_alloc(gvizCudaForce *h) {
       cudaMalloc(&h->d_leafPre, Vs * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&h->d_cellCnt, h->maxNodes * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&h->d_groups, Vs * sizeof(uint4)) != cudaSuccess ||
-      cudaMalloc(&h->d_kids, h->maxNodes * sizeof(uint4)) != cudaSuccess ||
       cudaMalloc(&h->d_groupCount, 2 * sizeof(uint32_t)) != cudaSuccess)
     return GVIZ_CUDA_ERR_ALLOC;
   return GVIZ_CUDA_OK;
@@ -509,14 +508,12 @@ void far_side_free(gvizCudaForce *h) {
   cudaFree(h->d_leafPre);
   cudaFree(h->d_cellCnt);
   cudaFree(h->d_groups);
-  cudaFree(h->d_kids);
   cudaFree(h->d_groupCount);
   h->d_bQ = h->d_nQ = nullptr;
   h->d_cells = nullptr;
   h->d_leafPre = nullptr;
   h->d_cellCnt = nullptr;
   h->d_groups = nullptr;
-  h->d_kids = nullptr;
   h->d_groupCount = nullptr;
 }
 

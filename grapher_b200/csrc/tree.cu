@@ -1108,7 +1108,7 @@ EM make_em(gvizCudaForce *h) {
   a.cellCnt = (h->farSide && h->params.farCellGroups) ? h->d_cellCnt : nullptr;
   a.nLeft = h->d_nLeft;
   a.nRight = h->d_nRight;
-  a.kids = (h->farSide && h->params.farCellGroups && !a.f64) ? h->d_kids : nullptr;
+  a.kids = a.f64 ? nullptr : h->d_kids;  // the FP32 walks expand cells by them
   return a;
 }
 

@@ -320,12 +320,12 @@ class ForceLayout:
                 "gvizCudaForceFarJudgeStatus")
         return n.value, le.value, pe.value, bool(fb.value)
 
-    def set_cell_stack_cap(self, entries):
-        """Stack entries per warp of the learned cell-group walk (32..512; 0
-        restores 512): a tuning and test knob, forces agree up to the order
-        of the per-target sums."""
-        N.check(self.L.gvizCudaForceSetCellStackCap(self.h, entries),
-                "gvizCudaForceSetCellStackCap")
+    def set_walk_stack_cap(self, entries):
+        """Stack entries per warp of the FP32 walks, plain and learned
+        (32..512; 0 restores 512): a tuning and test knob, forces agree up
+        to the order of the per-target sums."""
+        N.check(self.L.gvizCudaForceSetWalkStackCap(self.h, entries),
+                "gvizCudaForceSetWalkStackCap")
 
     def set_walk_shape(self, threads, persistent):
         N.check(self.L.gvizCudaForceSetWalkShape(self.h, threads, int(persistent)),

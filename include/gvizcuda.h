@@ -234,7 +234,7 @@ int gvizCudaForceCountInteractions(gvizCudaForce *h, uint64_t *interactions,
  * (farCellGroups 1): groupRows = one row per group and accepted cell,
  * laneRows = 0, and laneRowCause = {node visits of the longest group walk,
  * subtrees walked in place because the stack was full
- * (gvizCudaForceSetCellStackCap), targets walked over all groups}. Zeros
+ * (gvizCudaForceSetWalkStackCap), targets walked over all groups}. Zeros
  * when the correction is off. */
 int gvizCudaForceCountFarRows(gvizCudaForce *h, uint64_t *groupRows,
                               uint64_t *laneRows, uint64_t *laneRowCause);
@@ -456,13 +456,14 @@ int gvizCudaForceJudgeFarField(gvizCudaForce *h, double *learnedErr, double *pla
 int gvizCudaForceFarJudgeStatus(const gvizCudaForce *h, uint64_t *checks, double *learnedErr,
                                 double *plainErr, int32_t *fellBack);
 
-/* The learned cell-group walk expands the tree 32 cells at a time through a
- * per-warp stack of pending nodes in shared memory (512 entries); a subtree
- * whose children do not fit is walked in place instead. Sets the stack
- * entries the walk may use, 32 to 512 (0 restores 512); forces agree up to
- * the order of the per-target sums. A tuning and test knob. No reference
- * counterpart. */
-int gvizCudaForceSetCellStackCap(gvizCudaForce *h, uint32_t entries);
+/* The FP32 Barnes-Hut walks (plain and learned cell-group) expand the tree
+ * 32 nodes at a time through a per-warp stack of pending nodes in shared
+ * memory (512 entries); an opened cell whose children do not fit is walked
+ * in place with the stackless preorder walk instead (the same decisions).
+ * Sets the stack entries the walks may use, 32 to 512 (0 restores 512);
+ * forces agree up to the order of the per-target sums. A tuning and test
+ * knob. No reference counterpart. */
+int gvizCudaForceSetWalkStackCap(gvizCudaForce *h, uint32_t entries);
 
 /* ---- checkpoints ------------------------------------------------------ */
 

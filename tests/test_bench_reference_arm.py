@@ -51,3 +51,33 @@ def test_learned_metric_is_the_headline_string():
     w = bench.Workload.__new__(bench.Workload)
     w.name = "ba1m_learned"
     assert w.metric() == metric
+
+
+def test_layout_stress_of_a_perfect_layout_is_zero():
+    """Stress at the best scale: zero for a path laid out on a line (graph
+    distance = Euclidean distance up to scale), positive once it is bent."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    V = 50
+    a = np.arange(V - 1, dtype=np.uint32)
+    b = a + 1
+    row, col = bench.csr_numpy(V, a, b)
+    line = np.stack([3.0 * np.arange(V), np.zeros(V)], 1).reshape(-1)
+    assert abs(bench.layout_stress(row, col, line, sources=5)) < 1e-12
+    bent = np.stack([np.cos(np.arange(V) * 0.3), np.sin(np.arange(V) * 0.3)], 1).reshape(-1)
+    assert bench.layout_stress(row, col, bent, sources=5) > 1e-3
+
+
+def test_vector_error_definitions():
+    sys.path.insert(0, ROOT)
+    import numpy as np
+
+    import bench
+    b = np.array([[1.0, 0.0], [0.0, 2.0]])
+    a = np.array([[1.1, 0.0], [0.0, 2.0]])
+    e = bench.vector_error(a, b)
+    assert abs(e["rms_err"] - 0.1 / np.sqrt(5.0)) < 1e-12
+    assert abs(e["max_rel_err_per_vertex"] - 0.1) < 1e-12
+    assert abs(e["rms_rel_err_per_vertex"] - np.sqrt(0.01 / 2)) < 1e-12

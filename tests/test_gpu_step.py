@@ -238,3 +238,34 @@ def test_fp32_free_run_tracks_oracle_as_a_layout(oracle):
     assert abs(e_gpu - e_ref) <= 1e-2 * e_ref, (e_gpu, e_ref)
     assert abs(r_gpu - r_ref) <= 1e-2 * r_ref, (r_gpu, r_ref)
     lay.close()
+
+
+@pytest.mark.parametrize("kw", [dict(model=1, theta=0.5, gravity=1.0),
+                                dict(model=0, theta=1.0, k=3),
+                                dict(model=1, theta=0.8, gravity=1.0, radius_base=1.0,
+                                     radius_per_degree=0.5, prevent_overlap=True)])
+def test_plain_walk_in_place_subtrees_agree(kw):
+    """The expanding plain walk with a stack too small for its pushes walks
+    those subtrees in place with the stackless union walk: the same
+    decisions (the same number of terms) and the same terms, so the forces
+    agree up to the order of the compensated FP32 sums. k = 3 gives cells
+    whose children are runs of points."""
+    from grapher_b200 import graphs
+    V = 20000
+    a, b = graphs.barabasi_albert(V, 3, 31)
+    row, col = csr_of(V, a, b)
+    lay = make_layout(row, col, cfg(**kw))
+    lay.begin(0, positions=graphs.randomize_positions(V, 300.0, 5))
+    for _ in range(3):
+        lay.step()
+    full = lay.repulsion()
+    n_full = lay.count_interactions()[0]
+    lay.set_walk_stack_cap(32)
+    small = lay.repulsion()
+    n_small = lay.count_interactions()[0]
+    lay.close()
+    assert n_small == n_full
+    d = np.linalg.norm(small - full, axis=1)
+    n = np.linalg.norm(full, axis=1)
+    assert float(np.sqrt(np.sum(d * d) / np.sum(n * n))) < 1e-6
+    assert float(np.max(d / np.maximum(n, 1e-30))) < 1e-4
