@@ -95,8 +95,8 @@ ADAPTER_LIB = os.path.join(LIBDIR, "libgvizcuda_gviz.so")
 def build_gviz_adapter(gviz_include: str | None = None) -> str | None:
     """Compiles the gviz-side glue against gviz's headers. The gviz symbols
     stay undefined: the program that loads it (gviz itself) provides them."""
-    inc = gviz_include or os.environ.get("GVIZ_INCLUDE") or "/root/reference/include"
-    if not os.path.isdir(inc):
+    inc = gviz_include or os.environ.get("GVIZ_INCLUDE")
+    if not inc or not os.path.isdir(inc):
         return None
     if os.path.exists(ADAPTER_LIB) and os.path.getmtime(ADAPTER_LIB) >= max(
             os.path.getmtime(ADAPTER_SRC), os.path.getmtime(GRIP_ADAPTER_SRC),
@@ -113,7 +113,9 @@ def build_gviz_adapter(gviz_include: str | None = None) -> str | None:
     return ADAPTER_LIB
 
 
-def build(verbose: bool = False) -> str:
+def build(verbose: bool = False, gviz_include: str | None = None) -> str:
+    """Compiles libgvizcuda and libgvizworkloads; the gviz glue as well when
+    gviz's headers are given (gviz_include or $GVIZ_INCLUDE)."""
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     hdr = _headers_mtime()
@@ -127,7 +129,7 @@ def build(verbose: bool = False) -> str:
         if out.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{out.stdout}{out.stderr}")
     build_workloads()
-    build_gviz_adapter()
+    build_gviz_adapter(gviz_include)
     return LIB
 
 
