@@ -892,6 +892,7 @@ constexpr uint32_t kGroupMax = 32;
 
 struct GroupArgs {
   const NodeF *nodes;
+  const uint4 *kids;
   const FarCell *cells;
   const uint32_t *cellCnt, *counts, *graphBase, *rootT;
   uint4 *groups;
@@ -943,20 +944,20 @@ __global__ __launch_bounds__(kThreads) void k_far_groups(GroupArgs a) {
       const uint32_t end = min(max((uint32_t)l.z, t + 1u), total);
       uint32_t chX[4], chY[4], chC[4], chQ[4];
       int nc = 0;
-      bool bucket = false;
-      for (uint32_t ch = t + 1u; ch < end;) {
-        const int4 m = node_link(a.nodes, ch);
-        const bool leaf = m.w >= 0;
-        const uint32_t sib = min(leaf ? ch + 1u : max((uint32_t)m.z, ch + 1u), end);
-        if (nc == 4) {
-          bucket = true;
-          break;
+      // the children from the cell's child record (independent loads): a
+      // run of more than four points is a leaf bucket
+      const uint4 kd = a.kids[t];
+      const bool bucket = kd.y == GVIZ_KIDS_RUN;
+      if (!bucket) {
+        const uint32_t kk[4] = {kd.x, kd.y, kd.z, kd.w};
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+          if (kk[i] > t && kk[i] < end) chX[nc++] = kk[i];
+        for (int i = 0; i < nc; i++) {
+          chY[i] = i + 1 < nc ? chX[i + 1] : end;
+          const int4 m = node_link(a.nodes, chX[i]);
+          chC[i] = m.w >= 0 ? 1u : a.cellCnt[chX[i]];
         }
-        chX[nc] = ch;
-        chY[nc] = sib;
-        chC[nc] = leaf ? 1u : a.cellCnt[ch];
-        nc++;
-        ch = sib;
       }
       if (bucket) {  // points of one smallest cell: runs of kGroupMax leaves
         runX = t + 1u;
@@ -1200,6 +1201,7 @@ void enqueue_tree_build(gvizCudaForce *h) {
   if (em.cellCnt && !em.f64) {
     GroupArgs ga;
     ga.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
+    ga.kids = h->d_kids;
     ga.cells = h->d_cells;
     ga.cellCnt = h->d_cellCnt;
     ga.counts = h->d_counts;
