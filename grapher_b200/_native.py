@@ -157,6 +157,7 @@ _SIGS = {
     "gvizCudaMlpCreate": (C.c_int, [C.POINTER(P), C.c_int, C.c_uint64]),
     "gvizCudaMlpDestroy": (None, [P]),
     "gvizCudaMlpParamCount": (C.c_int, []),
+    "gvizCudaMlpSetTrainingKernels": (C.c_int, [P, C.c_int]),
     "gvizCudaMlpSetWeights": (C.c_int, [P, C.POINTER(C.c_float)]),
     "gvizCudaMlpGetWeights": (C.c_int, [P, C.POINTER(C.c_float)]),
     "gvizCudaMlpGradient": (C.c_int, [P, C.POINTER(C.c_float), C.POINTER(C.c_float),

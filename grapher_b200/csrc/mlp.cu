@@ -41,6 +41,10 @@ struct gvizCudaMlp {
   float *d_gsum = nullptr;   // reduced gradient + loss
   size_t gradBlocks = 0;
   uint64_t step = 0;
+  bool tc = true;                // training kernels: tcgen05 (true) or mma.sync
+  uint32_t *d_status = nullptr;  // set by a tcgen05 kernel that gave up waiting
+  float *d_epochLoss = nullptr;  // per-epoch loss sums of a training run
+  size_t epochCap = 0;
 };
 
 namespace {
@@ -322,6 +326,372 @@ __global__ __launch_bounds__(32) void k_mlp_grad(const float *__restrict__ w,
   if (l == 0) out[MLP_PAD] = S.loss;
 }
 
+// ---------------------------------------------------------------------------
+// Training on the 5th-generation tensor cores (tcgen05): one CTA of 128
+// threads takes tiles of 128 samples (thread r = sample r of the tile = row
+// r of every M = 128 product); operands are staged in shared memory in the
+// no-swizzle canonical layouts (core matrices of 8 rows x 16 bytes),
+// accumulators live in tensor memory (TMEM), one thread issues the MMAs and
+// their completion is signalled through an mbarrier.
+//   D_act [128 x 64] (TMEM columns 0..63), reused by three products:
+//     X H1-pre = X W1^T, H2-pre = H1 W2^T, dH1-pre = dH2 W2
+//   D_grad [128 x 96] (columns 64..159), accumulated over the CTA's tiles:
+//     [dH2 | dH1]^T [H1 | X | 1]: rows 0..63 give dW2 and (column 80) db2,
+//     rows 64..127 give dW1 (columns 64..79) and db1 (column 80)
+//   D_w3 [128 x 16] (columns 160..175): [H2 | 1 | 0]^T [dY | 0]: rows 0..63
+//     give dW3^T, row 64 gives db3
+// The shared-memory buffers serve two roles each: the MN-major operand
+// [H1 | X | 1] (features x samples) is, read as K-major, the A operand of
+// the first two products, and [dH2 | dH1] is, read as K-major, the A of the
+// third. Layer 3 (64 -> 2) and dH2 = dY W3 run on the CUDA cores per thread.
+// BF16 rounding happens where the mma.sync kernel (and the oracle) round.
+// Every gradient entry is written by exactly one thread of the CTA.
+// ---------------------------------------------------------------------------
+constexpr int kTcThreads = 128;
+constexpr int kTcTilesPerBlock = 2;
+constexpr uint32_t kTcCols = 256;  // TMEM columns allocated (power of two >= 176)
+constexpr uint32_t kTcColGrad = 64, kTcColW3 = 160;
+constexpr uint32_t kTcSpin = 1u << 22;  // mbarrier polls before giving up
+
+struct __align__(128) TcSmem {
+  __nv_bfloat16 w1[64 * 16];     // K-major [n = hidden 1][k = input]
+  __nv_bfloat16 w2[64 * 64];     // K-major [n = hidden 2][k = hidden 1]
+  __nv_bfloat16 w2t[64 * 64];    // K-major [n = hidden 1][k = hidden 2]
+  __nv_bfloat16 bst[96 * 128];   // MN-major [n: H1 0..63 | X 64..79 | 1 80][k = sample]
+  __nv_bfloat16 ast[128 * 128];  // MN-major [m: dH2 0..63 | dH1 64..127][k = sample]
+  __nv_bfloat16 a2[128 * 128];   // MN-major [m: H2 0..63 | 1 64][k = sample]
+  __nv_bfloat16 b2[16 * 128];    // MN-major [n: dY 0..1][k = sample]
+  float w3[2][64];               // layer 3, BF16-rounded
+  float b1[64], b2v[64], b3[2];
+  float red[4];
+  unsigned long long bar;
+  uint32_t tmem;
+};
+
+// byte offset of element (row r, column k) of a K-major operand whose
+// 8-row groups are `sbo` bytes apart (K chunks of 8 elements 128 bytes apart)
+__device__ __forceinline__ uint32_t kmaj_off(uint32_t r, uint32_t k, uint32_t sbo) {
+  return (r & 7u) * 16u + (r >> 3) * sbo + (k >> 3) * 128u + (k & 7u) * 2u;
+}
+// byte offset of the 16-byte chunk holding elements n0..n0+7 (n0 % 8 == 0)
+// of sample k in an MN-major operand whose 8-sample groups are `lbo` apart
+__device__ __forceinline__ uint32_t mn_off(uint32_t n0, uint32_t k, uint32_t lbo) {
+  return (k & 7u) * 16u + (n0 >> 3) * 128u + (k >> 3) * lbo;
+}
+
+// shared-memory matrix descriptor: start, leading (K-group) and stride
+// (MN-group) byte offsets, version 1, no swizzle
+__device__ __forceinline__ uint64_t tc_desc(const void *p, uint32_t lbo, uint32_t sbo) {
+  const uint32_t a = smem_u32(p);
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B
+__host__ __device__ constexpr uint32_t tc_idesc(uint32_t M, uint32_t N, uint32_t aMN, uint32_t bMN) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (aMN << 15) | (bMN << 16) | ((N >> 3) << 17) |
+         ((M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc,
+                                       uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_commit(const unsigned long long *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void proxy_fence() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Waits for the mbarrier phase with a bounded number of polls; false when
+// it gave up.
+__device__ __forceinline__ bool tc_wait(const unsigned long long *bar, uint32_t phase) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < kTcSpin; it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_wait_ld() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float bfr(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// 8 BF16 values as one 16-byte chunk
+__device__ __forceinline__ uint4 pack8(const float *v) {
+  return make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]),
+                    pack_bf16(v[6], v[7]));
+}
+
+__global__ __launch_bounds__(kTcThreads, 1) void k_mlp_grad_tc(
+    const float *__restrict__ w, const float *__restrict__ X, const float *__restrict__ T,
+    const float *__restrict__ Wt, const uint32_t *__restrict__ order, uint32_t n, float scale,
+    float *partial, uint32_t *status) {
+  extern __shared__ __align__(128) unsigned char tcraw[];
+  TcSmem &S = *reinterpret_cast<TcSmem *>(tcraw);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  unsigned char *w1b = reinterpret_cast<unsigned char *>(S.w1);
+  unsigned char *w2b = reinterpret_cast<unsigned char *>(S.w2);
+  unsigned char *w2tb = reinterpret_cast<unsigned char *>(S.w2t);
+  unsigned char *bstb = reinterpret_cast<unsigned char *>(S.bst);
+  unsigned char *astb = reinterpret_cast<unsigned char *>(S.ast);
+  unsigned char *a2b = reinterpret_cast<unsigned char *>(S.a2);
+  unsigned char *b2b = reinterpret_cast<unsigned char *>(S.b2);
+  // ---- weights and constant operand parts --------------------------------
+  for (uint32_t i = tid; i < 64 * 16; i += kTcThreads) {
+    const uint32_t r = i / 16, k = i % 16;
+    *reinterpret_cast<__nv_bfloat16 *>(w1b + kmaj_off(r, k, 256)) =
+        __float2bfloat16_rn(k < MLP_IN ? w[OFF_W1 + i] : 0.f);
+  }
+  for (uint32_t i = tid; i < 64 * 64; i += kTcThreads) {
+    const uint32_t r = i / 64, k = i % 64;  // w2t master: [out r][in k]
+    const __nv_bfloat16 v = __float2bfloat16_rn(w[OFF_W2 + i]);
+    *reinterpret_cast<__nv_bfloat16 *>(w2b + kmaj_off(r, k, 1024)) = v;
+    *reinterpret_cast<__nv_bfloat16 *>(w2tb + kmaj_off(k, r, 1024)) = v;
+  }
+  for (uint32_t i = tid; i < 2 * 64; i += kTcThreads) S.w3[i / 64][i % 64] = bfr(w[OFF_W3 + i]);
+  for (uint32_t i = tid; i < 64; i += kTcThreads) {
+    S.b1[i] = w[OFF_B1 + i];
+    S.b2v[i] = w[OFF_B2 + i];
+  }
+  if (tid < 2) S.b3[tid] = w[OFF_B3 + tid];
+  {
+    // per sample: bst n 80..95 = [1, 0 ...], a2 m 64..127 = [1, 0 ...],
+    // b2 n 8..15 = 0
+    const float one[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const uint32_t k = tid;
+    *reinterpret_cast<uint4 *>(bstb + mn_off(80, k, 1536)) = pack8(one);
+    *reinterpret_cast<uint4 *>(bstb + mn_off(88, k, 1536)) = pack8(zero);
+    *reinterpret_cast<uint4 *>(a2b + mn_off(64, k, 2048)) = pack8(one);
+    for (uint32_t n0 = 72; n0 < 128; n0 += 8)
+      *reinterpret_cast<uint4 *>(a2b + mn_off(n0, k, 2048)) = pack8(zero);
+    *reinterpret_cast<uint4 *>(b2b + mn_off(8, k, 256)) = pack8(zero);
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&S.tmem)),
+                 "r"(kTcCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  proxy_fence();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = S.tmem;
+  const uint32_t lane_base = tbase + ((warp * 32u) << 16);  // this warp's TMEM lanes
+  const uint32_t idAct = tc_idesc(128, 64, 0, 0);
+  const uint32_t idGrad = tc_idesc(128, 96, 1, 1);
+  const uint32_t idW3 = tc_idesc(128, 16, 1, 1);
+  uint32_t phase = 0;
+  bool ok = true;
+  float lossAcc = 0.f;
+  const uint32_t nTiles = (n + kTcThreads - 1) / kTcThreads;
+  const uint32_t t0 = blockIdx.x * kTcTilesPerBlock;
+  const uint32_t t1 = min(t0 + kTcTilesPerBlock, nTiles);
+  // issue (thread 0) a chain of MMAs after the block's shared-memory
+  // writes, then wait for it everywhere
+  // (ok stays block-uniform: a wait that gave up anywhere stops every thread)
+  auto sync_issue_wait = [&](auto issue) {
+    proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      issue();
+      tc_commit(&S.bar);
+    }
+    const bool got = tc_wait(&S.bar, phase);
+    phase ^= 1u;
+    ok = __syncthreads_and(got ? 1 : 0) != 0;
+    tc_fence_after();
+  };
+  for (uint32_t tile = t0; tile < t1 && ok; tile++) {
+    const uint32_t sIdx = tile * kTcThreads + tid;
+    const bool valid = sIdx < n;
+    const uint32_t src = valid ? (order ? order[sIdx] : sIdx) : 0u;
+    float x[16];
+#pragma unroll
+    for (int f = 0; f < 16; f++)
+      x[f] = (valid && f < MLP_IN) ? X[(size_t)src * MLP_IN + f] : 0.f;
+    const float tg0 = valid ? T[(size_t)src * 2] : 0.f, tg1 = valid ? T[(size_t)src * 2 + 1] : 0.f;
+    const float wt = valid ? (Wt ? Wt[src] : 1.f) : 0.f;
+    *reinterpret_cast<uint4 *>(bstb + mn_off(64, tid, 1536)) = pack8(x);
+    *reinterpret_cast<uint4 *>(bstb + mn_off(72, tid, 1536)) = pack8(x + 8);
+    // ---- layer 1: D_act = X W1^T (K = 16) -------------------------------
+    sync_issue_wait([&] {
+      tc_mma(tbase, tc_desc(bstb + 1024, 128, 1536), tc_desc(w1b, 128, 256), idAct, 0u);
+    });
+    if (!ok) break;
+    float h1[64];
+    uint32_t m1a = 0, m1b = 0;  // ReLU masks of layer 1 (bits 0..31, 32..63)
+#pragma unroll
+    for (int c = 0; c < 4; c++) tc_ld16(lane_base + 16 * c, h1 + 16 * c);
+    tc_wait_ld();
+#pragma unroll
+    for (int j = 0; j < 64; j++) {
+      const float v = fmaxf(h1[j] + S.b1[j], 0.f);
+      h1[j] = v;
+      if (v > 0.f) {
+        if (j < 32) m1a |= 1u << j;
+        else m1b |= 1u << (j - 32);
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < 8; g++)
+      *reinterpret_cast<uint4 *>(bstb + mn_off(8 * g, tid, 1536)) = pack8(h1 + 8 * g);
+    // ---- layer 2: D_act = H1 W2^T (K = 64) -------------------------------
+    sync_issue_wait([&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < 4; kk++)
+        tc_mma(tbase, tc_desc(bstb + 256 * kk, 128, 1536), tc_desc(w2b + 256 * kk, 128, 1024),
+               idAct, kk);
+    });
+    if (!ok) break;
+    float h2[64];
+#pragma unroll
+    for (int c = 0; c < 4; c++) tc_ld16(lane_base + 16 * c, h2 + 16 * c);
+    tc_wait_ld();
+    float y0 = S.b3[0], y1 = S.b3[1];
+#pragma unroll
+    for (int j = 0; j < 64; j++) {
+      h2[j] = bfr(fmaxf(h2[j] + S.b2v[j], 0.f));
+      y0 += h2[j] * S.w3[0][j];
+      y1 += h2[j] * S.w3[1][j];
+    }
+    // ---- layer 3 on the CUDA cores, loss and dY ----------------------------
+    const float e0 = y0 - tg0, e1 = y1 - tg1;
+    const float d0 = bfr(2.f * scale * wt * e0), d1 = bfr(2.f * scale * wt * e1);
+    lossAcc += scale * wt * (e0 * e0 + e1 * e1);
+    {
+      const float dy[8] = {d0, d1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      *reinterpret_cast<uint4 *>(b2b + mn_off(0, tid, 256)) = pack8(dy);
+    }
+    // dH2 = (dY W3) masked by H2 > 0, BF16
+    float dh[64];
+#pragma unroll
+    for (int j = 0; j < 64; j++) dh[j] = h2[j] > 0.f ? d0 * S.w3[0][j] + d1 * S.w3[1][j] : 0.f;
+#pragma unroll
+    for (int g = 0; g < 8; g++) {
+      *reinterpret_cast<uint4 *>(a2b + mn_off(8 * g, tid, 2048)) = pack8(h2 + 8 * g);
+      *reinterpret_cast<uint4 *>(astb + mn_off(8 * g, tid, 2048)) = pack8(dh + 8 * g);
+    }
+    // ---- dH1 = dH2 W2 (K = 64) --------------------------------------------
+    sync_issue_wait([&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < 4; kk++)
+        tc_mma(tbase, tc_desc(astb + 256 * kk, 128, 2048), tc_desc(w2tb + 256 * kk, 128, 1024),
+               idAct, kk);
+    });
+    if (!ok) break;
+#pragma unroll
+    for (int c = 0; c < 4; c++) tc_ld16(lane_base + 16 * c, dh + 16 * c);
+    tc_wait_ld();
+#pragma unroll
+    for (int j = 0; j < 64; j++) {
+      const bool on = j < 32 ? (m1a >> j) & 1u : (m1b >> (j - 32)) & 1u;
+      dh[j] = on ? dh[j] : 0.f;
+    }
+#pragma unroll
+    for (int g = 0; g < 8; g++)
+      *reinterpret_cast<uint4 *>(astb + mn_off(64 + 8 * g, tid, 2048)) = pack8(dh + 8 * g);
+    // ---- weight gradients, accumulated in TMEM over the CTA's tiles (K = 128)
+    const uint32_t first = tile == t0 ? 1u : 0u;
+    sync_issue_wait([&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < 8; kk++) {
+        const uint32_t acc = (first && kk == 0) ? 0u : 1u;
+        tc_mma(tbase + kTcColGrad, tc_desc(astb + 4096 * kk, 2048, 128),
+               tc_desc(bstb + 3072 * kk, 1536, 128), idGrad, acc);
+        tc_mma(tbase + kTcColW3, tc_desc(a2b + 4096 * kk, 2048, 128),
+               tc_desc(b2b + 512 * kk, 256, 128), idW3, acc);
+      }
+    });
+  }
+  // ---- this CTA's gradient: row tid of D_grad and D_w3 ---------------------
+  float *out = partial + (size_t)blockIdx.x * (MLP_PAD + 1);
+  if (ok && t0 < t1) {
+    float g[96], g3[16];
+#pragma unroll
+    for (int c = 0; c < 6; c++) tc_ld16(lane_base + kTcColGrad + 16 * c, g + 16 * c);
+    tc_ld16(lane_base + kTcColW3, g3);
+    tc_wait_ld();
+    if (tid < 64) {
+      for (int j = 0; j < 64; j++) out[OFF_W2 + tid * 64 + j] = g[j];
+      out[OFF_B2 + tid] = g[80];
+      out[OFF_W3 + tid] = g3[0];
+      out[OFF_W3 + 64 + tid] = g3[1];
+      for (int o = 2; o < MLP_OUTP; o++) out[OFF_W3 + o * 64 + tid] = 0.f;
+    } else {
+      const uint32_t r = tid - 64;
+      for (int c = 0; c < MLP_INP; c++) out[OFF_W1 + r * MLP_INP + c] = g[64 + c];
+      out[OFF_B1 + r] = g[80];
+      if (tid == 64) {
+        out[OFF_B3] = g3[0];
+        out[OFF_B3 + 1] = g3[1];
+        for (int o = 2; o < MLP_OUTP; o++) out[OFF_B3 + o] = 0.f;
+      }
+    }
+  } else {
+    for (uint32_t i = tid; i < MLP_PAD; i += kTcThreads) out[i] = 0.f;
+  }
+  // loss: the block's sum
+  float l = lossAcc;
+  for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+  if ((tid & 31u) == 0) S.red[warp] = l;
+  tc_fence_before();
+  __syncthreads();
+  if (tid == 0) out[MLP_PAD] = ok ? (S.red[0] + S.red[1]) + (S.red[2] + S.red[3]) : NAN;
+  if (!ok && tid == 0) atomicOr(status, 1u);
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase),
+                 "r"(kTcCols)
+                 : "memory");
+  }
+}
+
 // Sum of the per-block partials in block order.
 __global__ void k_mlp_reduce(const float *partial, uint32_t blocks, float *sum) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -333,8 +703,9 @@ __global__ void k_mlp_reduce(const float *partial, uint32_t blocks, float *sum) 
 
 __global__ void k_mlp_adam(float *w, float *m, float *v, const float *grad,
                            float lr, float b1, float b2, float eps,
-                           float c1, float c2) {
+                           float c1, float c2, float *epochLoss, float batchSamples) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0 && epochLoss) *epochLoss += grad[MLP_PAD] * batchSamples;
   if (i >= MLP_PAD) return;
   if (!is_real_param(i)) {
     w[i] = 0.f;
@@ -538,7 +909,9 @@ int gvizCudaMlpCreate(gvizCudaMlp **out, int device, uint64_t seed) {
       cudaMalloc(&m->d_m, MLP_PAD * 4) != cudaSuccess ||
       cudaMalloc(&m->d_v, MLP_PAD * 4) != cudaSuccess ||
       cudaMalloc(&m->d_dev, sizeof(MlpDev)) != cudaSuccess ||
-      cudaMalloc(&m->d_gsum, (MLP_PAD + 1) * 4) != cudaSuccess) {
+      cudaMalloc(&m->d_gsum, (MLP_PAD + 1) * 4) != cudaSuccess ||
+      cudaMalloc(&m->d_status, 4) != cudaSuccess ||
+      cudaMemset(m->d_status, 0, 4) != cudaSuccess) {
     gvizCudaMlpDestroy(m);
     return GVIZ_CUDA_ERR_ALLOC;
   }
@@ -576,11 +949,19 @@ void gvizCudaMlpDestroy(gvizCudaMlp *m) {
   cudaFree(m->d_dev);
   cudaFree(m->d_grad);
   cudaFree(m->d_gsum);
+  cudaFree(m->d_status);
+  cudaFree(m->d_epochLoss);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
 }
 
 int gvizCudaMlpParamCount(void) { return MLP_PAD; }
+
+int gvizCudaMlpSetTrainingKernels(gvizCudaMlp *m, int tcgen05) {
+  if (!m || (tcgen05 != 0 && tcgen05 != 1)) return GVIZ_CUDA_ERR_ARG;
+  m->tc = tcgen05 != 0;
+  return GVIZ_CUDA_OK;
+}
 
 int gvizCudaMlpSetWeights(gvizCudaMlp *m, const float *w) {
   if (!m || !w) return GVIZ_CUDA_ERR_ARG;
@@ -605,8 +986,9 @@ int gvizCudaMlpGetWeights(gvizCudaMlp *m, float *w) {
 static int mlp_grad_launch(gvizCudaMlp *m, const float *dX, const float *dT,
                            const float *dW, const uint32_t *dOrder, uint32_t n,
                            float scale) {
-  const uint32_t tiles = (n + 31) / 32;
-  const uint32_t blocks = (tiles + kTilesPerBlock - 1) / kTilesPerBlock;
+  const uint32_t tiles = m->tc ? (n + kTcThreads - 1) / kTcThreads : (n + 31) / 32;
+  const uint32_t per = m->tc ? kTcTilesPerBlock : kTilesPerBlock;
+  const uint32_t blocks = (tiles + per - 1) / per;
   if (blocks > m->gradBlocks) {
     cudaFree(m->d_grad);
     m->d_grad = nullptr;
@@ -618,11 +1000,30 @@ static int mlp_grad_launch(gvizCudaMlp *m, const float *dX, const float *dT,
   if (!attr) {
     cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)sizeof(TrainSmem));
+    cudaFuncSetAttribute(k_mlp_grad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(TcSmem));
     attr = true;
   }
-  k_mlp_grad<<<blocks, 32, sizeof(TrainSmem), m->stream>>>(m->d_w, dX, dT, dW, dOrder, n,
-                                                           scale, m->d_grad);
+  if (m->tc)
+    k_mlp_grad_tc<<<blocks, kTcThreads, sizeof(TcSmem), m->stream>>>(
+        m->d_w, dX, dT, dW, dOrder, n, scale, m->d_grad, m->d_status);
+  else
+    k_mlp_grad<<<blocks, 32, sizeof(TrainSmem), m->stream>>>(m->d_w, dX, dT, dW, dOrder, n,
+                                                             scale, m->d_grad);
   k_mlp_reduce<<<(MLP_PAD + 1 + 255) / 256, 256, 0, m->stream>>>(m->d_grad, blocks, m->d_gsum);
+  return GVIZ_CUDA_OK;
+}
+
+// After a synchronisation: GVIZ_CUDA_ERR_CUDA when a tcgen05 kernel gave up
+// waiting for its tensor-core work (status cleared for the next call).
+static int mlp_status(gvizCudaMlp *m) {
+  uint32_t st = 0;
+  if (cudaMemcpy(&st, m->d_status, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return GVIZ_CUDA_ERR_CUDA;
+  if (st) {
+    cudaMemset(m->d_status, 0, 4);
+    return GVIZ_CUDA_ERR_CUDA;
+  }
   return GVIZ_CUDA_OK;
 }
 
@@ -649,8 +1050,9 @@ int gvizCudaMlpGradient(gvizCudaMlp *m, const float *X, const float *T,
   if (!rc && cudaMemcpyAsync(gs.data(), m->d_gsum, (MLP_PAD + 1) * 4, cudaMemcpyDeviceToHost,
                              m->stream) == cudaSuccess &&
       cudaStreamSynchronize(m->stream) == cudaSuccess) {
-    if (grad) memcpy(grad, gs.data(), MLP_PAD * 4);
-    if (loss) *loss = gs[MLP_PAD];
+    rc = mlp_status(m);
+    if (!rc && grad) memcpy(grad, gs.data(), MLP_PAD * 4);
+    if (!rc && loss) *loss = gs[MLP_PAD];
   } else if (!rc) {
     rc = GVIZ_CUDA_ERR_CUDA;
   }
@@ -691,11 +1093,26 @@ int gvizCudaMlpTrain(gvizCudaMlp *m, const float *X, const float *T,
     return z ^ (z >> 31);
   };
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-  std::vector<float> gs(MLP_PAD + 1);
+  // the epochs' losses are summed on the device (no synchronisation per
+  // mini-batch) and read once at the end
+  if (!rc && lossOut && epochs > m->epochCap) {
+    cudaFree(m->d_epochLoss);
+    m->d_epochLoss = nullptr;
+    m->epochCap = 0;
+    if (cudaMalloc(&m->d_epochLoss, epochs * sizeof(float)) != cudaSuccess)
+      rc = GVIZ_CUDA_ERR_ALLOC;
+    else
+      m->epochCap = epochs;
+  }
+  if (!rc && lossOut) cudaMemsetAsync(m->d_epochLoss, 0, epochs * sizeof(float), m->stream);
+  // one pinned staging buffer for the per-epoch order upload
+  uint32_t *hOrder = nullptr;
+  if (!rc && cudaMallocHost(&hOrder, n * 4) != cudaSuccess) rc = GVIZ_CUDA_ERR_ALLOC;
   for (uint32_t ep = 0; ep < epochs && !rc; ep++) {
     for (size_t i = n - 1; i > 0; i--) std::swap(order[i], order[rnd() % (i + 1)]);
-    cudaMemcpyAsync(dOrder, order.data(), n * 4, cudaMemcpyHostToDevice, m->stream);
-    double epochLoss = 0.0;
+    cudaStreamSynchronize(m->stream);  // the previous epoch's upload is done
+    memcpy(hOrder, order.data(), n * 4);
+    cudaMemcpyAsync(dOrder, hOrder, n * 4, cudaMemcpyHostToDevice, m->stream);
     for (size_t b0 = 0; b0 < n && !rc; b0 += batch) {
       const uint32_t nb = (uint32_t)std::min<size_t>(batch, n - b0);
       double wsum = 0.0;
@@ -704,19 +1121,22 @@ int gvizCudaMlpTrain(gvizCudaMlp *m, const float *X, const float *T,
       if (rc) break;
       m->step++;
       const float c1 = 1.f - powf(b1, (float)m->step), c2 = 1.f - powf(b2, (float)m->step);
-      k_mlp_adam<<<(MLP_PAD + 255) / 256, 256, 0, m->stream>>>(m->d_w, m->d_m, m->d_v,
-                                                               m->d_gsum, lr, b1, b2, eps, c1, c2);
-      if (lossOut) {
-        float lv = 0.f;
-        cudaMemcpyAsync(&lv, m->d_gsum + MLP_PAD, 4, cudaMemcpyDeviceToHost, m->stream);
-        cudaStreamSynchronize(m->stream);
-        epochLoss += (double)lv * nb;
-      }
+      k_mlp_adam<<<(MLP_PAD + 255) / 256, 256, 0, m->stream>>>(
+          m->d_w, m->d_m, m->d_v, m->d_gsum, lr, b1, b2, eps, c1, c2,
+          lossOut ? m->d_epochLoss + ep : nullptr, (float)nb);
     }
-    if (lossOut) lossOut[ep] = (float)(epochLoss / (double)n);
   }
   k_mlp_to_dev<<<(MLP_PAD + 255) / 256, 256, 0, m->stream>>>(m->d_w, m->d_dev);
   if (cudaStreamSynchronize(m->stream) != cudaSuccess && !rc) rc = GVIZ_CUDA_ERR_CUDA;
+  if (!rc) rc = mlp_status(m);
+  if (!rc && lossOut) {
+    std::vector<float> el(epochs);
+    if (cudaMemcpy(el.data(), m->d_epochLoss, epochs * sizeof(float), cudaMemcpyDeviceToHost) !=
+        cudaSuccess)
+      rc = GVIZ_CUDA_ERR_CUDA;
+    for (uint32_t ep = 0; ep < epochs && !rc; ep++) lossOut[ep] = (float)(el[ep] / (double)n);
+  }
+  cudaFreeHost(hOrder);
   cudaFree(dX);
   cudaFree(dT);
   cudaFree(dW);

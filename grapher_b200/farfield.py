@@ -33,6 +33,11 @@ class FarFieldModel:
         self.h = h
         self.nparams = int(self.L.gvizCudaMlpParamCount())
 
+    def set_training_kernels(self, tcgen05=True):
+        """Gradient and training kernels: tcgen05 (default) or mma.sync."""
+        N.check(self.L.gvizCudaMlpSetTrainingKernels(self.h, 1 if tcgen05 else 0),
+                "gvizCudaMlpSetTrainingKernels")
+
     def weights(self):
         w = np.zeros(self.nparams, np.float32)
         N.check(self.L.gvizCudaMlpGetWeights(self.h, N.ptr(w, C.c_float)), "gvizCudaMlpGetWeights")

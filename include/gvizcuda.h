@@ -275,6 +275,13 @@ int gvizCudaMlpParamCount(void);
 int gvizCudaMlpSetWeights(gvizCudaMlp *m, const float *w);
 int gvizCudaMlpGetWeights(gvizCudaMlp *m, float *w);
 
+/* The kernels of the gradient and of training: 1 (default) the tcgen05
+ * path (tiles of 128 samples, one M = 128 MMA per layer with the
+ * accumulators in tensor memory, weight gradients accumulated there over a
+ * CTA's tiles), 0 the mma.sync path (warp tiles of 32 samples). Both round
+ * to BF16 at the same places; results differ by FP32 summation order. */
+int gvizCudaMlpSetTrainingKernels(gvizCudaMlp *m, int tcgen05);
+
 /* Gradient (master layout) and value of the weighted mean squared error
  * sum_i W_i |MLP(X_i) - T_i|^2 / sum_i W_i over n samples (X n*10, T n*2,
  * W n or NULL), from the BF16 tensor-core forward/backward kernels. */

@@ -25,10 +25,14 @@ def _batch(n=1000, seed=0):
     return X, T, W
 
 
+@pytest.mark.parametrize("tc", [True, False], ids=["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("n", [1, 17, 1000, 5000])
-def test_gradient_matches_oracle(n):
+def test_gradient_matches_oracle(n, tc):
+    """Both training paths (tcgen05 with TMEM accumulators, and mma.sync)
+    against the FP64 oracle with BF16 rounding where the kernels round."""
     from oracle import mlp_oracle as MO
     m = _model()
+    m.set_training_kernels(tc)
     w = m.weights().astype(np.float64)
     X, T, W = _batch(n)
     loss, g = m.gradient(X, T, W)
@@ -41,6 +45,19 @@ def test_gradient_matches_oracle(n):
     assert np.linalg.norm(g - go) <= 2e-3 * np.linalg.norm(go)
     # padding entries of the master layout never receive gradient
     assert np.all(g[go == 0.0] == 0.0)
+
+
+def test_training_paths_agree():
+    """The tcgen05 and mma.sync gradients of one batch (several CTAs, a
+    ragged last tile) agree up to FP32 summation order."""
+    X, T, W = _batch(3000, 5)
+    m = _model(2)
+    m.set_training_kernels(True)
+    l1, g1 = m.gradient(X, T, W)
+    m.set_training_kernels(False)
+    l2, g2 = m.gradient(X, T, W)
+    assert abs(l1 - l2) <= 1e-5 * abs(l2)
+    assert np.linalg.norm(g1 - g2) <= 1e-3 * np.linalg.norm(g2)
 
 
 def test_gradient_unweighted_equals_unit_weights():
@@ -70,10 +87,12 @@ def test_weights_round_trip_and_validation():
         m.gradient(np.zeros((0, 10), np.float32), np.zeros((0, 2), np.float32))
 
 
-def test_training_fits_quadrupole_law():
+@pytest.mark.parametrize("tc", [True, False], ids=["tcgen05", "mma_sync"])
+def test_training_fits_quadrupole_law(tc):
     """Adam over the tensor-core gradient learns the leading 1/r correction
     t = (f1, -f2) from random features."""
     m = _model(7)
+    m.set_training_kernels(tc)
     rng = np.random.default_rng(8)
     X = rng.uniform(-0.3, 0.3, (20000, 10)).astype(np.float32)
     T = np.stack([X[:, 1], -X[:, 2]], 1).astype(np.float32)
