@@ -446,11 +446,15 @@ HUB_THETA = 0.35         # their plain walk's opening threshold
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
 # The learned comparison starts from a fixed point of the layout, whatever
 # --warmup asks for: LEARNED_PRE_STEPS plain steps from the initial
-# positions, then the harvest snapshots HARVEST_GAP steps apart; the judged
-# and timed state is the one after the last snapshot. --warmup steps run
-# before each timed region, from that saved state.
+# positions, then the harvest snapshots of HARVEST_SCHEDULE; the judged and
+# timed state is the one of the last snapshot. --warmup steps run before each
+# timed region, from that saved state.
 LEARNED_PRE_STEPS = 20
-HARVEST_GAP = 5
+# (steps before the snapshot, opening threshold of its pairs): earlier
+# states at smaller thresholds, and the state the learned walk then runs
+# from at the large ones it is meant for (the network fits the layout it is
+# trained on; the judge checks it on every vertex of that state)
+HARVEST_SCHEDULE = ((0, 0.7), (5, 0.95), (5, 1.2), (0, 1.05))
 JUDGE_VERTICES = 65536
 JUDGE_ALL_MAX = 1 << 20  # layouts up to this size are judged on every vertex
 JUDGE_CHUNK = 262144     # targets per exact FP64 repulsion call
@@ -492,10 +496,9 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     rng = np.random.default_rng(SEED)
     t0 = time.perf_counter()
     Xs, Ts, Ws = [], [], []
-    for snap, th in enumerate((1.2, 0.9, 0.6)):  # cells of every angular size
-        if snap:
-            for _ in range(HARVEST_GAP):
-                lay.step()
+    for snap, (gap, th) in enumerate(HARVEST_SCHEDULE):  # cells of every angular size
+        for _ in range(gap):
+            lay.step()
         t = np.sort(rng.choice(w.V, HARVEST_TARGETS, replace=False)).astype(np.uint32)
         X, T, Wt = harvest_training_set(lay, th, t)
         Xs.append(X), Ts.append(T), Ws.append(Wt)
