@@ -166,6 +166,7 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_graphBase);
   dfree(h->d_nodes);
   dfree(h->d_kids);
+  dfree(h->d_exactPartial);
   dfree(h->d_leafDepth);
   dfree(h->d_counters);
   dfree(h->d_walkQueue);
@@ -739,6 +740,12 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_graphBase, G);
   rc |= dalloc(h, &h->d_nodes, h->maxNodes * sizeof(NodeD));
   rc |= dalloc(h, &h->d_kids, h->maxNodes);
+  {
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+    h->exactSplits = exact_splits(V, sms);
+    if (h->exactSplits > 1) rc |= dalloc(h, &h->d_exactPartial, (size_t)h->exactSplits * V);
+  }
   rc |= dalloc(h, &h->d_leafDepth, Vs);
   rc |= dalloc(h, &h->d_counters, 8);
   rc |= dalloc(h, &h->d_walkQueue, 1);

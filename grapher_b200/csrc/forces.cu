@@ -15,6 +15,8 @@
 // Per-vertex sums are Kahan-compensated FP32; the epilogue is FP64.
 #include <math.h>
 
+#include <algorithm>
+
 #include "epilogue.cuh"
 #include "internal.cuh"
 #include "mlp.cuh"
@@ -29,8 +31,8 @@ namespace {
 constexpr int kWalkThreads = 128;     // default block size of the walk
 constexpr int kWalkMaxThreads = 512;  // largest block size the autotuner tries
 constexpr int kAttrThreads = 256;
-constexpr int kExactThreads = 256;
-constexpr int kExactTile = 256;
+constexpr int kExactThreads = 128;
+constexpr int kExactTile = 128;
 constexpr int kExactTpt = 4;     // exact mode: targets per thread
 constexpr int kExactChunk = 32;  // exact mode: sources per plain partial sum
 constexpr uint32_t kInf = 0xffffffffu;
@@ -1378,6 +1380,8 @@ struct ExactArgs {
   EpiArgs epi;
   float num, overlapC;
   uint32_t V;
+  double2 *partial;  // [splits][V] per-split sums (splits > 1)
+  uint32_t splits;
 };
 
 // Exact all-pairs repulsion (src/embedders/gvizForceEmbedder.c:104-115) as
@@ -1392,6 +1396,10 @@ struct ExactArgs {
 // d2 == 0) sends the warp through the guarded path for that source, which
 // skips the self pair and applies the coincident direction. Tiles that
 // straddle a graph boundary of a forest take the guarded path too.
+// The sources are split into gridDim.y consecutive ranges of whole tiles
+// (so that small layouts still fill the GPU); with more than one range each
+// block writes its per-target partial sums and k_exact_combine adds them in
+// range order.
 template <int MODEL, bool OVERLAP>
 __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
   __shared__ float4 sp[kExactTile];
@@ -1431,7 +1439,12 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
   }
   __syncthreads();
   const uint32_t lo = sRange[0], hi = sRange[1];
-  for (uint32_t t0 = lo; t0 < hi; t0 += kExactTile) {
+  // this block's source range: whole tiles, split blockIdx.y of gridDim.y
+  const uint32_t nTile = hi > lo ? (hi - lo + kExactTile - 1) / kExactTile : 0u;
+  const uint32_t per = (nTile + gridDim.y - 1) / gridDim.y;
+  const uint32_t s0 = lo + min(blockIdx.y * per, nTile) * kExactTile;
+  const uint32_t s1 = min(hi, lo + min((blockIdx.y + 1) * per, nTile) * kExactTile);
+  for (uint32_t t0 = s0; t0 < s1; t0 += kExactTile) {
     __syncthreads();
     const uint32_t j = t0 + threadIdx.x;
     if (threadIdx.x < kExactTile && j < hi) {
@@ -1499,9 +1512,29 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
 #pragma unroll
   for (int k = 0; k < kExactTpt; k++) {
     if (!act[k]) continue;
+    if (gridDim.y > 1) {
+      a.partial[(size_t)blockIdx.y * a.V + v[k]] = make_double2(kx[k].value(), ky[k].value());
+      continue;
+    }
     const float2 at = a.attF[v[k]];
     force_epilogue(a.epi, v[k], (double)at.x, (double)at.y, kx[k].value(), ky[k].value());
   }
+}
+
+// The split sums of each target added in range order, then its epilogue.
+__global__ __launch_bounds__(256) void k_exact_combine(ExactArgs a) {
+  const uint32_t v = blockIdx.x * 256 + threadIdx.x;
+  if (v >= a.V) return;
+  const uint32_t g = a.gid ? a.gid[v] : 0u;
+  if (a.active && a.active[g] == 0u) return;
+  double sx = 0.0, sy = 0.0;
+  for (uint32_t s = 0; s < a.splits; s++) {
+    const double2 p = a.partial[(size_t)s * a.V + v];
+    sx += p.x;
+    sy += p.y;
+  }
+  const float2 at = a.attF[v];
+  force_epilogue(a.epi, v, (double)at.x, (double)at.y, sx, sy);
 }
 
 inline uint32_t blocks(size_t n, int t) { return (uint32_t)((n + t - 1) / t); }
@@ -1798,6 +1831,16 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   prof_mark(h, "bh_walk_f32");
 }
 
+// Source ranges of the exact FP32 kernel for V vertices on a GPU of `sms`
+// SMs: enough blocks for about four waves, at least four tiles per range.
+uint32_t exact_splits(size_t V, int sms) {
+  const size_t tb = (V + kExactThreads * kExactTpt - 1) / (kExactThreads * kExactTpt);
+  if (tb == 0) return 1;
+  size_t s = (4 * (size_t)(sms > 0 ? sms : 1) + tb - 1) / tb;
+  s = std::min<size_t>(s, (V + 4 * kExactTile - 1) / (4 * kExactTile));
+  return (uint32_t)std::max<size_t>(1, std::min<size_t>(s, 32));
+}
+
 void enqueue_exact_f32(gvizCudaForce *h) {
   ExactArgs a;
   a.pos = h->d_pos;
@@ -1811,7 +1854,9 @@ void enqueue_exact_f32(gvizCudaForce *h) {
   a.num = (float)(h->params.edgeLength * h->params.edgeLength);
   a.overlapC = (float)h->params.overlapConstant;
   a.V = (uint32_t)h->V;
-  const uint32_t grid = blocks(h->V, kExactThreads * kExactTpt);
+  a.partial = h->d_exactPartial;
+  a.splits = h->d_exactPartial ? h->exactSplits : 1u;
+  const dim3 grid(blocks(h->V, kExactThreads * kExactTpt), a.splits);
   const bool ov = h->params.preventOverlap != 0;
   if (h->model == GVIZ_CUDA_MODEL_FR) {
     if (ov) k_exact_f32<GVIZ_CUDA_MODEL_FR, true><<<grid, kExactThreads, 0, h->stream>>>(a);
@@ -1820,5 +1865,6 @@ void enqueue_exact_f32(gvizCudaForce *h) {
     if (ov) k_exact_f32<GVIZ_CUDA_MODEL_LINLOG, true><<<grid, kExactThreads, 0, h->stream>>>(a);
     else k_exact_f32<GVIZ_CUDA_MODEL_LINLOG, false><<<grid, kExactThreads, 0, h->stream>>>(a);
   }
+  if (a.splits > 1) k_exact_combine<<<blocks(h->V, 256), 256, 0, h->stream>>>(a);
   prof_mark(h, "exact_f32");
 }

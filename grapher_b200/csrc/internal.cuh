@@ -179,6 +179,8 @@ struct gvizCudaForce {
   uint32_t *d_rootNode = nullptr, *d_rootT = nullptr, *d_graphBase = nullptr;
   void *d_nodes = nullptr;  // NodeF or NodeD, maxNodes records
   uint4 *d_kids = nullptr;  // per cell: children's preorder slots (FP32 builds)
+  double2 *d_exactPartial = nullptr;  // exact FP32 mode: [exactSplits][V] split sums
+  uint32_t exactSplits = 1;
   uint32_t *d_leafDepth = nullptr;  // per vertex (inspection only)
 
   // forces-only evaluation (no FA2 history update): structForce goes to
@@ -306,6 +308,7 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters);
 uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads);
 void forces_set_smem_limits();
 void enqueue_exact_f32(gvizCudaForce *h);
+uint32_t exact_splits(size_t V, int sms);
 
 // precise.cu (FP64 + FA2, compiled without fused multiply-add)
 void enqueue_attraction_f64(gvizCudaForce *h);

@@ -559,7 +559,7 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
     if (a.nQ) {
       double px = 0.0, py = 0.0;
       if (M > 1e-9 || M < -1e-9) {
-        const double im = 1.0 / M;
+        const double im = __drcp_rn(M);  // one reciprocal on the serial climb
         px = SX * im;
         py = SY * im;
       }
