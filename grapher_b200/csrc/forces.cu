@@ -12,7 +12,8 @@
 //
 // Geometry is double-single: a coordinate is hi + lo floats, so a difference
 // (ah - bh) + (al - bl) keeps ~FP32 relative accuracy even at |x| ~ 1e3.
-// Per-vertex sums are Kahan-compensated FP32; the epilogue is FP64.
+// Per-vertex sums are Kahan-compensated FP32 (the walks first add the terms of
+// one round, at most 32, in a plain FP32 partial); the epilogue is FP64.
 #include <math.h>
 
 #include <algorithm>
@@ -275,7 +276,7 @@ struct PlainTarget {
 // term of a point or an accepted cell; returns true when the cell is opened.
 template <int MODEL, bool OVERLAP>
 __device__ __forceinline__ bool plain_visit(const WalkArgs &a, const PlainTarget &t, bool in,
-                                            float4 n0, float4 n1, Kahan &kx, Kahan &ky,
+                                            float4 n0, float4 n1, float &px, float &py,
                                             unsigned long long &nInter) {
   const float nmass = n1.x, nsize = n1.y;
   const int32_t ninfo = __float_as_int(n1.w);
@@ -293,15 +294,15 @@ __device__ __forceinline__ bool plain_visit(const WalkArgs &a, const PlainTarget
       float fx, fy;
       rep_term<MODEL, OVERLAP>(dx, dy, d2, t.mv, nmass, t.rv + (isLeaf ? nsize : 0.0f), a.num,
                                a.overlapC, t.v, isLeaf ? (uint32_t)ninfo : t.v, fx, fy);
-      kx.add(fx);
-      ky.add(fy);
+      px += fx;
+      py += fy;
     }
   } else if (doForce) {
     float fx, fy;
     rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, nmass, t.rv + (isLeaf ? nsize : 0.0f),
                                    a.num, a.overlapC, fx, fy);
-    kx.add(fx);
-    ky.add(fy);
+    px += fx;
+    py += fy;
   }
   nInter += doForce ? 1ull : 0ull;
   return in && massOk && !isLeaf && !accept;
@@ -319,15 +320,25 @@ __device__ void plain_walk_range(const WalkArgs &a, const PlainTarget &t, uint32
   const bool mine = (lanes >> lane) & 1u;
   uint32_t resume = mine ? lo : kInf;
   uint32_t cur = __reduce_min_sync(0xffffffffu, resume < hi ? resume : kInf);
+  float px = 0.f, py = 0.f;
+  uint32_t run = 0;
   while (cur != kInf) {
     const float4 n0 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur));
     const float4 n1 = __ldg(reinterpret_cast<const float4 *>(a.nodes + cur) + 1);
     const bool in = mine && cur == resume;
-    const bool open = plain_visit<MODEL, OVERLAP>(a, t, in, n0, n1, kx, ky, nInter);
+    const bool open = plain_visit<MODEL, OVERLAP>(a, t, in, n0, n1, px, py, nInter);
     if (in) resume = open ? cur + 1u : max((uint32_t)__float_as_int(n1.z), cur + 1u);
     nVisit++;
+    if (++run == 32u) {  // the cascade of the round-based walk: 32 terms, then Kahan
+      kx.add(px);
+      ky.add(py);
+      px = py = 0.f;
+      run = 0;
+    }
     cur = __reduce_min_sync(0xffffffffu, resume < hi ? resume : kInf);
   }
+  kx.add(px);
+  ky.add(py);
 }
 
 template <int MODEL, bool OVERLAP, bool COUNT>
@@ -387,14 +398,19 @@ __device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, Plai
     }
     __syncwarp();
     if (COUNT) nVisit += n;
+    // the round's terms in a plain FP32 partial, which then joins the
+    // target's Kahan-compensated sum (cascade summation, <= 32 terms a run)
     uint32_t myOpen = 0;
+    float px = 0.f, py = 0.f;
     for (uint32_t j = 0; j < n; j++) {
       const uint32_t lanes = __shfl_sync(0xffffffffu, e.y, j);
       const bool open = plain_visit<MODEL, OVERLAP>(a, t, (lanes >> lane) & 1u, q.rec[j][0],
-                                                    q.rec[j][1], kx, ky, nInter);
+                                                    q.rec[j][1], px, py, nInter);
       const uint32_t ob = __ballot_sync(0xffffffffu, open);
       if (lane == j) myOpen = ob;
     }
+    kx.add(px);
+    ky.add(py);
     // opened nodes push their children (inside the graph's subtree) with the
     // lanes that opened them, in lane order, while they fit
     uint32_t nk = 0;
@@ -859,7 +875,7 @@ template <int MODEL, bool OVERLAP, bool COUNT>
 __device__ __forceinline__ void cell_eval_points(const WalkArgs &a, CellWarpSmem &q,
                                                  const CellTarget &t, CellSums &s, uint32_t k) {
   __syncwarp();
-#pragma unroll 4
+#pragma unroll 1  // a compact loop: the walk is sensitive to instruction-cache misses
   for (uint32_t j = 0; j < k; j++) {
     const uint32_t e = (s.ph + j) & (kCellRing - 1);
     const float4 p = q.pPos[e];
@@ -924,7 +940,7 @@ __device__ __forceinline__ void cell_eval_cells(const WalkArgs &a, const FarCell
   __syncwarp();
   mlp_forward_tile<true>(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
   __syncwarp();
-#pragma unroll 4
+#pragma unroll 1  // a compact loop: the walk is sensitive to instruction-cache misses
   for (uint32_t r = 0; r < k; r++) {
     const uint32_t e = (s.ch + r) & (kCellRing - 1);
     const float4 p = q.cPos[e];
@@ -1481,13 +1497,29 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
           zero = zero || d2[k] == 0.0f;
         }
         if (fastTile && !__any_sync(0xffffffffu, zero)) {
+          if (OVERLAP) {
 #pragma unroll
-          for (int k = 0; k < kExactTpt; k++) {
-            float fx, fy;
-            rep_term_apart<MODEL, OVERLAP>(dx[k], dy[k], d2[k], mv[k], m.x, rv[k] + m.y, a.num,
-                                           a.overlapC, fx, fy);
-            px[k] += fx;
-            py[k] += fy;
+            for (int k = 0; k < kExactTpt; k++) {
+              float fx, fy;
+              rep_term_apart<MODEL, OVERLAP>(dx[k], dy[k], d2[k], mv[k], m.x, rv[k] + m.y,
+                                             a.num, a.overlapC, fx, fy);
+              px[k] += fx;
+              py[k] += fy;
+            }
+          } else {
+            // without overlap the term is numer / d2 along (dx, dy): the
+            // source's share of the numerator once per source (FR: k^2 times
+            // the truncated mass, src/embedders/gvizForceModel.c:20; LinLog:
+            // its mass), one approximate reciprocal per pair, and the term
+            // fused into the chunk's partial sum
+            const float w = MODEL == GVIZ_CUDA_MODEL_FR ? a.num * truncf(m.x) : m.x;
+#pragma unroll
+            for (int k = 0; k < kExactTpt; k++) {
+              float s = __fdividef(w, d2[k]);
+              if (MODEL != GVIZ_CUDA_MODEL_FR) s *= mv[k];
+              px[k] = fmaf(-s, dx[k], px[k]);
+              py[k] = fmaf(-s, dy[k], py[k]);
+            }
           }
         } else {
           const uint32_t jj = t0 + q;
