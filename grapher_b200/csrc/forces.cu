@@ -1407,11 +1407,11 @@ struct ExactArgs {
 // shared memory serves kExactTpt targets. Per target the terms of each run
 // of kExactChunk sources are added in plain FP32 and that partial joins a
 // Kahan-compensated running sum (cascade summation: the rounding of a
-// V-term sum stays at a chunk's). The pair term runs straight-line; a source
-// that coincides with a target (the target itself, or a duplicate point,
-// d2 == 0) sends the warp through the guarded path for that source, which
-// skips the self pair and applies the coincident direction. Tiles that
-// straddle a graph boundary of a forest take the guarded path too.
+// V-term sum stays at a chunk's). The pair term runs straight-line; a chunk
+// whose sum meets the target itself or a duplicate point (d2 == 0) is summed
+// again on the guarded path, which skips the self pair and applies the
+// coincident direction. Tiles that straddle a graph boundary of a forest,
+// and every tile with overlap prevention, take the guarded path.
 // The sources are split into gridDim.y consecutive ranges of whole tiles
 // (so that small layouts still fill the GPU); with more than one range each
 // block writes its per-target partial sums and k_exact_combine adds them in
@@ -1483,21 +1483,57 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
       float px[kExactTpt], py[kExactTpt];
 #pragma unroll
       for (int k = 0; k < kExactTpt; k++) px[k] = py[k] = 0.f;
+      bool redo = true;
+      if (!OVERLAP && fastTile) {
+        // Optimistic: without overlap the term is numer / d2 along (dx, dy),
+        // with the source's share of the numerator taken once per source
+        // (FR: k^2 times the truncated mass, src/embedders/gvizForceModel.c:20;
+        // LinLog: its mass), one approximate reciprocal per pair, and the
+        // term fused into the chunk's partial. The self pair or a coincident
+        // point (d2 == 0) leaves a partial that is not finite; the chunk is
+        // then summed again on the guarded path below.
 #pragma unroll 4
-      for (uint32_t q = c0; q < c1; q++) {
-        const float4 f = sp[q];
-        const float2 m = sm[q];
-        float dx[kExactTpt], dy[kExactTpt], d2[kExactTpt];
-        bool zero = false;
+        for (uint32_t q = c0; q < c1; q++) {
+          const float4 f = sp[q];
+          const float w = MODEL == GVIZ_CUDA_MODEL_FR ? a.num * truncf(sm[q].x) : sm[q].x;
 #pragma unroll
-        for (int k = 0; k < kExactTpt; k++) {
-          dx[k] = (f.x - vxh[k]) + (f.z - vxl[k]);
-          dy[k] = (f.y - vyh[k]) + (f.w - vyl[k]);
-          d2[k] = dx[k] * dx[k] + dy[k] * dy[k];
-          zero = zero || d2[k] == 0.0f;
+          for (int k = 0; k < kExactTpt; k++) {
+            const float dx = (f.x - vxh[k]) + (f.z - vxl[k]);
+            const float dy = (f.y - vyh[k]) + (f.w - vyl[k]);
+            float sc = __fdividef(w, dx * dx + dy * dy);
+            if (MODEL != GVIZ_CUDA_MODEL_FR) sc *= mv[k];
+            px[k] = fmaf(-sc, dx, px[k]);
+            py[k] = fmaf(-sc, dy, py[k]);
+          }
         }
-        if (fastTile && !__any_sync(0xffffffffu, zero)) {
-          if (OVERLAP) {
+        bool bad = false;
+#pragma unroll
+        for (int k = 0; k < kExactTpt; k++)
+          bad = bad || (act[k] && !(isfinite(px[k]) && isfinite(py[k])));
+        redo = __any_sync(0xffffffffu, bad);
+        if (redo) {
+#pragma unroll
+          for (int k = 0; k < kExactTpt; k++) px[k] = py[k] = 0.f;
+        }
+      }
+      if (redo) {
+        // guarded: the graph ranges of a forest, the self pair skipped, a
+        // coincident point through the deterministic direction; with
+        // overlap the term of include/core/gvizVec.h:404-428 / 552-578
+        for (uint32_t q = c0; q < c1; q++) {
+          const float4 f = sp[q];
+          const float2 m = sm[q];
+          const uint32_t jj = t0 + q;
+          float dx[kExactTpt], dy[kExactTpt], d2[kExactTpt];
+          bool zero = false;
+#pragma unroll
+          for (int k = 0; k < kExactTpt; k++) {
+            dx[k] = (f.x - vxh[k]) + (f.z - vxl[k]);
+            dy[k] = (f.y - vyh[k]) + (f.w - vyl[k]);
+            d2[k] = dx[k] * dx[k] + dy[k] * dy[k];
+            zero = zero || (act[k] && d2[k] == 0.0f);
+          }
+          if (fastTile && !__any_sync(0xffffffffu, zero)) {
 #pragma unroll
             for (int k = 0; k < kExactTpt; k++) {
               float fx, fy;
@@ -1507,30 +1543,15 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
               py[k] += fy;
             }
           } else {
-            // without overlap the term is numer / d2 along (dx, dy): the
-            // source's share of the numerator once per source (FR: k^2 times
-            // the truncated mass, src/embedders/gvizForceModel.c:20; LinLog:
-            // its mass), one approximate reciprocal per pair, and the term
-            // fused into the chunk's partial sum
-            const float w = MODEL == GVIZ_CUDA_MODEL_FR ? a.num * truncf(m.x) : m.x;
 #pragma unroll
             for (int k = 0; k < kExactTpt; k++) {
-              float s = __fdividef(w, d2[k]);
-              if (MODEL != GVIZ_CUDA_MODEL_FR) s *= mv[k];
-              px[k] = fmaf(-s, dx[k], px[k]);
-              py[k] = fmaf(-s, dy[k], py[k]);
+              if (!act[k] || jj == v[k] || jj < gb[k] || jj >= ge[k]) continue;
+              float fx, fy;
+              rep_term<MODEL, OVERLAP>(dx[k], dy[k], d2[k], mv[k], m.x, rv[k] + m.y, a.num,
+                                       a.overlapC, v[k], jj, fx, fy);
+              px[k] += fx;
+              py[k] += fy;
             }
-          }
-        } else {
-          const uint32_t jj = t0 + q;
-#pragma unroll
-          for (int k = 0; k < kExactTpt; k++) {
-            if (!act[k] || jj == v[k] || jj < gb[k] || jj >= ge[k]) continue;
-            float fx, fy;
-            rep_term<MODEL, OVERLAP>(dx[k], dy[k], d2[k], mv[k], m.x, rv[k] + m.y, a.num,
-                                     a.overlapC, v[k], jj, fx, fy);
-            px[k] += fx;
-            py[k] += fy;
           }
         }
       }

@@ -348,7 +348,7 @@ __global__ __launch_bounds__(32) void k_mlp_grad(const float *__restrict__ w,
 // Every gradient entry is written by exactly one thread of the CTA.
 // ---------------------------------------------------------------------------
 constexpr int kTcThreads = 128;
-constexpr int kTcTilesPerBlock = 2;
+constexpr int kTcTilesPerBlock = 1;
 constexpr uint32_t kTcCols = 256;  // TMEM columns allocated (power of two >= 176)
 constexpr uint32_t kTcColGrad = 64, kTcColW3 = 160;
 constexpr uint32_t kTcSpin = 1u << 22;  // mbarrier polls before giving up
