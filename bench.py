@@ -446,9 +446,9 @@ HUB_THETA = 0.35         # their plain walk's opening threshold
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
 # The learned comparison starts from a fixed point of the layout, whatever
 # --warmup asks for: LEARNED_PRE_STEPS plain steps from the initial
-# positions, then the harvest snapshots of HARVEST_SCHEDULE; the judged and
-# timed state is the one of the last snapshot. --warmup steps run before each
-# timed region, from that saved state.
+# positions, then the harvest snapshots of HARVEST_SCHEDULE, all in the FP64
+# path; the judged and timed state is the one of the last snapshot. --warmup
+# steps run before each timed region, from that saved state.
 LEARNED_PRE_STEPS = 20
 # (steps before the snapshot, opening threshold of its pairs): earlier
 # states at smaller thresholds, and the state the learned walk then runs
@@ -485,6 +485,18 @@ def learned_params(linfo):
                 farHubTheta=HUB_THETA)
 
 
+def setup_steps(lay, n):
+    """n untimed steps of the learned setup in the FP64 path (the reference's
+    arithmetic), so that the state the comparison judges and times does not
+    move with the FP32 kernels' rounding; the FP32 path is restored after."""
+    if n <= 0:
+        return
+    lay.set_params(precision=1)
+    for _ in range(n):
+        lay.step()
+    lay.set_params(precision=0)
+
+
 def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     """Trains the far-field MLP on this layout's own harvested pairs, judges
     plain theta = 0.5 and the learned walk, without and with hub targets,
@@ -497,8 +509,7 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
     t0 = time.perf_counter()
     Xs, Ts, Ws = [], [], []
     for snap, (gap, th) in enumerate(HARVEST_SCHEDULE):  # cells of every angular size
-        for _ in range(gap):
-            lay.step()
+        setup_steps(lay, gap)
         t = np.sort(rng.choice(w.V, HARVEST_TARGETS, replace=False)).astype(np.uint32)
         X, T, Wt = harvest_training_set(lay, th, t)
         Xs.append(X), Ts.append(T), Ws.append(Wt)
@@ -892,8 +903,11 @@ def main():
     lay = ForceLayout(w.row, w.col, model=w.spec["model"], graph_offsets=w.goff, device=local)
     w.configure(lay)
     lay.begin(0, positions=w.x0)
-    for _ in range(LEARNED_PRE_STEPS if learned else args.warmup):
-        lay.step()
+    if learned:
+        setup_steps(lay, LEARNED_PRE_STEPS)
+    else:
+        for _ in range(args.warmup):
+            lay.step()
     # the walk's launch shape for this layout (block size, static or
     # persistent schedule), timed on the warmed-up positions
     shape = lay.autotune() if w.spec["bh"] else None
