@@ -932,9 +932,15 @@ def main():
         with nvtx_range("plain_steps"):
             pms = max_over_ranks(lay.time_steps(args.steps))
         pprof = lay.profile_step()
+        p_inter, p_visits = lay.count_interactions()
+        p_walk = dict(pprof).get("bh_walk_f32")
+        fp32_peak = 148 * 128 * 2 * load_peaks()[0].get("sm_max_mhz", 1965.0) * 1e6 / 1e12
         plain_line = {"theta": w.spec["theta"], "value": world * args.steps / (pms / 1e3),
                       "ms_per_step": pms / args.steps, "rms_err": linfo["plain_rms_err"],
-                      "kernel_ms": {k: round(v, 4) for k, v in pprof}}
+                      "kernel_ms": {k: round(v, 4) for k, v in pprof},
+                      "interactions": p_inter, "warp_node_visits": p_visits,
+                      "walk_fp32_frac": (FLOP_PER_INTERACTION * p_inter / (p_walk * 1e-3) / 1e12
+                                         / fp32_peak) if p_walk else None}
         # then the learned walk from the same state
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
