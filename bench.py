@@ -7,10 +7,12 @@
 Default workload (the headline metric: learned vs plain Barnes-Hut at equal
 force error): Barabasi-Albert graph, n = 1,048,576, m = 4 (4,194,294 edges,
 seeded), LinLog with gravity 1.0, start uniform in [-1000, 1000]^2 (rand_r,
-seed 7). After the warm-up steps (plain, theta = 0.5) the far-field MLP is
-trained on the GPU (40 epochs) from pairs harvested for 32,768 sampled
-vertices at theta = 1.2, 0.9 and 0.6 on three snapshots of this layout
-(untimed setup, reported as train_s). Force error is the
+seed 7). Setup (untimed, in the FP64 path so that the judged state does not
+depend on FP32 rounding): 20 plain steps at theta = 0.5, then four snapshots
+of this layout (iterations 20, 25, 30, 30) from which pairs are harvested for
+32,768 sampled vertices each at theta = 0.7, 0.95, 1.2 and 1.05; the
+far-field MLP is trained on them on the GPU (40 epochs, reported as
+train_s), and the state of iteration 30 is judged and timed. Force error is the
 normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
 every vertex (on 65,536 sampled vertices for layouts above 2^20 vertices),
 all configurations judged on the same positions; the error tables also carry
@@ -261,6 +263,28 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# DRAM bytes per launch of the dominant kernels (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum, one capture each), reported as roofline.traffic on the
+# workload the capture ran: kernel -> (workload, bytes, capture)
+NCU_TRAFFIC = {
+    "bh_walk_f32_learned": ("ba1m_learned", 681.7e6 + 186.6e6,
+                            "profiles/learned_walk_ba1m.md (theta 1.25, 4096 hub targets)"),
+    "bh_walk_f32": ("ba1m_learned", 636.1e6 + 172.9e6,
+                    "profiles/plain_walk_ba1m.md (theta 0.5)"),
+    "exact_f32": ("er65k_exact", 1.358e6 + 0.0, "profiles/exact_er65k.md"),
+    "k_grip_pass1": ("grip_ba200k", 121.1e6 + 8.4e6, "profiles/grip_round_ba200k.md"),
+}
+
+
+def ncu_traffic(kernel, workload):
+    """(bytes per launch, capture) from NCU_TRAFFIC when the capture ran this
+    workload, else (None, None)."""
+    t = NCU_TRAFFIC.get(kernel)
+    if t is None or t[0] != workload:
+        return None, None
+    return t[1], t[2]
 
 
 def load_peaks():
@@ -845,7 +869,9 @@ def grip_bench(args):
         "gpu_launches": 5 * args.steps, "kernels_per_step": 5,
         "roofline": {"kernel": "k_grip_pass1", "bound": "hbm", "achieved": achieved,
                      "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "frac": achieved / peaks["hbm_gbs"],
+                     "traffic": ncu_traffic("k_grip_pass1", "grip_ba200k")[0],
+                     "traffic_source": ncu_traffic("k_grip_pass1", "grip_ba200k")[1],
                      "peak_source": f"hbm_gbs ({src})",
                      "algorithmic": (f"{bytes_launch} B per launch: {GRIP_V} vertices x "
                                      f"{per_vertex} B + {K} nearest x 24 B + {E2} edge "
@@ -940,7 +966,8 @@ def main():
                       "kernel_ms": {k: round(v, 4) for k, v in pprof},
                       "interactions": p_inter, "warp_node_visits": p_visits,
                       "walk_fp32_frac": (FLOP_PER_INTERACTION * p_inter / (p_walk * 1e-3) / 1e12
-                                         / fp32_peak) if p_walk else None}
+                                         / fp32_peak) if p_walk else None,
+                      "walk_traffic": ncu_traffic("bh_walk_f32", args.workload)[0]}
         # then the learned walk from the same state
         lay.set_positions(x_s)
         lay.set_fa2_state(sf_s, sp_s, ef_s)
@@ -988,8 +1015,10 @@ def main():
     flops = FLOP_PER_INTERACTION * inter
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     achieved = flops / (walk_ms * 1e-3) / 1e12
+    traffic, traffic_src = ncu_traffic(kname, args.workload)
     roofline = {"kernel": kname, "bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+                "traffic_source": traffic_src,
                 "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 FLOP) at the "
                                "MEASURED_PEAKS.json max SM clock (no measured FP32 figure)",
                 "algorithmic": f"{FLOP_PER_INTERACTION} FLOP x {inter} interactions per launch",
@@ -1001,7 +1030,8 @@ def main():
         tc = mlp_flop / (walk_ms * 1e-3) / 1e12
         roofline = {"kernel": kname, "bound": "tensor", "achieved": tc,
                     "peak": peaks.get("bf16_tflops", 1590.0), "unit": "TFLOP/s",
-                    "frac": tc / peaks.get("bf16_tflops", 1590.0), "traffic": None,
+                    "frac": tc / peaks.get("bf16_tflops", 1590.0), "traffic": traffic,
+                    "traffic_source": traffic_src,
                     "peak_source": f"bf16_tflops ({peak_src})",
                     "algorithmic": (f"{MLP_FLOP_PER_ROW} FLOP (10-64-64-2 MLP) x {rows} rows "
                                     f"({g_rows} shared, {l_rows} per target) per launch"),
