@@ -2,13 +2,19 @@
 //
 //  * k_attr_f32: edge attraction over CSR (src/embedders/gvizForceEmbedder.c:93-100;
 //    FR include/core/gvizVec.h:320-334, LinLog :486-499).
-//  * k_walk_f32: Barnes-Hut repulsion (src/embedders/gvizForceEmbedder.c:35-74)
-//    as a warp-shared stackless traversal of the preorder tree: the 32 lanes
-//    of a warp hold 32 path-sorted (hence nearby) vertices and step through
-//    the union of the nodes they need, every lane making the reference's own
-//    accept / open / pairwise decision. Node records are read once per warp
-//    (one broadcast), the next node is the warp minimum of each lane's next.
-//  * k_exact_f32: exact all-pairs repulsion (:104-115), shared-memory tiles.
+//  * k_walk_f32 / k_walk_f32_queue: Barnes-Hut repulsion
+//    (src/embedders/gvizForceEmbedder.c:35-74). The 32 lanes of a warp hold 32
+//    path-sorted (hence nearby) vertices; the warp expands the union of the
+//    nodes they need 32 at a time from a stack of (node, lanes) entries in
+//    shared memory, every lane making the reference's own accept / open /
+//    pairwise decision for its vertex. An opened cell whose children do not
+//    fit the stack is walked in place by the stackless preorder walk.
+//  * k_walk_f32_cells / k_walk_f32_far: walks with the learned far-field
+//    correction; the first expands the tree the same way with group-wide
+//    decisions for tree-cut target groups, the second steps through the
+//    warp's union stacklessly with per-target decisions.
+//  * k_exact_f32: exact all-pairs repulsion (:104-115), shared-memory tiles,
+//    sources split over blockIdx.y (k_exact_combine adds the partials).
 //
 // Geometry is double-single: a coordinate is hi + lo floats, so a difference
 // (ah - bh) + (al - bl) keeps ~FP32 relative accuracy even at |x| ~ 1e3.
@@ -32,6 +38,15 @@ namespace {
 constexpr int kWalkThreads = 128;     // default block size of the walk
 constexpr int kWalkMaxThreads = 512;  // largest block size the autotuner tries
 constexpr int kAttrThreads = 256;
+
+// 1 / x by the PTX approximate reciprocal (subnormal input and output
+// flushed to zero); only the exact kernel's optimistic pass uses it.
+__device__ __forceinline__ float rcp_approx_ftz(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 constexpr int kExactThreads = 128;
 constexpr int kExactTile = 128;
 constexpr int kExactTpt = 4;     // exact mode: targets per thread
@@ -1489,9 +1504,12 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
         // with the source's share of the numerator taken once per source
         // (FR: k^2 times the truncated mass, src/embedders/gvizForceModel.c:20;
         // LinLog: its mass), one approximate reciprocal per pair, and the
-        // term fused into the chunk's partial. The self pair or a coincident
-        // point (d2 == 0) leaves a partial that is not finite; the chunk is
-        // then summed again on the guarded path below.
+        // term fused into the chunk's partial. The reciprocal is the PTX
+        // instruction rcp.approx.ftz.f32 (one MUFU op, no range handling):
+        // the self pair, a coincident point (d2 == 0) or a d2 below the
+        // normal range (flushed to zero) gives an infinite term, so the
+        // chunk's partial is not finite and the chunk is summed again on
+        // the guarded path below.
 #pragma unroll 4
         for (uint32_t q = c0; q < c1; q++) {
           const float4 f = sp[q];
@@ -1500,7 +1518,7 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
           for (int k = 0; k < kExactTpt; k++) {
             const float dx = (f.x - vxh[k]) + (f.z - vxl[k]);
             const float dy = (f.y - vyh[k]) + (f.w - vyl[k]);
-            float sc = __fdividef(w, dx * dx + dy * dy);
+            float sc = w * rcp_approx_ftz(dx * dx + dy * dy);
             if (MODEL != GVIZ_CUDA_MODEL_FR) sc *= mv[k];
             px[k] = fmaf(-sc, dx, px[k]);
             py[k] = fmaf(-sc, dy, py[k]);
