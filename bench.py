@@ -1052,6 +1052,7 @@ def main():
     }
     if shape:
         line["walk_shape"] = {"threads": shape[0], "persistent": shape[1],
+                              "stack_entries": lay.walk_shape()[2],
                               "autotune_walk_ms": round(shape[2], 4)}
     if learned and args.workload == "rmat4m_learned":
         # the error along the run, every 20 iterations, for both paths from

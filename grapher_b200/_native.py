@@ -174,6 +174,7 @@ _SIGS = {
     "gvizCudaEdgesToCsr": (C.c_int, [SZ, U32P, U32P, SZ, U64P, U32P]),
     "gvizCudaForceAutotune": (C.c_int, [P, U32P, I32P, C.POINTER(C.c_float)]),
     "gvizCudaForceSetWalkShape": (C.c_int, [P, C.c_uint32, C.c_int32]),
+    "gvizCudaForceGetWalkShape": (C.c_int, [P, U32P, I32P, U32P]),
     "gvizCudaForceSetWalkStackCap": (C.c_int, [P, C.c_uint32]),
     "gvizCudaForceSetFarJudge": (C.c_int, [P, C.c_uint32, C.c_uint32, D, D, C.c_uint64]),
     "gvizCudaForceJudgeFarField": (C.c_int, [P, DP, DP, I32P]),

@@ -1619,9 +1619,16 @@ int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threadsOut, int32_t *persi
   float best = INFINITY;
   uint32_t bestThreads = kWalkDefaultThreads;
   bool bestPersistent = false;
-  uint32_t bestResident = 0;
+  uint32_t bestResident = 0, bestCap = 0;
+  // stack entries per warp: a smaller stack takes less shared memory, so
+  // more warps are resident, and walks more subtrees in place; a cap set by
+  // the caller is kept
+  static const uint32_t kCaps[] = {128, 256, 512};
+  const int nCaps = h->walkStackCap ? 1 : 3;
+  for (int ci = 0; ci < nCaps; ci++)
   for (int persistent = 0; persistent < 2; persistent++) {
     for (uint32_t t : kCandidates) {
+      h->walkTunedCap = h->walkStackCap ? 0u : kCaps[ci];
       h->walkThreads = t;
       h->walkPersistent = persistent != 0;
       h->walkResident = persistent ? walk_resident_blocks(h, t) : 0;
@@ -1641,6 +1648,7 @@ int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threadsOut, int32_t *persi
         bestThreads = t;
         bestPersistent = persistent != 0;
         bestResident = h->walkResident;
+        bestCap = h->walkTunedCap;
       }
     }
   }
@@ -1651,6 +1659,7 @@ int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threadsOut, int32_t *persi
   h->walkThreads = bestThreads;
   h->walkPersistent = bestPersistent;
   h->walkResident = bestResident;
+  h->walkTunedCap = bestCap;
   h->graphDirty = true;
   const int rc = sync_and_check(h);
   if (threadsOut) *threadsOut = bestThreads;
@@ -1701,7 +1710,15 @@ int gvizCudaForceFarJudgeStatus(const gvizCudaForce *h, uint64_t *checks, double
 
 int gvizCudaForceSetWalkStackCap(gvizCudaForce *h, uint32_t entries) {
   if (!h || (entries != 0 && (entries < 32 || entries > 512))) return GVIZ_CUDA_ERR_ARG;
+  DeviceGuard guard(h->device);
   h->walkStackCap = entries;
+  // the persistent grid of the plain walk follows its shared memory
+  if (h->walkPersistent) {
+    const uint32_t resident = walk_resident_blocks(h, h->walkThreads ? h->walkThreads
+                                                                      : kWalkDefaultThreads);
+    if (!resident) return set_err(h, GVIZ_CUDA_ERR_CUDA);
+    h->walkResident = resident;
+  }
   h->graphDirty = true;
   return GVIZ_CUDA_OK;
 }
@@ -1715,6 +1732,15 @@ int gvizCudaForceSetWalkShape(gvizCudaForce *h, uint32_t threads, int32_t persis
   h->walkPersistent = persistent != 0;
   h->walkResident = resident;
   h->graphDirty = true;
+  return GVIZ_CUDA_OK;
+}
+
+int gvizCudaForceGetWalkShape(const gvizCudaForce *h, uint32_t *threads, int32_t *persistent,
+                              uint32_t *stackEntries) {
+  if (!h) return GVIZ_CUDA_ERR_ARG;
+  if (threads) *threads = h->walkThreads ? h->walkThreads : kWalkDefaultThreads;
+  if (persistent) *persistent = (h->walkPersistent && h->walkResident) ? 1 : 0;
+  if (stackEntries) *stackEntries = plain_cap(h);
   return GVIZ_CUDA_OK;
 }
 

@@ -274,12 +274,28 @@ __device__ __forceinline__ void rep_term_apart(float dx, float dy, float d2, flo
 // pushes its children (slots from the tree build's child records) with the
 // lanes that opened it. A push that would overflow the stack is walked in
 // place with the stackless union walk below (the same decisions).
-constexpr int kPlainStack = 512;  // pending (node, lanes) entries per warp
+constexpr int kPlainStack = 512;  // largest stack: pending (node, lanes) entries per warp
 
-struct __align__(16) PlainWarpSmem {
-  float4 rec[32][2];      // the round's node records
-  uint2 st[kPlainStack];  // pending entries: node, lanes
+// A warp's region of the plain walk's dynamic shared memory: the round's 32
+// node records (1 KiB), then a stack of stackCap entries; the region's
+// size follows the stack cap, so a smaller stack leaves room for more
+// resident warps.
+struct PlainWarpSmem {
+  float4 (*rec)[2];  // the round's node records
+  uint2 *st;         // pending entries: node, lanes
 };
+
+__host__ __device__ constexpr uint32_t plain_warp_bytes(uint32_t cap) {
+  return 32u * 2u * 16u + ((cap * 8u + 15u) & ~15u);
+}
+
+__device__ __forceinline__ PlainWarpSmem plain_warp_smem(unsigned char *dyn, uint32_t cap) {
+  unsigned char *base = dyn + (size_t)(threadIdx.x >> 5) * plain_warp_bytes(cap);
+  PlainWarpSmem q;
+  q.rec = reinterpret_cast<float4(*)[2]>(base);
+  q.st = reinterpret_cast<uint2 *>(base + 32 * 2 * 16);
+  return q;
+}
 
 struct PlainTarget {
   uint32_t v;
@@ -357,7 +373,7 @@ __device__ void plain_walk_range(const WalkArgs &a, const PlainTarget &t, uint32
 }
 
 template <int MODEL, bool OVERLAP, bool COUNT>
-__device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, PlainWarpSmem &q) {
+__device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, const PlainWarpSmem &q) {
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t below = (1u << lane) - 1u;
   // a task's targets all belong to one graph (tasks are cut per graph): the
@@ -432,7 +448,7 @@ __device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, Plai
     if (myOpen) {
       if (kd.y == GVIZ_KIDS_RUN) {
         nk = (kd.x > e.x && kd.x < entryEnd) ? min(kd.z, entryEnd - kd.x) : 0u;
-        nk = min(nk, (uint32_t)kPlainStack + 1u);  // a longer run never fits
+        nk = min(nk, a.stackCap + 1u);  // a longer run never fits
       } else {
         kd.x = (kd.x > e.x && kd.x < entryEnd) ? kd.x : GVIZ_NONE;
         kd.y = (kd.y > e.x && kd.y < entryEnd) ? kd.y : GVIZ_NONE;
@@ -492,7 +508,7 @@ __device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, Plai
 template <int MODEL, bool OVERLAP, bool COUNT>
 __global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char plainDyn[];
-  PlainWarpSmem &q = reinterpret_cast<PlainWarpSmem *>(plainDyn)[threadIdx.x >> 5];
+  const PlainWarpSmem q = plain_warp_smem(plainDyn, a.stackCap);
   const uint32_t task = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (task >= a.nTasks) return;  // the whole warp
   walk_task<MODEL, OVERLAP, COUNT>(a, task, q);
@@ -504,7 +520,7 @@ __global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32(WalkArgs a) {
 template <int MODEL, bool OVERLAP, bool COUNT>
 __global__ __launch_bounds__(kWalkMaxThreads) void k_walk_f32_queue(WalkArgs a) {
   extern __shared__ __align__(16) unsigned char plainDyn[];
-  PlainWarpSmem &q = reinterpret_cast<PlainWarpSmem *>(plainDyn)[threadIdx.x >> 5];
+  const PlainWarpSmem q = plain_warp_smem(plainDyn, a.stackCap);
   for (;;) {
     uint32_t t = 0;
     if ((threadIdx.x & 31u) == 0u) t = atomicAdd(a.queue, 1u);
@@ -1661,8 +1677,17 @@ void enqueue_attraction_f32(gvizCudaForce *h) {
   prof_mark(h, "attraction_f32");
 }
 
-// dynamic shared memory of the plain walk: one PlainWarpSmem per warp
-static size_t plain_smem(uint32_t threads) { return (threads / 32) * sizeof(PlainWarpSmem); }
+// the plain walk's stack entries per warp on this handle: the caller's cap
+// (gvizCudaForceSetWalkStackCap), else the autotuner's pick, else all 512
+uint32_t plain_cap(const gvizCudaForce *h) {
+  const uint32_t c = h->walkStackCap ? h->walkStackCap : h->walkTunedCap;
+  return (c >= 32 && c <= (uint32_t)kPlainStack) ? c : (uint32_t)kPlainStack;
+}
+
+// dynamic shared memory of the plain walk: one warp region per warp
+static size_t plain_smem(uint32_t threads, uint32_t cap) {
+  return (size_t)(threads / 32) * plain_warp_bytes(cap);
+}
 
 template <int MODEL, bool OVERLAP, bool COUNT>
 static void launch_walk(gvizCudaForce *h, const WalkArgs &a) {
@@ -1673,11 +1698,12 @@ static void launch_walk(gvizCudaForce *h, const WalkArgs &a) {
     cudaMemsetAsync(a.queue, 0, sizeof(uint32_t), h->stream);
     const uint32_t need = blocks((size_t)warps * 32, threads);
     const uint32_t grid = need < h->walkResident ? need : h->walkResident;
-    k_walk_f32_queue<MODEL, OVERLAP, COUNT><<<grid, threads, plain_smem(threads), h->stream>>>(a);
+    k_walk_f32_queue<MODEL, OVERLAP, COUNT><<<grid, threads, plain_smem(threads, a.stackCap),
+                                              h->stream>>>(a);
     return;
   }
   k_walk_f32<MODEL, OVERLAP, COUNT><<<blocks((size_t)warps * 32, threads), threads,
-                                      plain_smem(threads), h->stream>>>(a);
+                                      plain_smem(threads, a.stackCap), h->stream>>>(a);
 }
 
 template <int MODEL, bool OVERLAP>
@@ -1713,9 +1739,9 @@ static void launch_cells(gvizCudaForce *h, const CellArgs &ca, bool count) {
 template <int MODEL, bool OVERLAP, bool COUNT>
 static void plain_smem_limits() {
   cudaFuncSetAttribute(k_walk_f32<MODEL, OVERLAP, COUNT>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plain_smem(kWalkMaxThreads));
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plain_smem(kWalkMaxThreads, kPlainStack));
   cudaFuncSetAttribute(k_walk_f32_queue<MODEL, OVERLAP, COUNT>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plain_smem(kWalkMaxThreads));
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plain_smem(kWalkMaxThreads, kPlainStack));
 }
 
 void forces_set_smem_limits() {
@@ -1832,6 +1858,7 @@ static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *coun
 // walk of this handle's model and overlap setting.
 uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads) {
   int dev = 0, sms = 0, per = 0;
+  const size_t smem = plain_smem(threads, plain_cap(h));
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const bool ov = h->params.preventOverlap != 0;
@@ -1839,14 +1866,14 @@ uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads) {
   cudaError_t e;
   if (fr) {
     e = ov ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, true, false>, threads, plain_smem(threads))
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, true, false>, threads, smem)
            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, false, false>, threads, plain_smem(threads));
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_FR, false, false>, threads, smem);
   } else {
     e = ov ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, true, false>, threads, plain_smem(threads))
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, true, false>, threads, smem)
            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, false, false>, threads, plain_smem(threads));
+                 &per, k_walk_f32_queue<GVIZ_CUDA_MODEL_LINLOG, false, false>, threads, smem);
   }
   if (e != cudaSuccess || per <= 0 || sms <= 0) return 0;
   return (uint32_t)(per * sms);
@@ -1874,8 +1901,7 @@ void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters) {
   a.kids = h->d_kids;
   a.tasks = h->d_walkTasks;
   a.nTasks = h->nWalkTasks;
-  a.stackCap = (h->walkStackCap >= 32 && h->walkStackCap <= (uint32_t)kPlainStack)
-                   ? h->walkStackCap : (uint32_t)kPlainStack;
+  a.stackCap = plain_cap(h);
   const bool ov = h->params.preventOverlap != 0;
   const bool fr = h->model == GVIZ_CUDA_MODEL_FR;
   if (h->params.farField && h->d_mlp) {

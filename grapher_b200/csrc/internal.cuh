@@ -149,6 +149,7 @@ struct gvizCudaForce {
   bool walkPersistent = false;
   uint32_t walkResident = 0;
   uint32_t walkStackCap = 0;  // FP32 walks: stack entries per warp (0: all)
+  uint32_t walkTunedCap = 0;  // plain walk: the autotuner's stack entries (0: all)
   ChunkStat *d_chunkStat = nullptr;
   uint32_t *d_status = nullptr;
 
@@ -306,6 +307,7 @@ int dir_table_upload_precise(const double *t);
 void enqueue_attraction_f32(gvizCudaForce *h);
 void enqueue_walk_f32(gvizCudaForce *h, uint64_t *counters);
 uint32_t walk_resident_blocks(gvizCudaForce *h, uint32_t threads);
+uint32_t plain_cap(const gvizCudaForce *h);
 void forces_set_smem_limits();
 void enqueue_exact_f32(gvizCudaForce *h);
 uint32_t exact_splits(size_t V, int sms);

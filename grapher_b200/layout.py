@@ -322,14 +322,22 @@ class ForceLayout:
 
     def set_walk_stack_cap(self, entries):
         """Stack entries per warp of the FP32 walks, plain and learned
-        (32..512; 0 restores 512): a tuning and test knob, forces agree up
-        to the order of the per-target sums."""
+        (32..512; 0 restores the default: the autotuner's pick for the plain
+        walk, else 512): forces agree up to the order of the per-target sums."""
         N.check(self.L.gvizCudaForceSetWalkStackCap(self.h, entries),
                 "gvizCudaForceSetWalkStackCap")
 
     def set_walk_shape(self, threads, persistent):
         N.check(self.L.gvizCudaForceSetWalkShape(self.h, threads, int(persistent)),
                 "gvizCudaForceSetWalkShape")
+
+    def walk_shape(self):
+        """The plain FP32 walk's shape in use: (threads per block, persistent,
+        stack entries per warp)."""
+        t, p, c = C.c_uint32(), C.c_int32(), C.c_uint32()
+        N.check(self.L.gvizCudaForceGetWalkShape(self.h, C.byref(t), C.byref(p), C.byref(c)),
+                "gvizCudaForceGetWalkShape")
+        return int(t.value), bool(p.value), int(c.value)
 
     # ------------------------------------------------------------ checkpoints
     def save_checkpoint(self, filename, name=""):

@@ -423,18 +423,28 @@ int gvizCudaFa2SpeedUpdateNoAlloc(const double *d_structForce,
                                   double *d_speedState, void *stream);
 
 /* Picks the FP32 walk's launch shape for this layout by timing it on the
- * current positions: blocks of 64 to 512 threads, and a static grid (warp w
+ * current positions: blocks of 64 to 512 threads, a static grid (warp w
  * takes the 32 path-sorted targets of task w) or a persistent one (a grid
  * that fills the GPU once; each warp takes tasks from a device counter until
- * none are left). Forces do not depend on the choice. Keeps the fastest for
- * later steps; reports it (each output may be NULL). Does nothing for FP64,
- * exact or learned walks. No reference counterpart. */
+ * none are left), and, unless the caller set one with
+ * gvizCudaForceSetWalkStackCap, the stack entries per warp (128, 256 or 512:
+ * a smaller stack takes less shared memory, so more warps are resident).
+ * Forces do not depend on block size or schedule; a smaller stack that makes
+ * a subtree be walked in place changes the order of that target's sums.
+ * Keeps the fastest for later steps; reports it (each output may be NULL;
+ * gvizCudaForceGetWalkShape reports the stack). Does nothing for FP64, exact
+ * or learned walks. No reference counterpart. */
 int gvizCudaForceAutotune(gvizCudaForce *h, uint32_t *threads,
                           int32_t *persistent, float *walkMs);
 
 /* Sets the FP32 walk's launch shape directly: threads per block (a multiple
  * of 32, at most 512) and the persistent schedule (1) or the static one. */
 int gvizCudaForceSetWalkShape(gvizCudaForce *h, uint32_t threads, int32_t persistent);
+
+/* The plain FP32 walk's launch shape in use: threads per block, persistent
+ * schedule (1) or static, and stack entries per warp. Outputs may be NULL. */
+int gvizCudaForceGetWalkShape(const gvizCudaForce *h, uint32_t *threads, int32_t *persistent,
+                              uint32_t *stackEntries);
 
 /* The judge of the learned walk (no reference counterpart): the plain
  * Barnes-Hut walk stays both the learned walk's fallback and the judge of
@@ -467,7 +477,8 @@ int gvizCudaForceFarJudgeStatus(const gvizCudaForce *h, uint64_t *checks, double
  * 32 nodes at a time through a per-warp stack of pending nodes in shared
  * memory (512 entries); an opened cell whose children do not fit is walked
  * in place with the stackless preorder walk instead (the same decisions).
- * Sets the stack entries the walks may use, 32 to 512 (0 restores 512);
+ * Sets the stack entries the walks may use, 32 to 512 (0 restores the
+ * default: the autotuner's pick for the plain walk, else 512);
  * forces agree up to the order of the per-target sums. A tuning and test
  * knob. No reference counterpart. */
 int gvizCudaForceSetWalkStackCap(gvizCudaForce *h, uint32_t entries);

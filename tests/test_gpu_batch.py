@@ -102,6 +102,13 @@ def test_walk_shapes_and_autotune_give_identical_forces():
     lay.begin(0, positions=x0)
     threads, persistent, ms = lay.autotune()
     assert threads in (64, 128, 256, 512) and ms > 0
-    assert np.array_equal(lay.repulsion(), want)
+    t2, p2, cap = lay.walk_shape()
+    assert (t2, p2) == (threads, persistent) and cap in (128, 256, 512)
+    # the tuned stack: the same forces as the default shape with that stack
+    chk = make_layout(row, col, c, graph_offsets=offs)
+    chk.begin(0, positions=x0)
+    chk.set_walk_stack_cap(cap)
+    assert np.array_equal(lay.repulsion(), chk.repulsion())
+    chk.close()
     with pytest.raises(GvizCudaError):
         lay.set_walk_shape(100, False)

@@ -263,6 +263,11 @@ def test_plain_walk_in_place_subtrees_agree(kw):
     lay.set_walk_stack_cap(32)
     small = lay.repulsion()
     n_small = lay.count_interactions()[0]
+    # the warp regions of shared memory follow the stack: a persistent grid
+    # sized for the small stack computes the same as the static one
+    lay.set_walk_shape(256, True)
+    assert lay.walk_shape() == (256, True, 32)
+    assert np.array_equal(lay.repulsion(), small)
     lay.close()
     assert n_small == n_full
     d = np.linalg.norm(small - full, axis=1)
