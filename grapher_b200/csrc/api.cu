@@ -136,8 +136,8 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_runStart);
   dfree(h->d_deepRuns);
   dfree(h->d_counts);
-  dfree(h->d_radixHist);
-  dfree(h->d_scanTile);
+  dfree(h->d_sortState);
+  dfree(h->d_scanState);
   dfree(h->d_bHi);
   dfree(h->d_bLo);
   dfree(h->d_bGid);
@@ -708,10 +708,8 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_runStart, Vs);
   rc |= dalloc(h, &h->d_deepRuns, 2 * Vs);
   rc |= dalloc(h, &h->d_counts, 8);
-  rc |= dalloc(h, &h->d_radixHist, radix_hist_entries(Vs));
-  rc |= dalloc(h, &h->d_scanTile,
-               std::max(scan_scratch_entries(radix_hist_entries(Vs)),
-                        scan_scratch_entries(2 * Vs + G)));
+  rc |= dalloc(h, &h->d_sortState, sort_state_entries(Vs));
+  rc |= dalloc(h, &h->d_scanState, scan_state_entries(2 * Vs + G));
   rc |= dalloc(h, &h->d_bHi, Vs);
   rc |= dalloc(h, &h->d_bLo, Vs);
   rc |= dalloc(h, &h->d_bGid, Vs);

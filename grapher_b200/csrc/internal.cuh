@@ -164,8 +164,8 @@ struct gvizCudaForce {
   uint32_t *d_flag = nullptr, *d_scan = nullptr;    // V-sized
   uint32_t *d_runStart = nullptr, *d_deepRuns = nullptr;
   uint32_t *d_counts = nullptr;  // [0]=runs [1]=deep runs [2]=buckets [3]=nodes
-  uint32_t *d_radixHist = nullptr;  // 256 * tiles
-  uint32_t *d_scanTile = nullptr;   // scan scratch
+  uint64_t *d_sortState = nullptr;  // radix sort: look-back status, digit counts, tickets
+  uint64_t *d_scanState = nullptr;  // scan: ticket and look-back status
   uint64_t *d_bHi = nullptr, *d_bLo = nullptr;
   uint32_t *d_bGid = nullptr, *d_bStart = nullptr;
   uint32_t *d_nLeft = nullptr, *d_nRight = nullptr, *d_nFirst = nullptr,
@@ -288,8 +288,8 @@ void radix_sort_pairs(gvizCudaForce *h, uint64_t *keys, uint32_t *vals,
                       uint64_t *keysAlt, uint32_t *valsAlt, size_t n);
 void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
                     size_t n, uint32_t *total);
-size_t radix_hist_entries(size_t n);
-size_t scan_scratch_entries(size_t n);
+size_t sort_state_entries(size_t n);
+size_t scan_state_entries(size_t n);
 
 // tree.cu
 void enqueue_tree_build(gvizCudaForce *h);

@@ -4,6 +4,18 @@
 // The quadtree build sorts vertices by their quadrant path; stability keeps
 // equal paths in vertex-index order, which is the arrival order of points in
 // a reference leaf (src/ds/gvizQuadtree.c:129-131).
+//
+// Both are single-pass over their input per digit (per scan): a tile takes
+// its index from a ticket counter, so every lower tile has started before
+// it; it publishes its count (flag AGGREGATE), then adds the counts of the
+// tiles before it, walking back until one has published its inclusive
+// prefix (flag PREFIX), and publishes its own prefix (decoupled look-back).
+// The sort's digit counts of all passes come from one read of the keys.
+// Status words are 64 bits (flag in the high half, count in the low half),
+// written and read with single relaxed accesses; a wait that outlasts its
+// iteration limit sets GVIZ_ST_TREE and ends.
+#include <algorithm>
+
 #include "internal.cuh"
 
 namespace {
@@ -12,12 +24,50 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;  // 2048
 constexpr int kTopThreads = 1024;
-constexpr int kTopItems = 8;  // top level handles 8192 tiles -> 16.7M entries
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096 keys
+constexpr int kSortPasses = (64 - GVIZ_SORT_SKIP_BITS) / 8;
+static_assert(kSortPasses % 2 == 0, "the sorted pairs must end in the input buffers");
+
+constexpr uint64_t kFlagAggregate = 1ull << 32;
+constexpr uint64_t kFlagPrefix = 2ull << 32;
+constexpr uint32_t kLookbackSpin = 1u << 22;  // reads of a status word before giving up
+
+__device__ __forceinline__ uint64_t ld_status(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_status(uint64_t *p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// The sum of the counts of tiles [0, tile) in the status column `st` of
+// stride `stride` (tile t's word is st[t * stride]). Tile 0 publishes its
+// prefix without waiting, so the walk always ends.
+__device__ __forceinline__ uint32_t lookback(const uint64_t *st, size_t stride, uint32_t tile,
+                                             uint32_t *status) {
+  uint32_t excl = 0;
+  uint32_t spins = 0;
+  for (int64_t p = (int64_t)tile - 1; p >= 0;) {
+    const uint64_t w = ld_status(st + (size_t)p * stride);
+    if ((w >> 32) == 0) {  // not published yet
+      if (++spins > kLookbackSpin) {
+        atomicOr(status, GVIZ_ST_TREE);
+        return excl;
+      }
+      continue;
+    }
+    excl += (uint32_t)w;
+    if ((w & ~0xffffffffull) == kFlagPrefix) break;
+    --p;
+  }
+  return excl;
+}
 
 // Block-wide exclusive scan of one value per thread; returns the block total.
 template <int THREADS>
@@ -53,50 +103,48 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v,
   return bt;
 }
 
-__global__ __launch_bounds__(kScanThreads) void k_scan_tiles(
-    const uint32_t *__restrict__ in, uint32_t *out, uint32_t n,
-    uint32_t *tileSums) {
-  uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+// Single-pass exclusive scan: tile = ticket, 2048 entries per tile.
+// state: [0] ticket, [1 + t] status of tile t.
+__global__ __launch_bounds__(kScanThreads) void k_scan_onepass(
+    const uint32_t *in, uint32_t *out, uint32_t n, uint64_t *state, uint32_t *total,
+    uint32_t *status) {
+  __shared__ uint32_t sTile, sExcl;
+  if (threadIdx.x == 0) sTile = atomicAdd(reinterpret_cast<unsigned long long *>(state), 1ull);
+  __syncthreads();
+  const uint32_t tile = sTile;
+  const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
   uint32_t v[kScanItems];
   uint32_t s = 0;
 #pragma unroll
   for (int j = 0; j < kScanItems; j++) {
-    uint32_t i = base + j;
+    const uint32_t i = base + j;
     v[j] = i < n ? in[i] : 0u;
     s += v[j];
   }
   uint32_t excl;
-  uint32_t tot = block_exclusive_scan<kScanThreads>(s, excl);
+  const uint32_t tot = block_exclusive_scan<kScanThreads>(s, excl);
+  uint64_t *st = state + 1;
+  if (threadIdx.x == 0) {
+    if (tile == 0) {
+      st_status(st, kFlagPrefix | tot);
+      sExcl = 0;
+    } else {
+      st_status(st + tile, kFlagAggregate | tot);
+      const uint32_t before = lookback(st, 1, tile, status);
+      st_status(st + tile, kFlagPrefix | (before + tot));
+      sExcl = before;
+    }
+    const uint32_t nTiles = (n + kScanTile - 1) / kScanTile;
+    if (total && tile == nTiles - 1) *total = sExcl + tot;
+  }
+  __syncthreads();
+  excl += sExcl;
 #pragma unroll
   for (int j = 0; j < kScanItems; j++) {
-    uint32_t i = base + j;
+    const uint32_t i = base + j;
     if (i < n) out[i] = excl;
     excl += v[j];
   }
-  if (threadIdx.x == 0) tileSums[blockIdx.x] = tot;
-}
-
-__global__ __launch_bounds__(kTopThreads) void k_scan_top(uint32_t *tileSums,
-                                                          uint32_t nTiles,
-                                                          uint32_t *total) {
-  uint32_t per = (nTiles + kTopThreads - 1) / kTopThreads;
-  uint32_t b = threadIdx.x * per;
-  uint32_t s = 0;
-  for (uint32_t j = 0; j < per; j++) {
-    uint32_t i = b + j;
-    if (i < nTiles) s += tileSums[i];
-  }
-  uint32_t excl;
-  uint32_t tot = block_exclusive_scan<kTopThreads>(s, excl);
-  for (uint32_t j = 0; j < per; j++) {
-    uint32_t i = b + j;
-    if (i < nTiles) {
-      uint32_t t = tileSums[i];
-      tileSums[i] = excl;
-      excl += t;
-    }
-  }
-  if (threadIdx.x == 0 && total) *total = tot;
 }
 
 // Whole scan in one block: each thread owns a contiguous run of ceil(n/1024)
@@ -125,30 +173,31 @@ __global__ __launch_bounds__(kTopThreads) void k_scan_single(
   if (threadIdx.x == 0 && total) *total = tot;
 }
 
-__global__ void k_scan_add(uint32_t *out, uint32_t n,
-                           const uint32_t *__restrict__ tileSums) {
-  uint32_t add = tileSums[blockIdx.x];
-  uint32_t base = blockIdx.x * kScanTile;
-  for (uint32_t j = threadIdx.x; j < (uint32_t)kScanTile; j += blockDim.x) {
-    uint32_t i = base + j;
-    if (i < n) out[i] += add;
-  }
-}
-
-__global__ __launch_bounds__(kSortThreads) void k_radix_hist(
-    const uint64_t *__restrict__ keys, uint32_t n, int shift, uint32_t *hist,
-    uint32_t numTiles) {
-  __shared__ uint32_t sh[256];
-  sh[threadIdx.x] = 0;
+// Digit counts of every sort pass in one read of the keys; equal digits
+// of a warp's 32 keys are added by one lane.
+__global__ __launch_bounds__(kSortThreads) void k_radix_hist_all(
+    const uint64_t *__restrict__ keys, uint32_t n, uint32_t *ghist) {
+  __shared__ uint32_t sh[kSortPasses][256];
+  for (int i = threadIdx.x; i < kSortPasses * 256; i += kSortThreads) (&sh[0][0])[i] = 0u;
   __syncthreads();
-  uint32_t base = blockIdx.x * kSortTile;
-#pragma unroll 4
-  for (int r = 0; r < kSortRounds; r++) {
-    uint32_t i = base + r * kSortThreads + threadIdx.x;
-    if (i < n) atomicAdd(&sh[(uint32_t)(keys[i] >> shift) & 255u], 1u);
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t stride = gridDim.x * kSortThreads;
+  for (uint32_t i0 = blockIdx.x * kSortThreads; i0 < n; i0 += stride) {
+    const uint32_t i = i0 + threadIdx.x;
+    const bool valid = i < n;
+    const uint64_t k = valid ? keys[i] : 0ull;
+#pragma unroll
+    for (int p = 0; p < kSortPasses; p++) {
+      const uint32_t d = valid ? (uint32_t)(k >> (GVIZ_SORT_SKIP_BITS + 8 * p)) & 255u : 256u;
+      const uint32_t peers = __match_any_sync(0xffffffffu, d);
+      if (valid && (peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&sh[p][d], __popc(peers));
+    }
   }
   __syncthreads();
-  hist[threadIdx.x * numTiles + blockIdx.x] = sh[threadIdx.x];
+  for (int i = threadIdx.x; i < kSortPasses * 256; i += kSortThreads) {
+    const uint32_t c = (&sh[0][0])[i];
+    if (c) atomicAdd(ghist + i, c);
+  }
 }
 
 // Stable scatter: warp w of a tile owns 512 consecutive keys, taken in
@@ -157,10 +206,14 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_hist(
 // and values reordered by digit.
 constexpr size_t kScatterDyn = (size_t)kSortTile * (sizeof(uint64_t) + sizeof(uint32_t));
 
-__global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
+// One pass over digit `pass`: tile = ticket; each digit's start in the
+// output is its global start (a scan of ghist) plus its count in the tiles
+// before (look-back over the status words state[tile * 256 + digit]).
+__global__ __launch_bounds__(kSortThreads) void k_radix_onesweep(
     const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin,
     uint64_t *__restrict__ kout, uint32_t *__restrict__ vout, uint32_t n,
-    int shift, const uint32_t *__restrict__ offs, uint32_t numTiles) {
+    int pass, const uint32_t *__restrict__ ghist, uint64_t *state, uint32_t *ticket,
+    uint32_t *status) {
   extern __shared__ __align__(16) unsigned char dyn[];
   uint64_t *sk = reinterpret_cast<uint64_t *>(dyn);
   uint32_t *sv = reinterpret_cast<uint32_t *>(sk + kSortTile);
@@ -168,12 +221,18 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
   __shared__ uint32_t base[256];
   __shared__ uint32_t start[256];  // first in-tile position of each digit
   __shared__ uint32_t wsum[kSortWarps];
+  __shared__ uint32_t sTile;
   const unsigned tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
+  const int shift = GVIZ_SORT_SKIP_BITS + 8 * pass;
+  if (tid == 0) sTile = atomicAdd(ticket, 1u);
   for (unsigned d = tid; d < kSortWarps * 256; d += kSortThreads)
     (&wcnt[0][0])[d] = 0;
-  base[tid] = offs[tid * numTiles + blockIdx.x];
+  // the digit's first output position: exclusive scan of the global counts
+  uint32_t gstart;
+  block_exclusive_scan<kSortThreads>(ghist[pass * 256 + tid], gstart);
   __syncthreads();
-  const uint32_t tileBase = blockIdx.x * kSortTile + w * (kSortRounds * 32);
+  const uint32_t tile = sTile;
+  const uint32_t tileBase = tile * kSortTile + w * (kSortRounds * 32);
   uint64_t k[kSortRounds];
   uint32_t v[kSortRounds];
   uint32_t rank[kSortRounds];
@@ -202,6 +261,19 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
     wcnt[ww][tid] = run;
     run += t;
   }
+  // this tile's count of digit tid, then the counts of the tiles before
+  {
+    uint64_t *col = state + tid;
+    if (tile == 0) {
+      st_status(col, kFlagPrefix | run);
+      base[tid] = gstart;
+    } else {
+      st_status(col + (size_t)tile * 256, kFlagAggregate | run);
+      const uint32_t before = lookback(col, 256, tile, status);
+      st_status(col + (size_t)tile * 256, kFlagPrefix | (before + run));
+      base[tid] = gstart + before;
+    }
+  }
   uint32_t incl = run;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -227,7 +299,7 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
   }
   __syncthreads();
   // ... then written out in order: each digit's run lands contiguously
-  const uint32_t t0 = blockIdx.x * kSortTile;
+  const uint32_t t0 = tile * kSortTile;
   const uint32_t cnt = n - t0 < (uint32_t)kSortTile ? n - t0 : (uint32_t)kSortTile;
   for (uint32_t j = tid; j < cnt; j += kSortThreads) {
     const uint64_t kk = sk[j];
@@ -240,16 +312,18 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_scatter(
 
 }  // namespace
 
-size_t scan_scratch_entries(size_t n) {
+size_t scan_state_entries(size_t n) {
   return (n + kScanTile - 1) / kScanTile + 1;
 }
 
-size_t radix_hist_entries(size_t n) {
-  size_t tiles = (n + kSortTile - 1) / kSortTile;
-  return 256 * (tiles ? tiles : 1);
+size_t sort_state_entries(size_t n) {
+  const size_t tiles = (n + kSortTile - 1) / kSortTile;
+  // per pass: tiles * 256 status words; then the global counts (uint32) and
+  // the tickets, in 64-bit words
+  return (size_t)kSortPasses * 256 * (tiles ? tiles : 1) + kSortPasses * 128 + kSortPasses;
 }
 
-// Exclusive scan of n uint32 (n <= 16.7M); in == out allowed. total may be
+// Exclusive scan of n uint32 (n <= 2^31); in == out allowed. total may be
 // nullptr or a device pointer receiving the sum.
 void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
                     size_t n, uint32_t *total) {
@@ -261,12 +335,10 @@ void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
     k_scan_single<<<1, kTopThreads, 0, h->stream>>>(in, out, (uint32_t)n, total);
     return;
   }
-  uint32_t tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
-  k_scan_tiles<<<tiles, kScanThreads, 0, h->stream>>>(in, out, (uint32_t)n,
-                                                      h->d_scanTile);
-  k_scan_top<<<1, kTopThreads, 0, h->stream>>>(h->d_scanTile, tiles, total);
-  if (tiles > 1)
-    k_scan_add<<<tiles, 256, 0, h->stream>>>(out, (uint32_t)n, h->d_scanTile);
+  const uint32_t tiles = (uint32_t)((n + kScanTile - 1) / kScanTile);
+  cudaMemsetAsync(h->d_scanState, 0, (tiles + 1) * sizeof(uint64_t), h->stream);
+  k_scan_onepass<<<tiles, kScanThreads, 0, h->stream>>>(in, out, (uint32_t)n, h->d_scanState,
+                                                        total, h->d_status);
 }
 
 // Stable sort by the key bits above GVIZ_SORT_SKIP_BITS (an even number of
@@ -275,29 +347,33 @@ void scan_exclusive(gvizCudaForce *h, const uint32_t *in, uint32_t *out,
 // The scatter's shared memory exceeds the default per-block budget: opted
 // into once per device, at handle creation (outside any stream capture).
 void sort_set_smem_limits() {
-  cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaFuncSetAttribute(k_radix_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)kScatterDyn);
 }
 
 void radix_sort_pairs(gvizCudaForce *h, uint64_t *keys, uint32_t *vals,
                       uint64_t *keysAlt, uint32_t *valsAlt, size_t n) {
   if (n <= 1) return;
-  uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
+  const uint32_t tiles = (uint32_t)((n + kSortTile - 1) / kSortTile);
+  uint64_t *state = h->d_sortState;
+  const size_t statusWords = (size_t)kSortPasses * 256 * tiles;
+  uint32_t *ghist = reinterpret_cast<uint32_t *>(state + statusWords);
+  uint32_t *tickets = ghist + kSortPasses * 256;
+  cudaMemsetAsync(state, 0, (statusWords + kSortPasses * 128 + kSortPasses) * sizeof(uint64_t),
+                  h->stream);
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint32_t hb = std::min<uint32_t>(tiles * kSortRounds, (uint32_t)(sms > 0 ? sms : 1) * 8u);
+  k_radix_hist_all<<<hb, kSortThreads, 0, h->stream>>>(keys, (uint32_t)n, ghist);
   uint64_t *ka = keys, *kb = keysAlt;
   uint32_t *va = vals, *vb = valsAlt;
-  for (int shift = GVIZ_SORT_SKIP_BITS; shift < 64; shift += 8) {
-    k_radix_hist<<<tiles, kSortThreads, 0, h->stream>>>(ka, (uint32_t)n, shift,
-                                                        h->d_radixHist, tiles);
-    scan_exclusive(h, h->d_radixHist, h->d_radixHist, (size_t)256 * tiles,
-                   nullptr);
-    k_radix_scatter<<<tiles, kSortThreads, kScatterDyn, h->stream>>>(
-        ka, va, kb, vb, (uint32_t)n, shift, h->d_radixHist, tiles);
-    uint64_t *tk = ka;
-    ka = kb;
-    kb = tk;
-    uint32_t *tv = va;
-    va = vb;
-    vb = tv;
+  for (int pass = 0; pass < kSortPasses; pass++) {
+    k_radix_onesweep<<<tiles, kSortThreads, kScatterDyn, h->stream>>>(
+        ka, va, kb, vb, (uint32_t)n, pass, ghist, state + (size_t)pass * 256 * tiles,
+        tickets + pass, h->d_status);
+    std::swap(ka, kb);
+    std::swap(va, vb);
   }
   prof_mark(h, "radix_sort");
 }

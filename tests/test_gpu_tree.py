@@ -98,3 +98,38 @@ def test_forest_membership_matches_each_graph(oracle):
         s = slice(int(offs[g]), int(offs[g + 1]))
         assert np.array_equal(d[s], od) and np.array_equal(hi[s], ohi) and np.array_equal(lo[s], olo)
     lay.close()
+
+
+@pytest.mark.parametrize("k", [1, 4])
+def test_membership_with_many_sort_and_scan_tiles(oracle, k):
+    """300,000 points: the radix sort's passes run over 74 tiles of 4,096 keys
+    and the scans over 147 tiles of 2,048, so every tile's offsets come from
+    the look-back over the tiles before it."""
+    rng = np.random.default_rng(11)
+    pts = np.concatenate([rng.uniform(-1000, 1000, (250000, 2)),
+                          rng.normal(0, 1e-2, (50000, 2))])
+    mass = 1.0 + (np.arange(len(pts)) % 7).astype(np.float64)
+    od, ohi, olo, _ = oracle.quadtree_leaves(pts, mass, k)
+    lay = point_layout(pts, mass, k)
+    d, hi, lo, _ = lay.tree_leaves()
+    assert np.array_equal(d, od)
+    assert np.array_equal(hi, ohi) and np.array_equal(lo, olo)
+    check_cells(lay.tree_nodes(), oracle.quadtree_nodes(pts, mass, k), 1000.0)
+    lay.close()
+
+
+def test_forest_of_many_graphs(oracle):
+    """9,000 graphs of 1 to 39 points: the scan over the graphs' node counts
+    runs over several tiles (more than one block's worth of entries)."""
+    rng = np.random.default_rng(5)
+    sizes = rng.integers(1, 40, 9000)
+    pts = [rng.uniform(-10, 10, (int(n), 2)) * 10 ** rng.uniform(-2, 2) for n in sizes]
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    allp = np.concatenate(pts)
+    lay = point_layout(allp, np.ones(len(allp)), 1, graph_offsets=offs)
+    d, hi, lo, _ = lay.tree_leaves()
+    for g, p in enumerate(pts):
+        od, ohi, olo, _ = oracle.quadtree_leaves(p, np.ones(len(p)), 1)
+        s = slice(int(offs[g]), int(offs[g + 1]))
+        assert np.array_equal(d[s], od) and np.array_equal(hi[s], ohi) and np.array_equal(lo[s], olo)
+    lay.close()
