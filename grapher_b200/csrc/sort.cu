@@ -10,7 +10,8 @@
 // it; it publishes its count (flag AGGREGATE), then adds the counts of the
 // tiles before it, walking back until one has published its inclusive
 // prefix (flag PREFIX), and publishes its own prefix (decoupled look-back).
-// The sort's digit counts of all passes come from one read of the keys.
+// The first pass's digit counts come from one read of the keys; each pass
+// counts the next pass's digits of the keys it holds.
 // Status words are 64 bits (flag in the high half, count in the low half),
 // written and read with single relaxed accesses; a wait that outlasts its
 // iteration limit sets GVIZ_ST_TREE and ends.
@@ -47,24 +48,32 @@ __device__ __forceinline__ void st_status(uint64_t *p, uint64_t v) {
 }
 
 // The sum of the counts of tiles [0, tile) in the status column `st` of
-// stride `stride` (tile t's word is st[t * stride]). Tile 0 publishes its
-// prefix without waiting, so the walk always ends.
+// stride `stride` (tile t's word is st[t * stride]), read kLookbackWidth
+// tiles at a time (independent loads). Tile 0 publishes its prefix without
+// waiting, so the walk always ends.
+constexpr int kLookbackWidth = 8;
+
 __device__ __forceinline__ uint32_t lookback(const uint64_t *st, size_t stride, uint32_t tile,
                                              uint32_t *status) {
   uint32_t excl = 0;
   uint32_t spins = 0;
-  for (int64_t p = (int64_t)tile - 1; p >= 0;) {
-    const uint64_t w = ld_status(st + (size_t)p * stride);
-    if ((w >> 32) == 0) {  // not published yet
-      if (++spins > kLookbackSpin) {
-        atomicOr(status, GVIZ_ST_TREE);
-        return excl;
+  for (int64_t p = (int64_t)tile - 1; p >= 0; p -= kLookbackWidth) {
+    uint64_t w[kLookbackWidth];
+#pragma unroll
+    for (int i = 0; i < kLookbackWidth; i++)
+      w[i] = p - i >= 0 ? ld_status(st + (size_t)(p - i) * stride) : kFlagPrefix;
+#pragma unroll
+    for (int i = 0; i < kLookbackWidth; i++) {
+      while ((w[i] >> 32) == 0) {  // not published yet
+        if (++spins > kLookbackSpin) {
+          atomicOr(status, GVIZ_ST_TREE);
+          return excl;
+        }
+        w[i] = ld_status(st + (size_t)(p - i) * stride);
       }
-      continue;
+      excl += (uint32_t)w[i];
+      if ((w[i] & ~0xffffffffull) == kFlagPrefix) return excl;
     }
-    excl += (uint32_t)w;
-    if ((w & ~0xffffffffull) == kFlagPrefix) break;
-    --p;
   }
   return excl;
 }
@@ -173,31 +182,19 @@ __global__ __launch_bounds__(kTopThreads) void k_scan_single(
   if (threadIdx.x == 0 && total) *total = tot;
 }
 
-// Digit counts of every sort pass in one read of the keys; equal digits
-// of a warp's 32 keys are added by one lane.
-__global__ __launch_bounds__(kSortThreads) void k_radix_hist_all(
+// Digit counts of the first sort pass (each later pass counts the digit of
+// the pass after it while it scatters).
+__global__ __launch_bounds__(kSortThreads) void k_radix_hist0(
     const uint64_t *__restrict__ keys, uint32_t n, uint32_t *ghist) {
-  __shared__ uint32_t sh[kSortPasses][256];
-  for (int i = threadIdx.x; i < kSortPasses * 256; i += kSortThreads) (&sh[0][0])[i] = 0u;
+  __shared__ uint32_t sh[256];
+  sh[threadIdx.x] = 0u;
   __syncthreads();
-  const unsigned lane = threadIdx.x & 31u;
   const uint32_t stride = gridDim.x * kSortThreads;
-  for (uint32_t i0 = blockIdx.x * kSortThreads; i0 < n; i0 += stride) {
-    const uint32_t i = i0 + threadIdx.x;
-    const bool valid = i < n;
-    const uint64_t k = valid ? keys[i] : 0ull;
-#pragma unroll
-    for (int p = 0; p < kSortPasses; p++) {
-      const uint32_t d = valid ? (uint32_t)(k >> (GVIZ_SORT_SKIP_BITS + 8 * p)) & 255u : 256u;
-      const uint32_t peers = __match_any_sync(0xffffffffu, d);
-      if (valid && (peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&sh[p][d], __popc(peers));
-    }
-  }
+  for (uint32_t i = blockIdx.x * kSortThreads + threadIdx.x; i < n; i += stride)
+    atomicAdd(&sh[(uint32_t)(keys[i] >> GVIZ_SORT_SKIP_BITS) & 255u], 1u);
   __syncthreads();
-  for (int i = threadIdx.x; i < kSortPasses * 256; i += kSortThreads) {
-    const uint32_t c = (&sh[0][0])[i];
-    if (c) atomicAdd(ghist + i, c);
-  }
+  const uint32_t c = sh[threadIdx.x];
+  if (c) atomicAdd(ghist + threadIdx.x, c);
 }
 
 // Stable scatter: warp w of a tile owns 512 consecutive keys, taken in
@@ -212,7 +209,7 @@ constexpr size_t kScatterDyn = (size_t)kSortTile * (sizeof(uint64_t) + sizeof(ui
 __global__ __launch_bounds__(kSortThreads) void k_radix_onesweep(
     const uint64_t *__restrict__ kin, const uint32_t *__restrict__ vin,
     uint64_t *__restrict__ kout, uint32_t *__restrict__ vout, uint32_t n,
-    int pass, const uint32_t *__restrict__ ghist, uint64_t *state, uint32_t *ticket,
+    int pass, uint32_t *ghist, uint64_t *state, uint32_t *ticket,
     uint32_t *status) {
   extern __shared__ __align__(16) unsigned char dyn[];
   uint64_t *sk = reinterpret_cast<uint64_t *>(dyn);
@@ -222,11 +219,14 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_onesweep(
   __shared__ uint32_t start[256];  // first in-tile position of each digit
   __shared__ uint32_t wsum[kSortWarps];
   __shared__ uint32_t sTile;
+  __shared__ uint32_t nextCnt[256];  // the next pass's digit counts of this tile
   const unsigned tid = threadIdx.x, w = tid >> 5, lane = tid & 31u;
   const int shift = GVIZ_SORT_SKIP_BITS + 8 * pass;
+  const bool countNext = pass + 1 < kSortPasses;
   if (tid == 0) sTile = atomicAdd(ticket, 1u);
   for (unsigned d = tid; d < kSortWarps * 256; d += kSortThreads)
     (&wcnt[0][0])[d] = 0;
+  nextCnt[tid] = 0u;
   // the digit's first output position: exclusive scan of the global counts
   uint32_t gstart;
   block_exclusive_scan<kSortThreads>(ghist[pass * 256 + tid], gstart);
@@ -243,6 +243,7 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_onesweep(
     k[r] = valid ? kin[i] : 0ull;
     v[r] = valid ? vin[i] : 0u;
     uint32_t d = valid ? ((uint32_t)(k[r] >> shift) & 255u) : 256u;
+    if (countNext && valid) atomicAdd(&nextCnt[(uint32_t)(k[r] >> (shift + 8)) & 255u], 1u);
     uint32_t peers = __match_any_sync(0xffffffffu, d);
     uint32_t lt = peers & ((1u << lane) - 1u);
     uint32_t before = valid ? wcnt[w][d] : 0u;
@@ -274,6 +275,7 @@ __global__ __launch_bounds__(kSortThreads) void k_radix_onesweep(
       base[tid] = gstart + before;
     }
   }
+  if (countNext && nextCnt[tid]) atomicAdd(ghist + (pass + 1) * 256 + tid, nextCnt[tid]);
   uint32_t incl = run;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -364,8 +366,8 @@ void radix_sort_pairs(gvizCudaForce *h, uint64_t *keys, uint32_t *vals,
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const uint32_t hb = std::min<uint32_t>(tiles * kSortRounds, (uint32_t)(sms > 0 ? sms : 1) * 8u);
-  k_radix_hist_all<<<hb, kSortThreads, 0, h->stream>>>(keys, (uint32_t)n, ghist);
+  const uint32_t hb = std::min<uint32_t>(tiles * 4u, (uint32_t)(sms > 0 ? sms : 1) * 2u);
+  k_radix_hist0<<<hb, kSortThreads, 0, h->stream>>>(keys, (uint32_t)n, ghist);
   uint64_t *ka = keys, *kb = keysAlt;
   uint32_t *va = vals, *vb = valsAlt;
   for (int pass = 0; pass < kSortPasses; pass++) {
