@@ -339,6 +339,31 @@ __device__ __forceinline__ bool plain_visit(const WalkArgs &a, const PlainTarget
   return in && massOk && !isLeaf && !accept;
 }
 
+// plain_visit without the coincidence vote: the term of a point or accepted
+// cell on the straight-line path (a coincident point gives a term that is
+// not finite; the caller then redoes the round with plain_visit).
+template <int MODEL, bool OVERLAP>
+__device__ __forceinline__ bool plain_visit_fast(const WalkArgs &a, const PlainTarget &t, bool in,
+                                                 float4 n0, float4 n1, float &px, float &py) {
+  const float nmass = n1.x, nsize = n1.y;
+  const int32_t ninfo = __float_as_int(n1.w);
+  const float dx = (n0.x - t.vxh) + (n0.z - t.vxl);
+  const float dy = (n0.y - t.vyh) + (n0.w - t.vyl);
+  const float d2 = dx * dx + dy * dy;
+  const bool isLeaf = ninfo >= 0;
+  const bool massOk = nmass != 0.0f;
+  const bool accept = !isLeaf && nsize < d2;
+  const bool doForce = in && massOk && (isLeaf ? ((uint32_t)ninfo != t.v) : accept);
+  if (doForce) {
+    float fx, fy;
+    rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, nmass, t.rv + (isLeaf ? nsize : 0.0f),
+                                   a.num, a.overlapC, fx, fy);
+    px += fx;
+    py += fy;
+  }
+  return in && massOk && !isLeaf && !accept;
+}
+
 // The stackless union walk of the preorder range [lo, hi) for the lanes in
 // `lanes`: the warp steps through the union of the nodes they need, each
 // lane's next node is cur + 1 (opened) or the node's skip pointer, the warp
@@ -433,12 +458,32 @@ __device__ __forceinline__ void walk_task(const WalkArgs &a, uint32_t task, cons
     // target's Kahan-compensated sum (cascade summation, <= 32 terms a run)
     uint32_t myOpen = 0;
     float px = 0.f, py = 0.f;
-    for (uint32_t j = 0; j < n; j++) {
-      const uint32_t lanes = __shfl_sync(0xffffffffu, e.y, j);
-      const bool open = plain_visit<MODEL, OVERLAP>(a, t, (lanes >> lane) & 1u, q.rec[j][0],
-                                                    q.rec[j][1], px, py, nInter);
-      const uint32_t ob = __ballot_sync(0xffffffffu, open);
-      if (lane == j) myOpen = ob;
+    if (COUNT) {  // instrumented: the guarded visits, counting terms
+      for (uint32_t j = 0; j < n; j++) {
+        const uint32_t lanes = __shfl_sync(0xffffffffu, e.y, j);
+        const bool open = plain_visit<MODEL, OVERLAP>(a, t, (lanes >> lane) & 1u, q.rec[j][0],
+                                                      q.rec[j][1], px, py, nInter);
+        const uint32_t ob = __ballot_sync(0xffffffffu, open);
+        if (lane == j) myOpen = ob;
+      }
+    } else {
+      for (uint32_t j = 0; j < n; j++) {
+        const uint32_t lanes = __shfl_sync(0xffffffffu, e.y, j);
+        const bool open = plain_visit_fast<MODEL, OVERLAP>(a, t, (lanes >> lane) & 1u, q.rec[j][0],
+                                                           q.rec[j][1], px, py);
+        const uint32_t ob = __ballot_sync(0xffffffffu, open);
+        if (lane == j) myOpen = ob;
+      }
+      // a coincident point in the round: the round again on the guarded path
+      // (the same decisions; the open masks above stand)
+      if (__any_sync(0xffffffffu, !(isfinite(px) && isfinite(py)))) {
+        px = py = 0.f;
+        for (uint32_t j = 0; j < n; j++) {
+          const uint32_t lanes = __shfl_sync(0xffffffffu, e.y, j);
+          plain_visit<MODEL, OVERLAP>(a, t, (lanes >> lane) & 1u, q.rec[j][0], q.rec[j][1], px,
+                                      py, nInter);
+        }
+      }
     }
     kx.add(px);
     ky.add(py);
@@ -901,11 +946,14 @@ struct CellSums {
   unsigned long long nInter = 0, nRows = 0;  // instrumentation only
 };
 
-// Every target takes the pair term of the first k listed points.
+// Every target takes the pair term of the first k listed points (at most
+// 32, summed in a plain FP32 partial that then joins the target's
+// Kahan-compensated sum: cascade summation, as in the plain walk).
 template <int MODEL, bool OVERLAP, bool COUNT>
 __device__ __forceinline__ void cell_eval_points(const WalkArgs &a, CellWarpSmem &q,
                                                  const CellTarget &t, CellSums &s, uint32_t k) {
   __syncwarp();
+  float px = 0.f, py = 0.f;
 #pragma unroll 1  // a compact loop: the walk is sensitive to instruction-cache misses
   for (uint32_t j = 0; j < k; j++) {
     const uint32_t e = (s.ph + j) & (kCellRing - 1);
@@ -925,12 +973,12 @@ __device__ __forceinline__ void cell_eval_points(const WalkArgs &a, CellWarpSmem
       rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, mr.x, t.rv + mr.y, a.num, a.overlapC,
                                      fx, fy);
     }
-    if (doForce) {
-      s.kx.add(fx);
-      s.ky.add(fy);
-      if (COUNT) s.nInter++;
-    }
+    px += fx;
+    py += fy;
+    if (COUNT && doForce) s.nInter++;
   }
+  s.kx.add(px);
+  s.ky.add(py);
   s.ph = (s.ph + k) & (kCellRing - 1);
   s.pn -= k;
   __syncwarp();
@@ -938,7 +986,8 @@ __device__ __forceinline__ void cell_eval_points(const WalkArgs &a, CellWarpSmem
 
 // The first k <= 16 listed cells: lane r < k builds row r (cell r seen from
 // the group's centroid), the tile runs on the tensor cores, then every
-// target adds each cell's monopole term and the row's correction of it.
+// target adds each cell's monopole term (a plain partial of the k terms,
+// then the Kahan sum) and the row's correction of it.
 template <int MODEL, bool OVERLAP, bool COUNT>
 __device__ __forceinline__ void cell_eval_cells(const WalkArgs &a, const FarCell *__restrict__ cells,
                                                 const MlpSmem &W, CellWarpSmem &q,
@@ -971,6 +1020,7 @@ __device__ __forceinline__ void cell_eval_cells(const WalkArgs &a, const FarCell
   __syncwarp();
   mlp_forward_tile<true>(W, q.gx, MLP_XS, reinterpret_cast<float *>(q.out));
   __syncwarp();
+  float px = 0.f, py = 0.f;
 #pragma unroll 1  // a compact loop: the walk is sensitive to instruction-cache misses
   for (uint32_t r = 0; r < k; r++) {
     const uint32_t e = (s.ch + r) & (kCellRing - 1);
@@ -986,13 +1036,15 @@ __device__ __forceinline__ void cell_eval_cells(const WalkArgs &a, const FarCell
     } else if (t.has) {
       rep_term_apart<MODEL, OVERLAP>(dx, dy, d2, t.mv, m, t.rv, a.num, a.overlapC, fx, fy);
     }
+    px += fx;
+    py += fy;
     if (t.has) {
-      s.kx.add(fx);
-      s.ky.add(fy);
       far_apply(q.out[r], make_float2(fx, fy), s.corrx, s.corry);
       if (COUNT) s.nInter++;
     }
   }
+  s.kx.add(px);
+  s.ky.add(py);
   if (COUNT) s.nRows += k;
   s.ch = (s.ch + k) & (kCellRing - 1);
   s.cn -= k;
