@@ -20,7 +20,7 @@ the RMS of the per-vertex relative errors and the largest per-vertex error
 over the RMS force.
 The plain walk runs at theta = 0.5; the learned walk (the cell-group walk:
 one warp per group of <= 32 targets cut from the tree, one network row per
-accepted cell) at the largest theta of 1.3, 1.25, ..., 0.6 whose error is
+accepted cell) at the largest theta of 1.3, 1.275, ..., 0.6 whose error is
 not above the plain walk's. It is judged alone and with hub targets (the
 V / 1024 or V / 256 heaviest vertices take the plain monopole walk at
 theta = 0.35, since LinLog's force on a vertex scales with its mass); each
@@ -462,12 +462,13 @@ def replica_value(ms_max, steps, world):
 
 
 # ------------------------------------------------------------ learned setup
-LEARNED_THETAS = tuple(round(1.3 - 0.05 * i, 2) for i in range(15))  # 1.3 ... 0.6
+LEARNED_THETAS = tuple(round(1.3 - 0.025 * i, 3) for i in range(29))  # 1.3, 1.275 ... 0.6
 LEARNED_SPREAD = 1.0
 LEARNED_CELL_GROUPS = 1  # the cell-group walk: one warp per tree-cut group of <= 32 targets
 HUB_SHARES = (1024, 256)  # hub-target candidates: the V / share heaviest vertices
 HUB_THETA = 0.35         # their plain walk's opening threshold
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
+TRAIN_EPOCHS = 40        # Adam passes over the harvested pairs
 # The learned comparison starts from a fixed point of the layout, whatever
 # --warmup asks for: LEARNED_PRE_STEPS plain steps from the initial
 # positions, then the harvest snapshots of HARVEST_SCHEDULE, all in the FP64
@@ -539,7 +540,7 @@ def learned_setup(lay, w, reduce=lambda x: x, hub_targets="auto"):
         Xs.append(X), Ts.append(T), Ws.append(Wt)
     model = FarFieldModel(seed=SEED)
     losses = model.train(np.concatenate(Xs), np.concatenate(Ts), np.concatenate(Ws),
-                         epochs=40, batch=4096, lr=2e-3, seed=SEED)
+                         epochs=TRAIN_EPOCHS, batch=4096, lr=2e-3, seed=SEED)
     train_s = time.perf_counter() - t0
     if w.V <= JUDGE_ALL_MAX:
         targets = np.arange(w.V, dtype=np.uint32)

@@ -184,6 +184,7 @@ _SIGS = {
     "gvizCudaForceSaveEmbeddingText": (C.c_int, [P, C.c_char_p, C.c_char_p]),
     "gvizCudaLoadEdgesFile": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(Csr)]),
     "gvizCudaLoadObjFile": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
+    "gvizCudaLoadGexfFile": (C.c_int, [C.c_char_p, C.POINTER(Csr)]),
     "gvizCudaCsrFree": (None, [C.POINTER(Csr)]),
     "gvizCudaRandomizePositions": (None, [DP, SZ, D, C.c_uint]),
 }

@@ -13,6 +13,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <string>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
@@ -84,6 +85,85 @@ int edges_to_csr(size_t V, const std::vector<uint32_t> &ea, const std::vector<ui
   out->rowOffsets = row;
   out->neighbors = col;
   out->directed = directed;
+  return 0;
+}
+
+// ---- GEXF (src/utils/graphLoader.c:186-800): the tag scanner's rules ----
+// A tag is its name followed by a blank, '/' or '>'; it ends at the first
+// '>' after it; an attribute is the first `name="` (else `name='`) inside
+// the tag, its value up to the matching quote and shorter than the
+// loader's buffer. Kept alike so that a file loads, or fails, the same way.
+
+bool gexf_tag_char(char c) {
+  return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '/' || c == '>';
+}
+
+const char *gexf_tag(const char *from, const char *name) {
+  const size_t n = strlen(name);
+  for (const char *p = from; (p = strstr(p, name)) != nullptr; p += n)
+    if (gexf_tag_char(p[n])) return p;
+  return nullptr;
+}
+
+// first occurrence of needle wholly inside [hay, end)
+const char *gexf_find(const char *hay, const char *end, const char *needle) {
+  const size_t n = strlen(needle);
+  if (n == 0 || end < hay || n > (size_t)(end - hay)) return nullptr;
+  for (const char *p = hay; p + n <= end; p++)
+    if (memcmp(p, needle, n) == 0) return p;
+  return nullptr;
+}
+
+const char *gexf_tag_in(const char *from, const char *end, const char *name) {
+  const size_t n = strlen(name);
+  for (const char *p = from; p < end;) {
+    const char *f = gexf_find(p, end, name);
+    if (!f) return nullptr;
+    if (f + n <= end && gexf_tag_char(f[n])) return f;
+    p = f + n;
+  }
+  return nullptr;
+}
+
+// 0 with the value in out, or -1 (absent, unterminated, or cap or longer)
+int gexf_attr(const char *ts, const char *te, const char *name, std::string &out, size_t cap) {
+  std::string pat = std::string(name) + "=\"";
+  char quote = '"';
+  const char *p = gexf_find(ts, te, pat.c_str());
+  if (!p) {
+    pat = std::string(name) + "='";
+    quote = '\'';
+    p = gexf_find(ts, te, pat.c_str());
+  }
+  if (!p) return -1;
+  p += pat.size();
+  const char *q = static_cast<const char *>(memchr(p, quote, (size_t)(te - p)));
+  if (!q || (size_t)(q - p) >= cap) return -1;
+  out.assign(p, q);
+  return 0;
+}
+
+// The checks of the attribute-type table (node attributes need an id);
+// the types themselves only shape gviz's per-vertex JSON, which the layout
+// does not use.
+int gexf_check_attribute_types(const char *buf) {
+  std::string v;
+  for (const char *p = buf, *ts; (ts = gexf_tag(p, "<attributes")) != nullptr;) {
+    const char *te = strchr(ts, '>');
+    if (!te) return -1;
+    const bool edgeClass = gexf_attr(ts, te, "class", v, 32) == 0 && v == "edge";
+    const char *body = te + 1;
+    const char *bodyEnd = strstr(body, "</attributes>");
+    if (!bodyEnd) return -1;
+    if (!edgeClass) {
+      for (const char *ap = body, *at; (at = gexf_tag_in(ap, bodyEnd, "<attribute")) != nullptr;) {
+        const char *ate = static_cast<const char *>(memchr(at, '>', (size_t)(bodyEnd - at)));
+        if (!ate || gexf_attr(at, ate, "id", v, 256) < 0) return -1;
+        ap = ate + 1;
+      }
+    }
+    p = bodyEnd + strlen("</attributes>");
+  }
   return 0;
 }
 
@@ -210,6 +290,82 @@ int gvizCudaLoadObjFile(const char *path, gvizCudaCsr *out) {
   }
   if (V == 0) return -1;
   return edges_to_csr(V, ea, eb, 0, out) == 0 ? 0 : -1;
+}
+
+int gvizCudaLoadGexfFile(const char *path, gvizCudaCsr *out) {
+  if (!path || !out) return -1;
+  memset(out, 0, sizeof(*out));
+  FILE *f = fopen(path, "rb");
+  if (!f) return -1;
+  std::string text;
+  if (fseek(f, 0, SEEK_END) != 0) {
+    fclose(f);
+    return -1;
+  }
+  const long size = ftell(f);
+  if (size < 0 || fseek(f, 0, SEEK_SET) != 0) {
+    fclose(f);
+    return -1;
+  }
+  try {
+    text.resize((size_t)size);
+    text.resize(fread(&text[0], 1, (size_t)size, f));
+  } catch (...) {
+    fclose(f);
+    return -1;
+  }
+  fclose(f);
+  const char *buf = text.c_str();  // scanned as a C string, as gviz does
+  try {
+    size_t nodeTags = 0;
+    for (const char *p = buf; (p = gexf_tag(p, "<node")) != nullptr; p += 5) nodeTags++;
+    if (nodeTags == 0 || nodeTags >= 0xffffffffull) return -1;
+    if (gexf_check_attribute_types(buf) < 0) return -1;
+    // vertices in tag order; an id names the first vertex that carried it
+    std::unordered_map<std::string, uint32_t> ids;
+    ids.reserve(nodeTags * 2);
+    uint32_t V = 0;
+    std::string id, v1, v2;
+    for (const char *p = buf, *ts; (ts = gexf_tag(p, "<node")) != nullptr;) {
+      const char *te = strchr(ts, '>');
+      if (!te || gexf_attr(ts, te, "id", id, 256) < 0) return -1;
+      const char *next = te + 1;
+      if (!(te > ts && te[-1] == '/')) {
+        const char *close = strstr(te + 1, "</node>");
+        if (!close) return -1;
+        // <attvalue for|id="..." value="..."> entries must parse
+        for (const char *ap = te + 1, *at; (at = gexf_tag_in(ap, close, "<attvalue")) != nullptr;) {
+          const char *ate = static_cast<const char *>(memchr(at, '>', (size_t)(close - at)));
+          if (!ate) return -1;
+          if ((gexf_attr(at, ate, "for", v1, 256) < 0 && gexf_attr(at, ate, "id", v1, 256) < 0) ||
+              gexf_attr(at, ate, "value", v2, 512) < 0)
+            return -1;
+          ap = ate + 1;
+        }
+        next = close + strlen("</node>");
+      }
+      ids.emplace(id, V);
+      V++;
+      p = next;
+    }
+    // undirected edges in tag order; both ends must name vertices
+    std::vector<uint32_t> ea, eb;
+    for (const char *p = buf, *ts; (ts = gexf_tag(p, "<edge")) != nullptr;) {
+      const char *te = strchr(ts, '>');
+      if (!te || gexf_attr(ts, te, "source", v1, 256) < 0 ||
+          gexf_attr(ts, te, "target", v2, 256) < 0)
+        return -1;
+      const auto a = ids.find(v1), b = ids.find(v2);
+      if (a == ids.end() || b == ids.end()) return -1;
+      ea.push_back(a->second);
+      eb.push_back(b->second);
+      p = te + 1;
+    }
+    return edges_to_csr(V, ea, eb, 0, out);
+  } catch (...) {
+    memset(out, 0, sizeof(*out));
+    return -1;
+  }
 }
 
 }  // extern "C"

@@ -118,3 +118,12 @@ def load_obj_file(path):
     rc = N.lib().gvizCudaLoadObjFile(str(path).encode(), C.byref(csr))
     row, col, _ = _take_csr(rc, csr, f"load_obj_file({path})")
     return row, col
+
+
+def load_gexf_file(path):
+    """gvizGraphLoadFromGexfFile straight to CSR: (row_offsets, neighbors),
+    vertices in <node> order, undirected edges in <edge> order."""
+    csr = N.Csr()
+    rc = N.lib().gvizCudaLoadGexfFile(str(path).encode(), C.byref(csr))
+    row, col, _ = _take_csr(rc, csr, f"load_gexf_file({path})")
+    return row, col

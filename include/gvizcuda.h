@@ -544,6 +544,17 @@ int gvizCudaLoadEdgesFile(const char *path, int directed, int skipHeader,
  * ignored, no repeats, no self-loops). Returns 0 or -1 like gviz. */
 int gvizCudaLoadObjFile(const char *path, gvizCudaCsr *out);
 
+/* gvizGraphLoadFromGexfFile (include/utils/graphLoader.h:36-61): one vertex
+ * per <node> tag in file order (ids matched as strings, the first vertex
+ * with an id keeps it), undirected edges in <edge> tag order, with the same
+ * scanner and the same failures as gviz's loader (no <node>, a node without
+ * an id, an unterminated node or attribute table, a malformed <attvalue>,
+ * an edge whose source or target names no node). gviz also builds each
+ * vertex's JSON string of label and attribute values; the layout does not
+ * use vertex data, so none is built here (externalIds stays NULL).
+ * Returns 0 or -1 like gviz. */
+int gvizCudaLoadGexfFile(const char *path, gvizCudaCsr *out);
+
 void gvizCudaCsrFree(gvizCudaCsr *csr);
 
 /* ---- host helpers: adjacency and initial placement ------------------- */

@@ -265,6 +265,10 @@ class Reference:
         """gvizGraphLoadFromObjFile, then the adjacency as CSR (or None)."""
         return self._load_csr(self.lib.ref_load_obj_csr, str(path).encode())
 
+    def load_gexf_csr(self, path):
+        """gvizGraphLoadFromGexfFile, then the adjacency as CSR (or None)."""
+        return self._load_csr(self.lib.ref_load_gexf_csr, str(path).encode())
+
     def create_builtin(self, kind, a, b=0, density=0.0, seed=0, model=MODEL_FR):
         h = self.lib.ref_create_builtin(C.c_int(kind), C.c_size_t(a), C.c_size_t(b),
                                         D(density), C.c_uint(seed), C.c_int(model))

@@ -448,6 +448,16 @@ long long ref_load_obj_csr(const char *path, uint64_t *row, uint32_t *col, size_
   return V;
 }
 
+long long ref_load_gexf_csr(const char *path, uint64_t *row, uint32_t *col, size_t *entries) {
+  gvizGraph g;
+  if (gvizGraphLoadFromGexfFile(path, &g) < 0)
+    return -1;
+  long long V = csr_of_graph(&g, row, col, entries);
+  gvizGraphFreeVertexDataStrings(&g);
+  gvizGraphRelease(&g);
+  return V;
+}
+
 /* gviz's own text embedding load / save on the embedder's graph. */
 int ref_load_embedding(refLayout *r, const char *path) {
   return gvizEmbeddedGraphLoadEmbedding((gvizEmbeddedGraph *)&r->s, path);

@@ -1,4 +1,5 @@
-"""Graph files straight to CSR (gvizCudaLoadEdgesFile / gvizCudaLoadObjFile)
+"""Graph files straight to CSR (gvizCudaLoadEdgesFile / gvizCudaLoadObjFile /
+gvizCudaLoadGexfFile)
 against gviz's own loaders (src/utils/graphLoader.c, the reference compiled
 from its sources) followed by its adjacency order: the same vertex numbering,
 the same neighbour lists, the same failures."""
@@ -77,6 +78,8 @@ def test_missing_file(tmp_path):
         graphs.load_edges_file(tmp_path / "absent.edges")
     with pytest.raises(OSError):
         graphs.load_obj_file(tmp_path / "absent.obj")
+    with pytest.raises(OSError):
+        graphs.load_gexf_file(tmp_path / "absent.gexf")
 
 
 @pytest.mark.parametrize("case", sorted(OBJ_CASES))
@@ -111,3 +114,92 @@ def test_random_edges_file_matches_gviz(ref, tmp_path):
     row, col, ext = graphs.load_edges_file(p)
     assert np.array_equal(row, want[0]) and np.array_equal(col, want[1])
     assert ext[0] == u[0]
+
+
+GEXF_HEAD = '<?xml version="1.0" encoding="UTF-8"?>\n<gexf version="1.3">\n<graph defaultedgetype="undirected">\n'
+GEXF_TAIL = '</graph>\n</gexf>\n'
+GEXF_CASES = {
+    "path_of_four": GEXF_HEAD + '<nodes>\n<node id="n1"/>\n<node id="n2" />\n<node id="n3"/>\n'
+                    '<node id="n4"/>\n</nodes>\n<edges>\n<edge id="e1" source="n1" target="n2"/>\n'
+                    '<edge id="e2" source="n3" target="n2"/>\n<edge id="e3" source="n3" target="n4"/>\n'
+                    '</edges>\n' + GEXF_TAIL,
+    "attribute_tables": GEXF_HEAD + '<attributes class="node">\n'
+                        '<attribute id="w" title="weight" type="double"/>\n'
+                        '<attribute id="k" title="kind"/>\n</attributes>\n'
+                        '<attributes class="edge">\n<attribute title="no id here"/>\n</attributes>\n'
+                        "<nodes>\n<node id='p' label='P'>\n<attvalues>\n"
+                        '<attvalue for="w" value="2.5"/>\n<attvalue for="k" value="x &amp; y"/>\n'
+                        '</attvalues>\n</node>\n<node id="q" label="Q"></node>\n<node id="r"/>\n'
+                        '</nodes>\n<edges>\n<edge source="r" target="p" weight="3"/>\n'
+                        "<edge source='q' target='p'/>\n</edges>\n" + GEXF_TAIL,
+    "legacy_attvalue_id": GEXF_HEAD + '<nodes>\n<node id="0" label="zero">\n<attvalues>'
+                          '<attvalue id="1" value="5"/></attvalues>\n</node>\n<node id="1"/>\n'
+                          '</nodes>\n<edges><edge source="1" target="0"/></edges>\n' + GEXF_TAIL,
+    "duplicates_selfloop_isolated": GEXF_HEAD + '<nodes>\n<node id="a"/>\n<node id="b"/>\n'
+                                    '<node id="a" label="second a"/>\n<node id="c"/>\n'
+                                    '<node id="lonely"/>\n</nodes>\n<edges>\n'
+                                    '<edge source="a" target="b"/>\n<edge source="b" target="a"/>\n'
+                                    '<edge source="a" target="b"/>\n<edge source="c" target="c"/>\n'
+                                    '<edge source="c" target="a"/>\n</edges>\n' + GEXF_TAIL,
+    "attribute_substring": GEXF_HEAD + '<nodes>\n<node pid="x" id="a"/>\n<node id="b"/>\n'
+                           '</nodes>\n<edges>\n<edge source="x" target="b"/>\n</edges>\n' + GEXF_TAIL,
+    "crlf_tabs_comment": (GEXF_HEAD + '<nodes>\r\n<node\tid="u"\t/>\r\n<!-- <node id="c1"/> -->\r\n'
+                          '<node\nid="v"/>\r\n</nodes>\r\n<edges>\r\n<edge\tsource="u"\ttarget="v"/>\r\n'
+                          '<edge source="c1" target="u">\r\n</edge>\r\n</edges>\r\n' + GEXF_TAIL),
+    "edges_first": GEXF_HEAD + '<edges>\n<edge source="b" target="a"/>\n</edges>\n<nodes>\n'
+                   '<node id="a"/>\n<node id="b"/>\n</nodes>\n' + GEXF_TAIL,
+}
+GEXF_BAD = {
+    "no_nodes": GEXF_HEAD + '<nodes>\n</nodes>\n<edges>\n</edges>\n' + GEXF_TAIL,
+    "node_without_id": GEXF_HEAD + '<nodes><node label="A"/></nodes>\n' + GEXF_TAIL,
+    "unknown_target": GEXF_HEAD + '<nodes><node id="a"/></nodes><edges><edge source="a" '
+                      'target="zz"/></edges>\n' + GEXF_TAIL,
+    "edge_without_target": GEXF_HEAD + '<nodes><node id="a"/></nodes><edges><edge source="a"/>'
+                           '</edges>\n' + GEXF_TAIL,
+    "unterminated_node": GEXF_HEAD + '<nodes><node id="a"><attvalues></attvalues>\n' + GEXF_TAIL,
+    "attvalue_without_value": GEXF_HEAD + '<nodes><node id="a"><attvalues><attvalue for="0"/>'
+                              '</attvalues></node></nodes>\n' + GEXF_TAIL,
+    "unterminated_attributes": GEXF_HEAD + '<attributes class="node">\n<nodes><node id="a"/>'
+                               '</nodes>\n' + GEXF_TAIL,
+    "attribute_without_id": GEXF_HEAD + '<attributes class="node"><attribute title="t"/>'
+                            '</attributes><nodes><node id="a"/></nodes>\n' + GEXF_TAIL,
+    "id_too_long": GEXF_HEAD + '<nodes><node id="' + "x" * 300 + '"/></nodes>\n' + GEXF_TAIL,
+}
+
+
+@pytest.mark.parametrize("case", sorted(GEXF_CASES))
+def test_gexf_file_matches_gviz(ref, tmp_path, case):
+    from grapher_b200 import graphs
+    p = _write(tmp_path, case + ".gexf", GEXF_CASES[case])
+    want = ref.load_gexf_csr(p)
+    row, col = graphs.load_gexf_file(p)
+    assert want is not None
+    assert np.array_equal(row, want[0]) and np.array_equal(col, want[1])
+
+
+@pytest.mark.parametrize("case", sorted(GEXF_BAD))
+def test_gexf_file_failures_match_gviz(ref, tmp_path, case):
+    from grapher_b200 import graphs
+    p = _write(tmp_path, case + ".gexf", GEXF_BAD[case])
+    assert ref.load_gexf_csr(p) is None
+    with pytest.raises(OSError):
+        graphs.load_gexf_file(p)
+
+
+def test_random_gexf_file_matches_gviz(ref, tmp_path):
+    """A seeded 20,000-node, 60,000-edge file with string ids in shuffled
+    order, duplicates and self-loops."""
+    from grapher_b200 import graphs
+    rng = np.random.default_rng(9)
+    names = [f"node-{i:05d}" for i in rng.permutation(20000)]
+    u = rng.integers(0, 20000, 60000)
+    v = rng.integers(0, 20000, 60000)
+    body = "".join(f'<node id="{n}" label="{n.upper()}"/>\n' for n in names)
+    edges = "".join(f'<edge id="{i}" source="{names[a]}" target="{names[b]}"/>\n'
+                    for i, (a, b) in enumerate(zip(u, v)))
+    p = _write(tmp_path, "rand.gexf", GEXF_HEAD + "<nodes>\n" + body + "</nodes>\n<edges>\n"
+               + edges + "</edges>\n" + GEXF_TAIL)
+    want = ref.load_gexf_csr(p)
+    row, col = graphs.load_gexf_file(p)
+    assert np.array_equal(row, want[0]) and np.array_equal(col, want[1])
+    assert len(row) == 20001 and len(col) == 120000
