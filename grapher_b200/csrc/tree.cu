@@ -22,6 +22,8 @@
 // (mass == 0, :38-39).
 #include <math.h>
 
+#include <algorithm>
+
 #include <cuda/atomic>
 
 #include "internal.cuh"
@@ -30,7 +32,6 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ uint32_t ld_u32(const uint32_t *p) { return __ldcg(p); }
 
 // ---------------------------------------------------------------------------
 // bounding boxes and roots
@@ -413,6 +414,9 @@ struct BU {
   // second central moments {Qxx, Qxy, Qyy, -}, or null: summed and shifted
   // in FP64, stored in FP32 (they only feed FP32 features)
   float4 *bQ, *nQ;
+  // nodes spanning blocks whose children are both summed when k_bottom_up
+  // ends (counts[4] of them)
+  uint32_t *ready;
   uint32_t V, k;
 };
 
@@ -463,25 +467,101 @@ __device__ __forceinline__ uint2 *up_of(const BU &a, uint32_t c) {
   return (c & GVIZ_LEAF_BIT) ? a.upLeaf + (c & ~GVIZ_LEAF_BIT) : a.upInt + c;
 }
 
+// Node p from its children l, r (left first: fixed order, deterministic
+// sums): mass, mass-weighted position sums, point count, subtree size in
+// emitted records, the absorbed (p shares its quadtree level with its parent
+// pp) and collapsed (a capacity leaf) flags and its children's preorder link
+// weights; with kQ the second moments about p's centre of mass.
+template <bool kQ>
+__device__ __forceinline__ void combine(const BU &a, uint32_t p, int dp, uint32_t pp, int dpp,
+                                        uint32_t l, uint32_t r, double Ml, double SXl,
+                                        double SYl, uint32_t cl, uint32_t Tl, float4 ql,
+                                        double Mr, double SXr, double SYr, uint32_t cr,
+                                        uint32_t Tr, float4 qr, double &M, double &SX,
+                                        double &SY, uint32_t &cnt, uint32_t &T,
+                                        float4 &q) {
+  M = Ml + Mr;
+  SX = SXl + SXr;
+  SY = SYl + SYr;
+  cnt = cl + cr;
+  const bool absorbed = pp != GVIZ_NONE && dpp >= 32 && ((dp - 32) >> 1) == ((dpp - 32) >> 1);
+  const bool collapsed = !absorbed && cnt <= a.k;
+  T = absorbed ? Tl + Tr : (collapsed ? 1u + cnt : 1u + Tl + Tr);
+  if (kQ) {
+    double px = 0.0, py = 0.0;
+    if (M > 1e-9 || M < -1e-9) {
+      const double im = __drcp_rn(M);  // one reciprocal on the serial climb
+      px = SX * im;
+      py = SY * im;
+    }
+    q = make_float4(0.f, 0.f, 0.f, 0.f);
+    add_shifted(q, ql, Ml, SXl, SYl, px, py);
+    add_shifted(q, qr, Mr, SXr, SYr, px, py);
+    a.nQ[p] = q;
+  }
+  a.nM[p] = M;
+  a.nSX[p] = SX;
+  a.nSY[p] = SY;
+  a.nCnt[p] = cnt;
+  a.nT[p] = T;
+  a.nFlag[p] = (absorbed ? 1u : 0u) | (collapsed ? 2u : 0u);
+  const uint32_t base = absorbed ? 0u : 1u;
+  const uint32_t dead = collapsed ? 0x80000000u : 0u;
+  up_of(a, l)->y = base | dead;
+  up_of(a, r)->y = (base + Tl) | dead;
+}
+
+// Per-block shared state of k_bottom_up: the sums of the block's buckets
+// [B0, B1) (slot b - B0), the sums of its in-block internal nodes (slot
+// p - B0; a Karras node is one end of its own range, so an internal node
+// whose bucket range lies in [B0, B1) has its index there too) and the shape
+// of the internal nodes [B0, B1), loaded once and coalesced.
+template <bool kQ>
+struct BUShared {
+  uint32_t arrive[kThreads];
+  double lM[kThreads], lSX[kThreads], lSY[kThreads];
+  double iM[kThreads], iSX[kThreads], iSY[kThreads];
+  uint32_t lCnt[kThreads], lT[kThreads], iCnt[kThreads], iT[kThreads];
+  uint32_t left[kThreads], right[kThreads], first[kThreads], last[kThreads], up[kThreads];
+  int32_t delta[kThreads];
+  float4 lQ[kQ ? kThreads : 1], iQ[kQ ? kThreads : 1];
+};
+
 // Sums per bucket, then each thread climbs; the second child to arrive at a
 // node combines both (left first: fixed order, deterministic sums). A node
 // whose buckets all belong to this block has both children summed by
 // threads of this block: its arrivals meet in shared memory with block-scope
-// ordering; only nodes spanning blocks pay for device-scope ordering.
+// ordering and its children's sums are read from shared memory. A climb
+// stops at the first node spanning blocks: its arrivals use a device-scope
+// counter, and the second one lists the node for k_bottom_up_top. (A block
+// that carried its climbs to the root stayed resident for ~20 device-scope
+// steps, and the kernel ran in several such waves.) Every node's sums also
+// go to global memory (k_emit reads them).
+template <bool kQ>
 __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
-  __shared__ uint32_t sArrive[kThreads];
-  sArrive[threadIdx.x] = 0u;
-  __syncthreads();
+  __shared__ BUShared<kQ> s;
   const uint32_t U = a.counts[2];
   const uint32_t B0 = blockIdx.x * kThreads;
   const uint32_t B1 = min(B0 + kThreads, U);
-  const uint32_t b = B0 + threadIdx.x;
+  const uint32_t tid = threadIdx.x;
+  s.arrive[tid] = 0u;
+  if (B0 + tid + 1 < U) {  // internal nodes are [0, U - 1)
+    const uint32_t p = B0 + tid;
+    s.left[tid] = a.nLeft[p];
+    s.right[tid] = a.nRight[p];
+    s.first[tid] = a.nFirst[p];
+    s.last[tid] = a.nLast[p];
+    s.up[tid] = a.upInt[p].x;
+    s.delta[tid] = a.nDelta[p];
+  }
+  __syncthreads();
+  const uint32_t b = B0 + tid;
   if (b >= U) return;
   const uint32_t start = a.bStart[b];
   const uint32_t end = (b + 1 < U) ? a.bStart[b + 1] : a.V;
   double M = 0.0, SX = 0.0, SY = 0.0;
-  for (uint32_t s = start; s < end; s++) {
-    uint32_t i = a.idx[s];
+  for (uint32_t j = start; j < end; j++) {
+    uint32_t i = a.idx[j];
     double m = a.mass[i];
     double2 p = a.pos[i];
     M += m;
@@ -490,15 +570,15 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
   }
   uint32_t cnt = end - start;
   uint32_t T = cnt == 1 ? 1u : 1u + cnt;
-  if (a.bQ) {
+  if (kQ) {
     double cx = 0.0, cy = 0.0;
     if (M > 1e-9 || M < -1e-9) {
       cx = SX / M;
       cy = SY / M;
     }
     double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
-    for (uint32_t s = start; s < end; s++) {
-      const uint32_t i = a.idx[s];
+    for (uint32_t j = start; j < end; j++) {
+      const uint32_t i = a.idx[j];
       const double m = a.mass[i];
       const double2 p = a.pos[i];
       const double dx = p.x - cx, dy = p.y - cy;
@@ -506,80 +586,161 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       q.y += m * dx * dy;
       q.z += m * dy * dy;
     }
-    a.bQ[b] = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+    const float4 fq = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+    a.bQ[b] = fq;
+    s.lQ[tid] = fq;
   }
   a.bM[b] = M;
   a.bSX[b] = SX;
   a.bSY[b] = SY;
   a.bCnt[b] = cnt;
   a.bT[b] = T;
+  s.lM[tid] = M;
+  s.lSX[tid] = SX;
+  s.lSY[tid] = SY;
+  s.lCnt[tid] = cnt;
+  s.lT[tid] = T;
   const uint32_t g = a.bGid[b];
   uint32_t x = b | GVIZ_LEAF_BIT;
-  uint32_t p = up_of(a, x)->x;
+  uint32_t p = a.upLeaf[b].x;
   for (int guard = 0;; guard++) {
     if (guard > GVIZ_MAX_CLIMB) {
       atomicOr(a.status, GVIZ_ST_TREE);
       return;
     }
-    const int dp = p == GVIZ_NONE ? 0 : a.nDelta[p];
+    const bool pin = p >= B0 && p < B1;  // false for GVIZ_NONE
+    const int dp = p == GVIZ_NONE ? 0 : (pin ? s.delta[p - B0] : a.nDelta[p]);
     if (p == GVIZ_NONE || dp < 32) {
       a.rootNode[g] = x;
       a.rootT[g] = T;
       *up_of(a, x) = make_uint2(GVIZ_NONE, 0u);
       return;
     }
-    // p's shape comes from the previous kernel: fetch all of it (and the
-    // grandparent's level) before waiting on the arrival
-    const uint32_t l = a.nLeft[p], r = a.nRight[p];
-    const uint32_t first = a.nFirst[p], last = a.nLast[p];
-    const uint32_t pp = a.upInt[p].x;
-    const int dpp = pp == GVIZ_NONE ? 0 : a.nDelta[pp];
-    // release this child's sums / acquire the sibling's: the second thread
-    // to arrive combines both (Karras node p is one end of its own range,
-    // so an in-block node has p in [B0, B1))
-    if (p >= B0 && p < B1 && first >= B0 && last < B1) {
-      cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrivals(sArrive[p - B0]);
-      if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
-    } else {
+    if (!pin || s.first[p - B0] < B0 || s.last[p - B0] >= B1) {
+      // a node spanning blocks: k_bottom_up_top sums it once both children
+      // are summed
       cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrivals(a.nCounter[p]);
       if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
       a.nCounter[p] = 0u;
+      a.ready[atomicAdd(const_cast<uint32_t *>(a.counts) + 4, 1u)] = p;
+      return;
     }
+    const uint32_t l = s.left[p - B0], r = s.right[p - B0], pp = s.up[p - B0];
+    const int dpp = pp == GVIZ_NONE ? 0
+                    : ((pp >= B0 && pp < B1) ? s.delta[pp - B0] : a.nDelta[pp]);
+    // release this child's sums / acquire the sibling's: the second thread
+    // to arrive combines both, reading them from shared memory (both
+    // children lie in [B0, B1) and were summed by this block)
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrivals(s.arrive[p - B0]);
+    if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) return;
     double Ml, SXl, SYl, Mr, SXr, SYr;
     uint32_t cl, Tl, cr, Tr;
-    child_vals(a, l, Ml, SXl, SYl, cl, Tl);
-    child_vals(a, r, Mr, SXr, SYr, cr, Tr);
-    M = Ml + Mr;
-    SX = SXl + SXr;
-    SY = SYl + SYr;
-    cnt = cl + cr;
-    const bool absorbed = pp != GVIZ_NONE && dpp >= 32 && ((dp - 32) >> 1) == ((dpp - 32) >> 1);
-    const bool collapsed = !absorbed && cnt <= a.k;
-    T = absorbed ? Tl + Tr : (collapsed ? 1u + cnt : 1u + Tl + Tr);
-    if (a.nQ) {
-      double px = 0.0, py = 0.0;
-      if (M > 1e-9 || M < -1e-9) {
-        const double im = __drcp_rn(M);  // one reciprocal on the serial climb
-        px = SX * im;
-        py = SY * im;
-      }
-      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-      add_shifted(q, child_q(a, l), Ml, SXl, SYl, px, py);
-      add_shifted(q, child_q(a, r), Mr, SXr, SYr, px, py);
-      a.nQ[p] = q;
+    float4 ql = make_float4(0.f, 0.f, 0.f, 0.f), qr = ql;
+    if (l & GVIZ_LEAF_BIT) {
+      const uint32_t c = (l & ~GVIZ_LEAF_BIT) - B0;
+      Ml = s.lM[c], SXl = s.lSX[c], SYl = s.lSY[c], cl = s.lCnt[c], Tl = s.lT[c];
+      if (kQ) ql = s.lQ[c];
+    } else {
+      const uint32_t c = l - B0;
+      Ml = s.iM[c], SXl = s.iSX[c], SYl = s.iSY[c], cl = s.iCnt[c], Tl = s.iT[c];
+      if (kQ) ql = s.iQ[c];
     }
-    a.nM[p] = M;
-    a.nSX[p] = SX;
-    a.nSY[p] = SY;
-    a.nCnt[p] = cnt;
-    a.nT[p] = T;
-    a.nFlag[p] = (absorbed ? 1u : 0u) | (collapsed ? 2u : 0u);
-    const uint32_t base = absorbed ? 0u : 1u;
-    const uint32_t dead = collapsed ? 0x80000000u : 0u;
-    up_of(a, l)->y = base | dead;
-    up_of(a, r)->y = (base + Tl) | dead;
+    if (r & GVIZ_LEAF_BIT) {
+      const uint32_t c = (r & ~GVIZ_LEAF_BIT) - B0;
+      Mr = s.lM[c], SXr = s.lSX[c], SYr = s.lSY[c], cr = s.lCnt[c], Tr = s.lT[c];
+      if (kQ) qr = s.lQ[c];
+    } else {
+      const uint32_t c = r - B0;
+      Mr = s.iM[c], SXr = s.iSX[c], SYr = s.iSY[c], cr = s.iCnt[c], Tr = s.iT[c];
+      if (kQ) qr = s.iQ[c];
+    }
+    float4 q;
+    combine<kQ>(a, p, dp, pp, dpp, l, r, Ml, SXl, SYl, cl, Tl, ql, Mr, SXr, SYr, cr, Tr, qr,
+                M, SX, SY, cnt, T, q);
+    const uint32_t c = p - B0;  // an in-block parent reads the sums from here
+    s.iM[c] = M;
+    s.iSX[c] = SX;
+    s.iSY[c] = SY;
+    s.iCnt[c] = cnt;
+    s.iT[c] = T;
+    if (kQ) s.iQ[c] = q;
     x = p;
     p = pp;
+  }
+}
+
+// The nodes spanning blocks, from those whose children k_bottom_up summed:
+// each thread takes one listed node, sums it from its children's sums and
+// climbs on while it arrives second (device-scope counters; the first
+// arrival may have come from k_bottom_up). The climb's critical path is the
+// tree's depth above the blocks (~20 levels at 1M points), so each level
+// issues the next level's shape loads before its arrival and reads only
+// the sibling's sums (the climbing child's are in registers). A persistent
+// grid: the list is short (~3 % of the nodes at 1M points).
+template <bool kQ>
+__global__ __launch_bounds__(kThreads) void k_bottom_up_top(BU a) {
+  const uint32_t nReady = a.counts[4];
+  for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < nReady;
+       i += gridDim.x * kThreads) {
+    uint32_t p = a.ready[i];
+    // p's shape (p is no root sentinel: k_bottom_up checked it)
+    int dp = a.nDelta[p];
+    uint32_t l = a.nLeft[p], r = a.nRight[p], pp = a.upInt[p].x;
+    int dpp = pp == GVIZ_NONE ? 0 : a.nDelta[pp];
+    // the climbing child's sums (none for a listed node: both are read)
+    uint32_t x = GVIZ_NONE, T = 0, cnt = 0;
+    double M = 0.0, SX = 0.0, SY = 0.0;
+    float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int guard = 0;; guard++) {
+      if (guard > GVIZ_MAX_CLIMB) {
+        atomicOr(a.status, GVIZ_ST_TREE);
+        break;
+      }
+      // the next level's shape, fetched while this level waits
+      const bool nextIn = pp != GVIZ_NONE && dpp >= 32;
+      uint32_t l2 = 0, r2 = 0, ppp = GVIZ_NONE;
+      if (nextIn) {
+        l2 = a.nLeft[pp];
+        r2 = a.nRight[pp];
+        ppp = a.upInt[pp].x;
+      }
+      if (x != GVIZ_NONE) {
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrivals(a.nCounter[p]);
+        if (arrivals.fetch_add(1u, cuda::memory_order_acq_rel) == 0u) break;
+        a.nCounter[p] = 0u;
+      }
+      double Ml, SXl, SYl, Mr, SXr, SYr;
+      uint32_t cl, Tl, cr, Tr;
+      float4 ql = make_float4(0.f, 0.f, 0.f, 0.f), qr = ql;
+      if (x == l) {
+        Ml = M, SXl = SX, SYl = SY, cl = cnt, Tl = T, ql = q;
+      } else {
+        child_vals(a, l, Ml, SXl, SYl, cl, Tl);
+        if (kQ) ql = child_q(a, l);
+      }
+      if (x == r) {
+        Mr = M, SXr = SX, SYr = SY, cr = cnt, Tr = T, qr = q;
+      } else {
+        child_vals(a, r, Mr, SXr, SYr, cr, Tr);
+        if (kQ) qr = child_q(a, r);
+      }
+      combine<kQ>(a, p, dp, pp, dpp, l, r, Ml, SXl, SYl, cl, Tl, ql, Mr, SXr, SYr, cr, Tr, qr,
+                  M, SX, SY, cnt, T, q);
+      x = p;
+      if (!nextIn) {  // x is its graph's root
+        const uint32_t g = a.bGid[a.nFirst[x]];
+        a.rootNode[g] = x;
+        a.rootT[g] = T;
+        *up_of(a, x) = make_uint2(GVIZ_NONE, 0u);
+        break;
+      }
+      p = pp;
+      dp = dpp;
+      l = l2;
+      r = r2;
+      pp = ppp;
+      dpp = pp == GVIZ_NONE ? 0 : a.nDelta[pp];
+    }
   }
 }
 
@@ -620,6 +781,9 @@ struct EM {
   uint32_t *leafPre;
   uint32_t *cellCnt;  // per cell: points below it (null unless requested)
   uint4 *kids;        // per cell: its children's preorder slots (null unless requested)
+  // per internal node (k_pre_top): its preorder position without the graph
+  // base if it spans blocks of k_bottom_up, else kPreLocal
+  const uint32_t *preTop;
 };
 
 __device__ __forceinline__ void put_count(const EM &a, uint32_t at, uint32_t c) {
@@ -799,62 +963,53 @@ __device__ __forceinline__ int quad_parent_depth(const EM &a, uint32_t p) {
   return p == GVIZ_NONE ? -1 : ((a.nDelta[p] - 32) >> 1);
 }
 
-__global__ __launch_bounds__(kThreads) void k_emit(EM a) {
-  const uint32_t U = a.counts[2];
-  const uint32_t t = blockIdx.x * kThreads + threadIdx.x;
-  const uint32_t nInt = U - 1;
-  if (t < nInt) {
-    const uint32_t p = t;
-    if (a.nDelta[p] < 32 || (a.nFlag[p] & 1u)) return;
-    uint32_t pre, dead;
-    walk_up(a.upInt[p], a.upInt, pre, dead);
-    if (dead) return;
-    const uint32_t fb = a.nFirst[p];
-    const uint32_t g = a.bGid[fb];
-    pre += a.graphBase[g];
-    const GraphRoot R = a.roots[g];
-    if (a.nFlag[p] & 2u) {  // capacity leaf: wrapper + points in vertex order
-      const uint32_t lb = a.nLast[p];
-      const uint32_t s0 = a.bStart[fb];
-      const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
-      put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], INFINITY,
-               pre + a.nT[p]);
-      put_count(a, pre, s1 - s0);
-      put_kids_run(a, pre, s1 - s0);
-      uint32_t ids[GVIZ_MAX_NODES_PER_CELL];
-      uint32_t c = s1 - s0;
-      for (uint32_t j = 0; j < c; j++) {
-        uint32_t v = a.idx[s0 + j];
-        uint32_t q = j;
-        while (q > 0 && ids[q - 1] > v) {
-          ids[q] = ids[q - 1];
-          q--;
-        }
-        ids[q] = v;
-      }
-      for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, ids[j]);
-      return;
-    }
-    const int q = (a.nDelta[p] - 32) >> 1;
-    put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], ldexp(R.h0, -q),
+// The records of internal node p (a quadtree cell or a capacity leaf) at
+// preorder position pre (without the graph base).
+__device__ void emit_internal(const EM &a, uint32_t U, uint32_t p, uint32_t pre) {
+  const uint32_t fb = a.nFirst[p];
+  const uint32_t g = a.bGid[fb];
+  pre += a.graphBase[g];
+  const GraphRoot R = a.roots[g];
+  if (a.nFlag[p] & 2u) {  // capacity leaf: wrapper + points in vertex order
+    const uint32_t lb = a.nLast[p];
+    const uint32_t s0 = a.bStart[fb];
+    const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
+    put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], INFINITY,
              pre + a.nT[p]);
-    put_kids_quad(a, pre, p);
-    if (a.cells) {
-      const uint32_t lb = a.nLast[p];
-      const uint32_t s0 = a.bStart[fb];
-      const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
-      put_far(a, pre, R, fb, q, ldexp(R.h0, -q), a.nQ[p], a.nM[p], a.nSX[p],
-              a.nSY[p], s0, s1);
-      put_count(a, pre, s1 - s0);
+    put_count(a, pre, s1 - s0);
+    put_kids_run(a, pre, s1 - s0);
+    uint32_t ids[GVIZ_MAX_NODES_PER_CELL];
+    uint32_t c = s1 - s0;
+    for (uint32_t j = 0; j < c; j++) {
+      uint32_t v = a.idx[s0 + j];
+      uint32_t q = j;
+      while (q > 0 && ids[q - 1] > v) {
+        ids[q] = ids[q - 1];
+        q--;
+      }
+      ids[q] = v;
     }
+    for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, ids[j]);
     return;
   }
-  const uint32_t b = t - nInt;
-  if (t < nInt || b >= U) return;
-  uint32_t pre, dead;
+  const int q = (a.nDelta[p] - 32) >> 1;
+  put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], ldexp(R.h0, -q),
+           pre + a.nT[p]);
+  put_kids_quad(a, pre, p);
+  if (a.cells) {
+    const uint32_t lb = a.nLast[p];
+    const uint32_t s0 = a.bStart[fb];
+    const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
+    put_far(a, pre, R, fb, q, ldexp(R.h0, -q), a.nQ[p], a.nM[p], a.nSX[p],
+            a.nSY[p], s0, s1);
+    put_count(a, pre, s1 - s0);
+  }
+}
+
+// The records of bucket b (a point, or the points of one smallest cell
+// behind a wrapper cell) at preorder position pre (without the graph base).
+__device__ void emit_bucket(const EM &a, uint32_t U, uint32_t b, uint32_t pre) {
   const uint2 ub = a.upLeaf[b];
-  walk_up(ub, a.upInt, pre, dead);
-  if (dead) return;
   const uint32_t g = a.bGid[b];
   pre += a.graphBase[g];
   const uint32_t c = a.bCnt[b];
@@ -874,6 +1029,96 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
     put_far(a, pre, R, b, R.D - 1, h, a.bQ[b], a.bM[b], a.bSX[b], a.bSY[b], s0,
             s0 + c);
   for (uint32_t j = 0; j < c; j++) put_leaf(a, pre + 1 + j, a.idx[s0 + j]);
+}
+
+// A node's preorder position relative to its graph's base is the sum of the
+// link weights up to the graph's root. k_pre_top stores it for every internal
+// node spanning blocks (GVIZ_NONE below a capacity leaf) and kPreLocal for
+// the others, so a walk up stops at the first ancestor spanning blocks.
+constexpr uint32_t kPreLocal = 0xFFFFFFFEu;
+
+__device__ __forceinline__ bool spans_blocks(uint32_t p, uint32_t first, uint32_t last,
+                                             uint32_t U) {
+  const uint32_t B0 = p & ~(uint32_t)(kThreads - 1);
+  return first < B0 || last >= min(B0 + kThreads, U);
+}
+
+__global__ __launch_bounds__(kThreads) void k_pre_top(const EM a) {
+  const uint32_t U = a.counts[2];
+  const uint32_t p = blockIdx.x * kThreads + threadIdx.x;
+  if (p + 1 >= U) return;  // internal nodes are [0, U - 1)
+  if (a.nDelta[p] < 32 || !spans_blocks(p, a.nFirst[p], a.nLast[p], U)) {
+    const_cast<uint32_t *>(a.preTop)[p] = kPreLocal;
+    return;
+  }
+  uint32_t pre, dead;
+  walk_up(a.upInt[p], a.upInt, pre, dead);  // its ancestors all span blocks
+  const_cast<uint32_t *>(a.preTop)[p] = dead ? GVIZ_NONE : pre;
+}
+
+// Shared by the threads of one k_emit block: parent links and k_pre_top's
+// entries of the internal nodes [C0, C0 + kEmitSpan).
+constexpr uint32_t kEmitSpan = kThreads / 2;
+struct EmitShared {
+  uint2 up[kEmitSpan];
+  uint32_t pre[kEmitSpan];
+};
+
+// Preorder position (without the graph base) of the node whose parent link
+// is u: the link weights summed up to the first ancestor spanning blocks,
+// whose own position k_pre_top wrote. dead: an ancestor is a capacity leaf.
+__device__ __forceinline__ uint32_t emit_pre(const EM &a, const EmitShared &s, uint32_t C0,
+                                             uint2 u, bool &dead) {
+  uint32_t pre = 0;
+  dead = false;
+  for (int guard = 0; u.x != GVIZ_NONE; guard++) {
+    if (guard > GVIZ_MAX_CLIMB || (u.y >> 31)) {  // the guard is never expected
+      dead = true;
+      return 0;
+    }
+    pre += u.y;
+    const uint32_t x = u.x;
+    const bool cached = x - C0 < kEmitSpan;
+    const uint32_t t = cached ? s.pre[x - C0] : a.preTop[x];
+    if (t != kPreLocal) {
+      if (t == GVIZ_NONE) dead = true;
+      return pre + t;
+    }
+    u = cached ? s.up[x - C0] : a.upInt[x];
+  }
+  return pre;
+}
+
+// Node and leaf records in preorder: block j emits internal nodes and
+// buckets [C0, C0 + kEmitSpan), C0 = kEmitSpan j, one per thread.
+__global__ __launch_bounds__(kThreads) void k_emit(EM a) {
+  __shared__ EmitShared s;
+  const uint32_t U = a.counts[2];
+  const uint32_t nInt = U - 1;
+  const uint32_t C0 = blockIdx.x * kEmitSpan;
+  if (C0 >= U) return;
+  const uint32_t i = threadIdx.x % kEmitSpan;
+  const uint32_t t = C0 + i;
+  if (threadIdx.x < kEmitSpan && t < nInt) {
+    s.up[i] = a.upInt[t];
+    s.pre[i] = a.preTop[t];
+  }
+  __syncthreads();
+  if (threadIdx.x < kEmitSpan) {
+    if (t < nInt && a.nDelta[t] >= 32 && !(a.nFlag[t] & 1u)) {
+      bool dead;
+      uint32_t pre = s.pre[i];
+      if (pre == kPreLocal)
+        pre = emit_pre(a, s, C0, s.up[i], dead);
+      else
+        dead = pre == GVIZ_NONE;
+      if (!dead) emit_internal(a, U, t, pre);
+    }
+  } else if (t < U) {
+    bool dead;
+    const uint32_t pre = emit_pre(a, s, C0, a.upLeaf[t], dead);
+    if (!dead) emit_bucket(a, U, t, pre);
+  }
 }
 
 // Target groups of the learned cell-group walk: every cell of at most
@@ -1110,6 +1355,7 @@ EM make_em(gvizCudaForce *h) {
   a.nLeft = h->d_nLeft;
   a.nRight = h->d_nRight;
   a.kids = a.f64 ? nullptr : h->d_kids;  // the FP32 walks expand cells by them
+  a.preTop = nullptr;
   return a;
 }
 
@@ -1194,10 +1440,23 @@ void enqueue_tree_build(gvizCudaForce *h) {
   bu.k = h->params.nodesPerCell;
   bu.bQ = h->farSide ? h->d_bQ : nullptr;
   bu.nQ = h->farSide ? h->d_nQ : nullptr;
-  k_bottom_up<<<blocks_for(V), kThreads, 0, st>>>(bu);
+  // free after the buckets: the list of nodes spanning blocks, and the
+  // preorder positions of k_pre_top
+  bu.ready = h->d_flag;
+  // the nodes spanning blocks are a few percent of the buckets: one wave
+  const uint32_t topBlocks = std::max(1u, std::min<uint32_t>(blocks_for(V), 148u * 4u));
+  if (bu.bQ) {
+    k_bottom_up<true><<<blocks_for(V), kThreads, 0, st>>>(bu);
+    k_bottom_up_top<true><<<topBlocks, kThreads, 0, st>>>(bu);
+  } else {
+    k_bottom_up<false><<<blocks_for(V), kThreads, 0, st>>>(bu);
+    k_bottom_up_top<false><<<topBlocks, kThreads, 0, st>>>(bu);
+  }
   scan_exclusive(h, h->d_rootT, h->d_graphBase, h->G, h->d_counts + 3);
   EM em = make_em(h);
-  k_emit<<<blocks_for(2 * (size_t)V), kThreads, 0, st>>>(em);
+  em.preTop = h->d_scan;
+  k_pre_top<<<blocks_for(V), kThreads, 0, st>>>(em);
+  k_emit<<<(uint32_t)((V + kEmitSpan - 1) / kEmitSpan), kThreads, 0, st>>>(em);
   if (em.cellCnt && !em.f64) {
     GroupArgs ga;
     ga.nodes = reinterpret_cast<const NodeF *>(h->d_nodes);
