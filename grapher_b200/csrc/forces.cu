@@ -1586,10 +1586,18 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
           for (int k = 0; k < kExactTpt; k++) {
             const float dx = (f.x - vxh[k]) + (f.z - vxl[k]);
             const float dy = (f.y - vyh[k]) + (f.w - vyl[k]);
-            float sc = w * rcp_approx_ftz(dx * dx + dy * dy);
-            if (MODEL != GVIZ_CUDA_MODEL_FR) sc *= mv[k];
+            const float sc = w * rcp_approx_ftz(dx * dx + dy * dy);
             px[k] = fmaf(-sc, dx, px[k]);
             py[k] = fmaf(-sc, dy, py[k]);
+          }
+        }
+        // LinLog's target mass is common to the chunk's terms: one multiply
+        // per chunk instead of one per pair
+        if (MODEL != GVIZ_CUDA_MODEL_FR) {
+#pragma unroll
+          for (int k = 0; k < kExactTpt; k++) {
+            px[k] *= mv[k];
+            py[k] *= mv[k];
           }
         }
         bool bad = false;
@@ -1838,7 +1846,7 @@ static void launch_far_hubs(gvizCudaForce *h, const FarHubArgs &ha) {
   k_walk_f32_hubs<MODEL, OVERLAP><<<need < fill ? need : fill, kHubThreads, 0, h->stream>>>(ha);
 }
 
-static void enqueue_far_hubs(gvizCudaForce *h, const WalkArgs &a) {
+static FarHubArgs far_hub_args(gvizCudaForce *h, const WalkArgs &a) {
   FarHubArgs ha;
   ha.w = a;
   ha.hubs = h->d_farHubs;
@@ -1847,6 +1855,10 @@ static void enqueue_far_hubs(gvizCudaForce *h, const WalkArgs &a) {
   ha.nHubs = h->nFarHubs;
   const double r = h->params.theta / h->params.farHubTheta;
   ha.sizeScale = (float)(r * r);
+  return ha;
+}
+
+static void enqueue_far_hub_walk(gvizCudaForce *h, const FarHubArgs &ha) {
   const bool ov = h->params.preventOverlap != 0;
   if (h->model == GVIZ_CUDA_MODEL_FR) {
     if (ov) launch_far_hubs<GVIZ_CUDA_MODEL_FR, true>(h, ha);
@@ -1855,17 +1867,38 @@ static void enqueue_far_hubs(gvizCudaForce *h, const WalkArgs &a) {
     if (ov) launch_far_hubs<GVIZ_CUDA_MODEL_LINLOG, true>(h, ha);
     else launch_far_hubs<GVIZ_CUDA_MODEL_LINLOG, false>(h, ha);
   }
-  prof_mark(h, "bh_walk_hubs");
-  k_far_hub_epilogue<<<blocks(h->nFarHubs, 256), 256, 0, h->stream>>>(ha);
 }
 
 static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters);
 
 // The learned walk (see k_walk_f32_far and k_walk_f32_cells), then the hub
-// targets' plain walk when params.farHubTargets asks for one.
+// targets' plain walk when params.farHubTargets asks for one. The hub walk
+// reads only the tree and the positions and writes its own buffer, so with a
+// side stream it runs beside the learned walk (in order while profiling, so
+// that each kernel keeps its own time); the hubs' epilogues, which replace
+// the learned walk's forces of those vertices, wait for both.
 static void enqueue_far(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters) {
-  enqueue_far_walk(h, a, counters);
-  if (h->nFarHubs > 0 && h->d_farHubs) enqueue_far_hubs(h, a);
+  if (!(h->nFarHubs > 0 && h->d_farHubs)) {
+    enqueue_far_walk(h, a, counters);
+    return;
+  }
+  const FarHubArgs ha = far_hub_args(h, a);
+  cudaStream_t st = h->stream;
+  if (h->side && !h->profiling) {
+    cudaEventRecord(h->evFork, st);
+    cudaStreamWaitEvent(h->side, h->evFork, 0);
+    h->stream = h->side;
+    enqueue_far_hub_walk(h, ha);
+    h->stream = st;
+    cudaEventRecord(h->evJoin, h->side);
+    enqueue_far_walk(h, a, counters);
+    cudaStreamWaitEvent(st, h->evJoin, 0);
+  } else {
+    enqueue_far_walk(h, a, counters);
+    enqueue_far_hub_walk(h, ha);
+    prof_mark(h, "bh_walk_hubs");
+  }
+  k_far_hub_epilogue<<<blocks(h->nFarHubs, 256), 256, 0, st>>>(ha);
 }
 
 static void enqueue_far_walk(gvizCudaForce *h, const WalkArgs &a, uint64_t *counters) {

@@ -888,19 +888,21 @@ __device__ void put_cell(const EM &a, uint32_t at, double M, double SX,
   }
 }
 
-__device__ void put_leaf(const EM &a, uint32_t at, uint32_t v) {
+// Point v's leaf record at preorder slot `at`, from its position, mass and
+// radius.
+__device__ void put_leaf_vals(const EM &a, uint32_t at, uint32_t v, double2 p, double m,
+                              double r) {
   if (at >= a.maxNodes) {
     atomicOr(a.status, GVIZ_ST_TREE);
     return;
   }
   if (a.leafPre) a.leafPre[v] = at;
-  double2 p = a.pos[v];
   if (a.f64) {
     NodeD n;
     n.x = p.x;
     n.y = p.y;
-    n.mass = a.mass[v];
-    n.size = a.radius[v];
+    n.mass = m;
+    n.size = r;
     n.next = (int32_t)(at + 1);
     n.info = (int32_t)v;
     n.pad0 = n.pad1 = 0;
@@ -909,12 +911,16 @@ __device__ void put_leaf(const EM &a, uint32_t at, uint32_t v) {
     NodeF n;
     ds_split(p.x, n.xh, n.xl);
     ds_split(p.y, n.yh, n.yl);
-    n.mass = (float)a.mass[v];
-    n.size = (float)a.radius[v];
+    n.mass = (float)m;
+    n.size = (float)r;
     n.next = (int32_t)(at + 1);
     n.info = (int32_t)v;
     reinterpret_cast<NodeF *>(a.nodes)[at] = n;
   }
+}
+
+__device__ void put_leaf(const EM &a, uint32_t at, uint32_t v) {
+  put_leaf_vals(a, at, v, a.pos[v], a.mass[v], a.radius[v]);
 }
 
 // Children of a cell for walks that expand several cells at once (a cell's
@@ -965,17 +971,15 @@ __device__ __forceinline__ int quad_parent_depth(const EM &a, uint32_t p) {
 
 // The records of internal node p (a quadtree cell or a capacity leaf) at
 // preorder position pre (without the graph base).
-__device__ void emit_internal(const EM &a, uint32_t U, uint32_t p, uint32_t pre) {
-  const uint32_t fb = a.nFirst[p];
-  const uint32_t g = a.bGid[fb];
-  pre += a.graphBase[g];
+__device__ void emit_internal(const EM &a, uint32_t U, uint32_t p, uint32_t pre,
+                              uint32_t fb, uint32_t g, double M, double SX, double SY,
+                              uint32_t T) {
   const GraphRoot R = a.roots[g];
   if (a.nFlag[p] & 2u) {  // capacity leaf: wrapper + points in vertex order
     const uint32_t lb = a.nLast[p];
     const uint32_t s0 = a.bStart[fb];
     const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
-    put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], INFINITY,
-             pre + a.nT[p]);
+    put_cell(a, pre, M, SX, SY, INFINITY, pre + T);
     put_count(a, pre, s1 - s0);
     put_kids_run(a, pre, s1 - s0);
     uint32_t ids[GVIZ_MAX_NODES_PER_CELL];
@@ -993,31 +997,21 @@ __device__ void emit_internal(const EM &a, uint32_t U, uint32_t p, uint32_t pre)
     return;
   }
   const int q = (a.nDelta[p] - 32) >> 1;
-  put_cell(a, pre, a.nM[p], a.nSX[p], a.nSY[p], ldexp(R.h0, -q),
-           pre + a.nT[p]);
+  put_cell(a, pre, M, SX, SY, ldexp(R.h0, -q), pre + T);
   put_kids_quad(a, pre, p);
   if (a.cells) {
     const uint32_t lb = a.nLast[p];
     const uint32_t s0 = a.bStart[fb];
     const uint32_t s1 = (lb + 1 < U) ? a.bStart[lb + 1] : a.V;
-    put_far(a, pre, R, fb, q, ldexp(R.h0, -q), a.nQ[p], a.nM[p], a.nSX[p],
-            a.nSY[p], s0, s1);
+    put_far(a, pre, R, fb, q, ldexp(R.h0, -q), a.nQ[p], M, SX, SY, s0, s1);
     put_count(a, pre, s1 - s0);
   }
 }
 
 // The records of bucket b (a point, or the points of one smallest cell
 // behind a wrapper cell) at preorder position pre (without the graph base).
-__device__ void emit_bucket(const EM &a, uint32_t U, uint32_t b, uint32_t pre) {
-  const uint2 ub = a.upLeaf[b];
-  const uint32_t g = a.bGid[b];
-  pre += a.graphBase[g];
-  const uint32_t c = a.bCnt[b];
-  const uint32_t s0 = a.bStart[b];
-  if (c == 1) {
-    put_leaf(a, pre, a.idx[s0]);
-    return;
-  }
+__device__ void emit_bucket(const EM &a, uint32_t U, uint32_t b, uint32_t pre, uint2 ub,
+                            uint32_t g, uint32_t c, uint32_t s0) {
   const GraphRoot R = a.roots[g];
   const int qp = quad_parent_depth(a, ub.x);
   const bool testable = c > a.k && qp < R.D - 1;
@@ -1104,20 +1098,42 @@ __global__ __launch_bounds__(kThreads) void k_emit(EM a) {
     s.pre[i] = a.preTop[t];
   }
   __syncthreads();
+  // each record's inputs are loaded before the walk up, whose end (the
+  // preorder position) only the stores need
   if (threadIdx.x < kEmitSpan) {
     if (t < nInt && a.nDelta[t] >= 32 && !(a.nFlag[t] & 1u)) {
+      const uint32_t fb = a.nFirst[t];
+      const double M = a.nM[t], SX = a.nSX[t], SY = a.nSY[t];
+      const uint32_t T = a.nT[t];
+      const uint32_t g = a.bGid[fb];
+      const uint32_t base = a.graphBase[g];
       bool dead;
       uint32_t pre = s.pre[i];
       if (pre == kPreLocal)
         pre = emit_pre(a, s, C0, s.up[i], dead);
       else
         dead = pre == GVIZ_NONE;
-      if (!dead) emit_internal(a, U, t, pre);
+      if (!dead) emit_internal(a, U, t, pre + base, fb, g, M, SX, SY, T);
     }
   } else if (t < U) {
+    const uint2 ub = a.upLeaf[t];
+    const uint32_t g = a.bGid[t], c = a.bCnt[t], s0 = a.bStart[t];
+    const uint32_t base = a.graphBase[g];
+    const uint32_t v = a.idx[s0];  // the point of a single-point bucket
+    double2 pv = make_double2(0.0, 0.0);
+    double mv = 0.0, rv = 0.0;
+    if (c == 1) {
+      pv = a.pos[v];
+      mv = a.mass[v];
+      rv = a.radius[v];
+    }
     bool dead;
-    const uint32_t pre = emit_pre(a, s, C0, a.upLeaf[t], dead);
-    if (!dead) emit_bucket(a, U, t, pre);
+    const uint32_t pre = emit_pre(a, s, C0, ub, dead);
+    if (dead) return;
+    if (c == 1)
+      put_leaf_vals(a, pre + base, v, pv, mv, rv);
+    else
+      emit_bucket(a, U, t, pre + base, ub, g, c, s0);
   }
 }
 
