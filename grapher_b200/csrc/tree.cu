@@ -576,8 +576,10 @@ __global__ __launch_bounds__(kThreads) void k_bottom_up(BU a) {
       cx = SX / M;
       cy = SY / M;
     }
+    // a single point has no second moments about itself: the bucket's own
+    // pass over its points runs only for two or more
     double4 q = make_double4(0.0, 0.0, 0.0, 0.0);
-    for (uint32_t j = start; j < end; j++) {
+    for (uint32_t j = start; cnt > 1u && j < end; j++) {
       const uint32_t i = a.idx[j];
       const double m = a.mass[i];
       const double2 p = a.pos[i];
