@@ -1,8 +1,9 @@
 """bench.learned_setup's choice of the learned configuration, on a fake
 layout (no GPU): each hub-target candidate runs at its own largest theta
-whose error is not above the plain walk's, the fastest candidate wins, a
-fixed --hub-targets count is kept, and layouts up to 2^20 vertices are
-judged on every vertex (a 65,536-vertex sample above)."""
+whose error is not above the plain walk's, the fastest candidate that
+reaches theta 1.2 wins (the fastest of all when none does), a fixed
+--hub-targets count is kept, and layouts up to 2^20 vertices are judged on
+every vertex (a 65,536-vertex sample above)."""
 import types
 
 import numpy as np
@@ -102,7 +103,9 @@ def test_candidates_take_their_largest_qualifying_theta(fake_training):
 
 def test_fastest_candidate_wins(fake_training):
     _, info = _setup(1 << 16)
-    best = min(info["candidates"], key=lambda c: c["ms_per_step"])
+    at_target = [c for c in info["candidates"] if c["theta"] >= bench.TARGET_THETA]
+    assert at_target
+    best = min(at_target, key=lambda c: c["ms_per_step"])
     assert info["hub_targets"] == best["hub_targets"]
     assert info["learned_theta"] == best["theta"]
     p = bench.learned_params(info)
@@ -121,3 +124,12 @@ def test_every_vertex_judged_up_to_2_pow_20(fake_training):
     assert info["judge_vertices"] == 1 << 20 and lay.judged == 1 << 20
     lay, info = _setup((1 << 20) + 1)
     assert info["judge_vertices"] == bench.JUDGE_VERTICES == lay.judged
+
+
+def test_candidates_reaching_the_target_theta_are_preferred():
+    c = [{"hub_targets": 0, "theta": 1.1, "ms_per_step": 1.70},
+         {"hub_targets": 1024, "theta": 1.175, "ms_per_step": 1.72},
+         {"hub_targets": 4096, "theta": 1.2, "ms_per_step": 1.74},
+         {"hub_targets": 16384, "theta": 1.25, "ms_per_step": 1.80}]
+    assert bench.pick_candidate(c) == 4096
+    assert bench.pick_candidate(c[:2]) == 0  # none reaches it: the fastest
