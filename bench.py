@@ -276,7 +276,7 @@ NCU_TRAFFIC = {
                             "profiles/learned_walk_ba1m.md (theta 1.2, 4096 hub targets)"),
     "bh_walk_f32": ("ba1m_learned", 613.3e6 + 169.9e6,
                     "profiles/plain_walk_ba1m.md (theta 0.5)"),
-    "exact_f32": ("er65k_exact", 1.358e6 + 0.0, "profiles/exact_er65k.md"),
+    "exact_f32": ("er65k_exact", 1.356e6 + 0.0, "profiles/exact_er65k.md"),
     "k_grip_pass1": ("grip_ba200k", 121.1e6 + 8.4e6, "profiles/grip_round_ba200k.md"),
 }
 

@@ -50,7 +50,7 @@ __device__ __forceinline__ float rcp_approx_ftz(float x) {
 constexpr int kExactThreads = 128;
 constexpr int kExactTile = 128;
 constexpr int kExactTpt = 4;     // exact mode: targets per thread
-constexpr int kExactChunk = 32;  // exact mode: sources per plain partial sum
+constexpr int kExactChunk = 64;  // exact mode: sources per plain partial sum
 constexpr uint32_t kInf = 0xffffffffu;
 
 struct Kahan {
@@ -1503,6 +1503,7 @@ template <int MODEL, bool OVERLAP>
 __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
   __shared__ float4 sp[kExactTile];
   __shared__ float2 sm[kExactTile];
+  __shared__ float sw[kExactTile];  // the source's share of the optimistic term's numerator
   __shared__ uint32_t sRange[2];
   uint32_t v[kExactTpt], gb[kExactTpt], ge[kExactTpt];
   bool act[kExactTpt];
@@ -1552,7 +1553,9 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
       ds_split(q.x, f.x, f.z);
       ds_split(q.y, f.y, f.w);
       sp[threadIdx.x] = f;
-      sm[threadIdx.x] = make_float2(a.massF[j], OVERLAP ? a.radiusF[j] : 0.f);
+      const float m = a.massF[j];
+      sm[threadIdx.x] = make_float2(m, OVERLAP ? a.radiusF[j] : 0.f);
+      sw[threadIdx.x] = MODEL == GVIZ_CUDA_MODEL_FR ? a.num * truncf(m) : m;
     }
     __syncthreads();
     const uint32_t cnt = min((uint32_t)kExactTile, hi - t0);
@@ -1581,7 +1584,7 @@ __global__ __launch_bounds__(kExactThreads) void k_exact_f32(ExactArgs a) {
 #pragma unroll 4
         for (uint32_t q = c0; q < c1; q++) {
           const float4 f = sp[q];
-          const float w = MODEL == GVIZ_CUDA_MODEL_FR ? a.num * truncf(sm[q].x) : sm[q].x;
+          const float w = sw[q];
 #pragma unroll
           for (int k = 0; k < kExactTpt; k++) {
             const float dx = (f.x - vxh[k]) + (f.z - vxl[k]);
