@@ -11,7 +11,7 @@ seed 7). Setup (untimed, in the FP64 path so that the judged state does not
 depend on FP32 rounding): 20 plain steps at theta = 0.5, then four snapshots
 of this layout (iterations 20, 25, 30, 30) from which pairs are harvested for
 32,768 sampled vertices each at theta = 0.7, 0.95, 1.2 and 1.05; the
-far-field MLP is trained on them on the GPU (40 epochs with a step-decayed
+far-field MLP is trained on them on the GPU (320 epochs with a step-decayed
 learning rate, reported as train_s), and the state of iteration 30 is judged
 and timed. Force error is the
 normalised RMS of the repulsion against exact FP64 all-pairs repulsion on
@@ -474,7 +474,7 @@ TARGET_THETA = 1.2       # candidates reaching it are preferred (see pick_candid
 HARVEST_TARGETS = 32768  # sampled target vertices per training snapshot
 # Adam passes over the harvested pairs as (epochs, learning rate): a step
 # decay; the optimiser's moments carry over from one stage to the next
-TRAIN_SCHEDULE = ((24, 2e-3), (10, 6e-4), (6, 2e-4))
+TRAIN_SCHEDULE = ((192, 2e-3), (80, 6e-4), (48, 2e-4))
 # The learned comparison starts from a fixed point of the layout, whatever
 # --warmup asks for: LEARNED_PRE_STEPS plain steps from the initial
 # positions, then the harvest snapshots of HARVEST_SCHEDULE, all in the FP64
