@@ -272,8 +272,8 @@ class ClockSampler:
 # dram__bytes_write.sum, one capture each), reported as roofline.traffic on the
 # workload the capture ran: kernel -> (workload, bytes, capture)
 NCU_TRAFFIC = {
-    "bh_walk_f32_learned": ("ba1m_learned", 678.2e6 + 188.8e6,
-                            "profiles/learned_walk_ba1m.md (theta 1.2, 4096 hub targets)"),
+    "bh_walk_f32_learned": ("ba1m_learned", 685.8e6 + 187.2e6,
+                            "profiles/learned_walk_ba1m.md (theta 1.225, 1024 hub targets)"),
     "bh_walk_f32": ("ba1m_learned", 613.3e6 + 169.9e6,
                     "profiles/plain_walk_ba1m.md (theta 0.5)"),
     "exact_f32": ("er65k_exact", 1.356e6 + 0.0, "profiles/exact_er65k.md"),
