@@ -168,28 +168,24 @@ __global__ __launch_bounds__(kThreads) void k_keys(
   idx[i] = i;
 }
 
+// The sorted points' full paths, and the starts of runs of equal composite
+// keys (the sorted bits of the composite key).
 __global__ __launch_bounds__(kThreads) void k_gather_keys(
     const uint32_t *__restrict__ idx, const uint64_t *__restrict__ keyHi,
-    const uint64_t *__restrict__ keyLo, uint64_t *sHi, uint64_t *sLo,
-    uint32_t V) {
+    const uint64_t *__restrict__ keyLo, const uint64_t *__restrict__ ck, uint64_t *sHi,
+    uint64_t *sLo, uint32_t *flag, uint32_t V) {
   uint32_t s = blockIdx.x * kThreads + threadIdx.x;
   if (s >= V) return;
   uint32_t i = idx[s];
   sHi[s] = keyHi[i];
   sLo[s] = keyLo[i];
+  flag[s] = (s == 0 || (ck[s] >> GVIZ_SORT_SKIP_BITS) !=
+                           (ck[s - 1] >> GVIZ_SORT_SKIP_BITS)) ? 1u : 0u;
 }
 
 // ---------------------------------------------------------------------------
 // runs of equal composite keys
 // ---------------------------------------------------------------------------
-
-__global__ __launch_bounds__(kThreads) void k_run_flags(
-    const uint64_t *__restrict__ ck, uint32_t *flag, uint32_t V) {
-  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
-  if (s >= V) return;
-  flag[s] = (s == 0 || (ck[s] >> GVIZ_SORT_SKIP_BITS) !=
-                           (ck[s - 1] >> GVIZ_SORT_SKIP_BITS)) ? 1u : 0u;
-}
 
 __global__ __launch_bounds__(kThreads) void k_run_starts(
     const uint32_t *__restrict__ flag, const uint32_t *__restrict__ scan,
@@ -334,47 +330,77 @@ __global__ __launch_bounds__(kThreads) void k_bucket_fill(
 }
 
 // Common-prefix length in bits of the composite keys (graph id:32,
-// path:128) of buckets a and b; -1 outside [0, U).
-__device__ __forceinline__ int bdelta(int a, int b, int U,
-                                      const uint64_t *__restrict__ bHi,
-                                      const uint64_t *__restrict__ bLo,
-                                      const uint32_t *__restrict__ bGid) {
-  if (b < 0 || b >= U) return -1;
-  uint32_t gx = bGid[a] ^ bGid[b];
-  if (gx) return __clz(gx);
-  uint64_t x = bHi[a] ^ bHi[b];
+// path:128) of buckets a and b; -1 outside [0, U). Keys of buckets
+// [T0, T0 + kKarrasTile) come from the block's shared-memory copy; bGid is
+// null for a single graph (every graph id is 0).
+constexpr int kKarrasTile = 3 * kThreads;
+
+struct KarrasKeys {
+  const uint64_t *bHi, *bLo;
+  const uint32_t *bGid;
+  const uint64_t *sHi, *sLo;  // shared copies of [T0, T0 + kKarrasTile)
+  int T0, U;
+  __device__ __forceinline__ uint64_t hi(int b) const {
+    return (unsigned)(b - T0) < (unsigned)kKarrasTile ? sHi[b - T0] : bHi[b];
+  }
+  __device__ __forceinline__ uint64_t lo(int b) const {
+    return (unsigned)(b - T0) < (unsigned)kKarrasTile ? sLo[b - T0] : bLo[b];
+  }
+};
+
+__device__ __forceinline__ int bdelta(int a, int b, const KarrasKeys &k) {
+  if (b < 0 || b >= k.U) return -1;
+  if (k.bGid) {
+    uint32_t gx = k.bGid[a] ^ k.bGid[b];
+    if (gx) return __clz(gx);
+  }
+  uint64_t x = k.hi(a) ^ k.hi(b);
   if (x) return 32 + __clzll(x);
-  x = bLo[a] ^ bLo[b];
+  x = k.lo(a) ^ k.lo(b);
   if (x) return 96 + __clzll(x);
   return 160;
 }
 
 // Karras, "Maximizing parallelism in the construction of BVHs, octrees and
 // k-d trees" (HPG 2012), algorithm of section 4 over unique bucket keys.
+// Block j finds nodes [256 j, 256 j + 256); the keys of the 256 buckets on
+// either side are staged in shared memory first, where most of the
+// searches stay.
 __global__ __launch_bounds__(kThreads) void k_karras(
     const uint64_t *__restrict__ bHi, const uint64_t *__restrict__ bLo,
     const uint32_t *__restrict__ bGid, const uint32_t *__restrict__ counts,
     uint32_t *nLeft, uint32_t *nRight, uint32_t *nFirst, uint32_t *nLast,
     int32_t *nDelta, uint2 *upInt, uint2 *upLeaf) {
+  __shared__ uint64_t sHi[kKarrasTile], sLo[kKarrasTile];
   const int U = (int)counts[2];
-  const int i = blockIdx.x * kThreads + threadIdx.x;
+  const int B0 = (int)(blockIdx.x * kThreads);
+  if (B0 >= U - 1) return;
+  KarrasKeys k{bHi, bLo, bGid, sHi, sLo, B0 - kThreads, U};
+  for (int j = threadIdx.x; j < kKarrasTile; j += kThreads) {
+    const int b = k.T0 + j;
+    if (b >= 0 && b < U) {
+      sHi[j] = bHi[b];
+      sLo[j] = bLo[b];
+    }
+  }
+  __syncthreads();
+  const int i = B0 + threadIdx.x;
   if (i >= U - 1) return;
-  const int dir = (bdelta(i, i + 1, U, bHi, bLo, bGid) -
-                   bdelta(i, i - 1, U, bHi, bLo, bGid)) >= 0 ? 1 : -1;
-  const int dmin = bdelta(i, i - dir, U, bHi, bLo, bGid);
+  const int dir = (bdelta(i, i + 1, k) - bdelta(i, i - 1, k)) >= 0 ? 1 : -1;
+  const int dmin = bdelta(i, i - dir, k);
   int lmax = 2;
-  while (bdelta(i, i + lmax * dir, U, bHi, bLo, bGid) > dmin) lmax <<= 1;
+  while (bdelta(i, i + lmax * dir, k) > dmin) lmax <<= 1;
   int l = 0;
   for (int t = lmax >> 1; t >= 1; t >>= 1)
-    if (bdelta(i, i + (l + t) * dir, U, bHi, bLo, bGid) > dmin) l += t;
+    if (bdelta(i, i + (l + t) * dir, k) > dmin) l += t;
   const int j = i + l * dir;
-  const int dnode = bdelta(i, j, U, bHi, bLo, bGid);
+  const int dnode = bdelta(i, j, k);
   int s = 0;
   int div = 2;
   int t;
   do {
     t = (l + div - 1) / div;
-    if (bdelta(i, i + (s + t) * dir, U, bHi, bLo, bGid) > dnode) s += t;
+    if (bdelta(i, i + (s + t) * dir, k) > dnode) s += t;
     div <<= 1;
   } while (t > 1);
   const int gamma = i + s * dir + min(dir, 0);
@@ -1400,10 +1426,9 @@ void enqueue_tree_build(gvizCudaForce *h) {
                                              h->d_idx, V, h->gbits);
   prof_mark(h, "tree_keys");
   radix_sort_pairs(h, h->d_ck, h->d_idx, h->d_ckAlt, h->d_idxAlt, V);
-  k_gather_keys<<<blocks_for(V), kThreads, 0, st>>>(h->d_idx, h->d_keyHi,
-                                                    h->d_keyLo, h->d_sHi,
-                                                    h->d_sLo, V);
-  k_run_flags<<<blocks_for(V), kThreads, 0, st>>>(h->d_ck, h->d_flag, V);
+  k_gather_keys<<<blocks_for(V), kThreads, 0, st>>>(h->d_idx, h->d_keyHi, h->d_keyLo,
+                                                    h->d_ck, h->d_sHi, h->d_sLo,
+                                                    h->d_flag, V);
   scan_exclusive(h, h->d_flag, h->d_scan, V, h->d_counts + 0);
   k_run_starts<<<blocks_for(V), kThreads, 0, st>>>(h->d_flag, h->d_scan,
                                                    h->d_runStart, V);
@@ -1423,7 +1448,7 @@ void enqueue_tree_build(gvizCudaForce *h) {
       h->d_bStart, h->d_bHi, h->d_bLo, h->d_bGid, h->d_upLeaf, V);
   prof_mark(h, "tree_buckets");
   k_karras<<<blocks_for(V), kThreads, 0, st>>>(
-      h->d_bHi, h->d_bLo, h->d_bGid, h->d_counts, h->d_nLeft, h->d_nRight,
+      h->d_bHi, h->d_bLo, h->G > 1 ? h->d_bGid : nullptr, h->d_counts, h->d_nLeft, h->d_nRight,
       h->d_nFirst, h->d_nLast, h->d_nDelta, h->d_upInt, h->d_upLeaf);
   BU bu;
   bu.idx = h->d_idx;
