@@ -9,8 +9,12 @@
 //   stable radix sort of (graph, path) -> fix-up sort of equal-prefix runs
 //   buckets = identical full paths -> Karras binary radix tree (2012)
 //   binary nodes merged into quadtree nodes (two path bits per level)
-//   bottom-up mass / centre-of-mass / subtree sizes (atomic counters)
-//   preorder index by walking up weighted parent links -> node records
+//   bottom-up mass / centre-of-mass / subtree sizes (arrival counters):
+//     inside blocks of 256 buckets through shared memory, then the few
+//     nodes spanning blocks on a persistent grid
+//   preorder index of the spanning nodes by walking up weighted parent
+//   links, then every node record, its own walk up stopping at the first
+//   spanning ancestor
 //
 // Why the compressed tree walks like the reference's: a chain of single-child
 // nodes shares one point set, hence one mass and centre of mass; the
