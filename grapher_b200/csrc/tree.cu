@@ -811,7 +811,7 @@ struct EM {
   const uint64_t *bHi, *bLo;
   FarCell *cells;
   uint32_t *leafPre;
-  uint32_t *cellCnt;  // per cell: points below it (null unless requested)
+  uint32_t *cellCnt;  // per record: points below it, 1 for a point (null unless requested)
   uint4 *kids;        // per cell: its children's preorder slots (null unless requested)
   // per internal node (k_pre_top): its preorder position without the graph
   // base if it spans blocks of k_bottom_up, else kPreLocal
@@ -929,6 +929,7 @@ __device__ void put_leaf_vals(const EM &a, uint32_t at, uint32_t v, double2 p, d
     return;
   }
   if (a.leafPre) a.leafPre[v] = at;
+  put_count(a, at, 1u);  // every record has its point count: k_far_groups reads it first
   if (a.f64) {
     NodeD n;
     n.x = p.x;
@@ -1221,8 +1222,7 @@ __global__ __launch_bounds__(kThreads) void k_far_groups(GroupArgs a) {
     if (g < a.G) {
       const uint32_t r = a.graphBase[g], T = a.rootT[g];
       if (T != 0 && r < total) {
-        const int4 l = node_link(a.nodes, r);
-        const uint32_t c = l.w >= 0 ? 1u : a.cellCnt[r];
+        const uint32_t c = a.cellCnt[r];
         if (c <= kGroupMax) {
           px[0] = r;
           py[0] = min(r + T, total);
@@ -1231,9 +1231,9 @@ __global__ __launch_bounds__(kThreads) void k_far_groups(GroupArgs a) {
         }
       }
     }
-  } else if (t < total) {
+  } else if (t < total && a.cellCnt[t] > kGroupMax) {  // (a point's count is 1)
     const int4 l = node_link(a.nodes, t);
-    if (l.w < 0 && a.cellCnt[t] > kGroupMax) {
+    {
       const uint32_t end = min(max((uint32_t)l.z, t + 1u), total);
       uint32_t chX[4], chY[4], chC[4], chQ[4];
       int nc = 0;
@@ -1248,8 +1248,7 @@ __global__ __launch_bounds__(kThreads) void k_far_groups(GroupArgs a) {
           if (kk[i] > t && kk[i] < end) chX[nc++] = kk[i];
         for (int i = 0; i < nc; i++) {
           chY[i] = i + 1 < nc ? chX[i + 1] : end;
-          const int4 m = node_link(a.nodes, chX[i]);
-          chC[i] = m.w >= 0 ? 1u : a.cellCnt[chX[i]];
+          chC[i] = a.cellCnt[chX[i]];
         }
       }
       if (bucket) {  // points of one smallest cell: runs of kGroupMax leaves
