@@ -133,7 +133,6 @@ void free_all(gvizCudaForce *h) {
   dfree(h->d_sLo);
   dfree(h->d_flag);
   dfree(h->d_scan);
-  dfree(h->d_runStart);
   dfree(h->d_deepRuns);
   dfree(h->d_counts);
   dfree(h->d_sortState);
@@ -705,7 +704,6 @@ int gvizCudaForceCreate(gvizCudaForce **out, const gvizCudaGraphDesc *g) {
   rc |= dalloc(h, &h->d_sLo, Vs);
   rc |= dalloc(h, &h->d_flag, Vs);
   rc |= dalloc(h, &h->d_scan, Vs);
-  rc |= dalloc(h, &h->d_runStart, Vs);
   rc |= dalloc(h, &h->d_deepRuns, 2 * Vs);
   rc |= dalloc(h, &h->d_counts, 8);
   rc |= dalloc(h, &h->d_sortState, sort_state_entries(Vs));

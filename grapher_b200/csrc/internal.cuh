@@ -162,7 +162,7 @@ struct gvizCudaForce {
   uint32_t *d_idx = nullptr, *d_idxAlt = nullptr;   // sorted vertex ids
   uint64_t *d_sHi = nullptr, *d_sLo = nullptr;      // full keys, sorted order
   uint32_t *d_flag = nullptr, *d_scan = nullptr;    // V-sized
-  uint32_t *d_runStart = nullptr, *d_deepRuns = nullptr;
+  uint32_t *d_deepRuns = nullptr;
   uint32_t *d_counts = nullptr;  // [0]=runs [1]=deep runs [2]=buckets [3]=nodes
   uint64_t *d_sortState = nullptr;  // radix sort: look-back status, digit counts, tickets
   uint64_t *d_scanState = nullptr;  // scan: ticket and look-back status

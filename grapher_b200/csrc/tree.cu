@@ -191,26 +191,41 @@ __global__ __launch_bounds__(kThreads) void k_gather_keys(
 // runs of equal composite keys
 // ---------------------------------------------------------------------------
 
-__global__ __launch_bounds__(kThreads) void k_run_starts(
-    const uint32_t *__restrict__ flag, const uint32_t *__restrict__ scan,
-    uint32_t *runStart, uint32_t V) {
-  uint32_t s = blockIdx.x * kThreads + threadIdx.x;
-  if (s >= V) return;
-  if (flag[s]) runStart[scan[s]] = s;
-}
-
-// Runs longer than the leaf capacity k need their deeper digits sorted;
-// runs of 2..k points lie in one leaf, so their keys are cut to the common
-// prefix (the leaf keeps them in vertex order, as the reference does).
-__global__ __launch_bounds__(kThreads) void k_run_classify(
-    const uint32_t *__restrict__ runStart, uint32_t *counts, uint32_t *deep,
-    uint64_t *sHi, uint64_t *sLo, uint32_t V, uint32_t k, int gbits) {
-  uint32_t r = blockIdx.x * kThreads + threadIdx.x;
-  uint32_t nRuns = counts[0];
-  if (r >= nRuns) return;
-  uint32_t start = runStart[r];
-  uint32_t end = (r + 1 < nRuns) ? runStart[r + 1] : V;
-  uint32_t len = end - start;
+// Runs of equal composite keys (equal sorted prefixes). The thread at a
+// run's start finds its end, the first later key whose sorted prefix
+// differs, by a galloping search over the sorted keys (most runs are one
+// key long, found by the first probe). Runs longer than the leaf capacity k
+// need their deeper digits sorted; runs of 2..k points lie in one leaf, so
+// their keys are cut to the common prefix (the leaf keeps them in vertex
+// order, as the reference does).
+__global__ __launch_bounds__(kThreads) void k_runs(
+    const uint64_t *__restrict__ ck, const uint32_t *__restrict__ flag, uint32_t *counts,
+    uint32_t *deep, uint64_t *sHi, uint64_t *sLo, uint32_t V, uint32_t k, int gbits) {
+  const uint32_t start = blockIdx.x * kThreads + threadIdx.x;
+  if (start >= V || !flag[start]) return;
+  const uint64_t key = ck[start] >> GVIZ_SORT_SKIP_BITS;
+  uint32_t end = start + 1u;
+  if (end < V && (ck[end] >> GVIZ_SORT_SKIP_BITS) == key) {
+    uint32_t lo = end, hi = V;  // ck[lo] is in the run, the end is in (lo, hi]
+    for (uint32_t step = 1u;; step <<= 1) {
+      const uint32_t probe = lo + step;
+      if (probe >= V || probe < lo) break;
+      if ((ck[probe] >> GVIZ_SORT_SKIP_BITS) != key) {
+        hi = probe;
+        break;
+      }
+      lo = probe;
+    }
+    while (hi - lo > 1u) {
+      const uint32_t mid = lo + (hi - lo) / 2u;
+      if ((ck[mid] >> GVIZ_SORT_SKIP_BITS) == key)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    end = hi;
+  }
+  const uint32_t len = end - start;
   if (len > k) {
     uint32_t slot = atomicAdd(&counts[1], 1u);
     deep[2 * slot] = start;
@@ -219,9 +234,9 @@ __global__ __launch_bounds__(kThreads) void k_run_classify(
     // path bits covered by the sorted prefix of the composite key
     const int covered = 64 - GVIZ_SORT_SKIP_BITS - gbits;
     const uint64_t mask = covered >= 64 ? ~0ull : (~0ull << (64 - covered));
-    for (uint32_t s = start; s < end; s++) {
-      sHi[s] &= mask;
-      sLo[s] = 0;
+    for (uint32_t j = start; j < end; j++) {
+      sHi[j] &= mask;
+      sLo[j] = 0;
     }
   }
 }
@@ -1432,12 +1447,9 @@ void enqueue_tree_build(gvizCudaForce *h) {
   k_gather_keys<<<blocks_for(V), kThreads, 0, st>>>(h->d_idx, h->d_keyHi, h->d_keyLo,
                                                     h->d_ck, h->d_sHi, h->d_sLo,
                                                     h->d_flag, V);
-  scan_exclusive(h, h->d_flag, h->d_scan, V, h->d_counts + 0);
-  k_run_starts<<<blocks_for(V), kThreads, 0, st>>>(h->d_flag, h->d_scan,
-                                                   h->d_runStart, V);
-  k_run_classify<<<blocks_for(V), kThreads, 0, st>>>(
-      h->d_runStart, h->d_counts, h->d_deepRuns, h->d_sHi, h->d_sLo, V,
-      h->params.nodesPerCell, h->gbits);
+  k_runs<<<blocks_for(V), kThreads, 0, st>>>(h->d_ck, h->d_flag, h->d_counts, h->d_deepRuns,
+                                             h->d_sHi, h->d_sLo, V, h->params.nodesPerCell,
+                                             h->gbits);
   const size_t fixSmem = (size_t)GVIZ_FIX_MAX * 20;
   k_sort_runs<<<148, 512, fixSmem, st>>>(h->d_sHi, h->d_sLo, h->d_idx,
                                           h->d_deepRuns, h->d_counts,
