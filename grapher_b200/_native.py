@@ -135,6 +135,7 @@ _SIGS = {
     "gvizCudaForceGetFa2State": (C.c_int, [P, DP, DP, DP]),
     "gvizCudaForceStep": (D, [P, C.POINTER(StepStats)]),
     "gvizCudaForceStepHost": (D, [P, DP, C.POINTER(StepStats)]),
+    "gvizCudaForceRunHost": (D, [P, DP, C.c_uint32, C.POINTER(StepStats)]),
     "gvizCudaForceEnqueueSteps": (C.c_int, [P, C.c_uint32]),
     "gvizCudaForceSynchronize": (C.c_int, [P]),
     "gvizCudaForceRun": (C.c_int, [P, SZ, D, U64P]),

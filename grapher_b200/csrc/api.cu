@@ -820,6 +820,13 @@ void gvizCudaForceDestroy(gvizCudaForce *h) {
   free_all(h);
   mlp_free(h);
   far_side_free(h);
+  if (h->upload) {
+    cudaStreamSynchronize(h->upload);
+    cudaStreamDestroy(h->upload);
+  }
+  if (h->evUp) cudaEventDestroy(h->evUp);
+  for (int c = 0; c < GVIZ_HOST_PIECES; c++)
+    if (h->evDown[c]) cudaEventDestroy(h->evDown[c]);
   if (h->side) {
     cudaStreamSynchronize(h->side);
     cudaStreamDestroy(h->side);
@@ -1001,6 +1008,81 @@ double gvizCudaForceStepHost(gvizCudaForce *h, double *xy,
     return (double)set_err(h, GVIZ_CUDA_ERR_CUDA);
   rc = sync_and_check(h);
   h->hostIteration++;
+  double md = fill_stats(h, stats);
+  return rc ? (double)rc : md;
+}
+
+// Streams and events of gvizCudaForceRunHost, made once per handle.
+static int host_pipeline(gvizCudaForce *h) {
+  if (h->upload) return GVIZ_CUDA_OK;
+  cudaStream_t up = nullptr;
+  if (cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking) != cudaSuccess)
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  bool ok = cudaEventCreateWithFlags(&h->evUp, cudaEventDisableTiming) == cudaSuccess;
+  for (int c = 0; ok && c < GVIZ_HOST_PIECES; c++)
+    ok = cudaEventCreateWithFlags(&h->evDown[c], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    if (h->evUp) cudaEventDestroy(h->evUp);
+    h->evUp = nullptr;
+    for (int c = 0; c < GVIZ_HOST_PIECES; c++) {
+      if (h->evDown[c]) cudaEventDestroy(h->evDown[c]);
+      h->evDown[c] = nullptr;
+    }
+    cudaStreamDestroy(up);
+    return set_err(h, GVIZ_CUDA_ERR_CUDA);
+  }
+  h->upload = up;
+  return GVIZ_CUDA_OK;
+}
+
+double gvizCudaForceRunHost(gvizCudaForce *h, double *xy, uint32_t steps,
+                            gvizCudaStepStats *stats) {
+  if (!h || (!xy && h->V)) return (double)GVIZ_CUDA_ERR_ARG;
+  if (!h->begun) return (double)set_err(h, GVIZ_CUDA_ERR_NOT_BEGUN);
+  DeviceGuard guard(h->device);
+  if (steps == 0) {
+    int rc = sync_and_check(h);
+    return rc ? (double)rc : fill_stats(h, stats);
+  }
+  if (h->V == 0) {
+    double md = 0.0;
+    for (uint32_t k = 0; k < steps; k++) {
+      md = gvizCudaForceStep(h, stats);
+      if (md < 0) return md;
+    }
+    return md;
+  }
+  int rc = host_pipeline(h);
+  if (rc) return (double)rc;
+  const size_t doubles = 2 * h->V;
+  const size_t piece = (doubles + GVIZ_HOST_PIECES - 1) / GVIZ_HOST_PIECES;
+  bool ok = cudaMemcpyAsync(h->d_pos, xy, doubles * 8, cudaMemcpyHostToDevice, h->stream) ==
+            cudaSuccess;
+  double *dpos = reinterpret_cast<double *>(h->d_pos);
+  for (uint32_t k = 0; ok && k < steps; k++) {
+    rc = launch_steps(h, 1);
+    if (rc) return (double)rc;
+    const bool again = k + 1 < steps;
+    for (int c = 0; ok && c < GVIZ_HOST_PIECES; c++) {
+      const size_t off = (size_t)c * piece;
+      if (off >= doubles) break;
+      const size_t n = std::min(piece, doubles - off);
+      ok = cudaMemcpyAsync(xy + off, dpos + off, n * 8, cudaMemcpyDeviceToHost, h->stream) ==
+           cudaSuccess;
+      if (ok && again) {  // the next step's upload of this piece, once it is back
+        ok = cudaEventRecord(h->evDown[c], h->stream) == cudaSuccess &&
+             cudaStreamWaitEvent(h->upload, h->evDown[c], 0) == cudaSuccess &&
+             cudaMemcpyAsync(dpos + off, xy + off, n * 8, cudaMemcpyHostToDevice,
+                             h->upload) == cudaSuccess;
+      }
+    }
+    if (ok && again)
+      ok = cudaEventRecord(h->evUp, h->upload) == cudaSuccess &&
+           cudaStreamWaitEvent(h->stream, h->evUp, 0) == cudaSuccess;
+  }
+  if (!ok) return (double)set_err(h, GVIZ_CUDA_ERR_CUDA);
+  rc = sync_and_check(h);
+  h->hostIteration += steps;
   double md = fill_stats(h, stats);
   return rc ? (double)rc : md;
 }

@@ -17,6 +17,7 @@
 #define GVIZ_HEAVY_DEGREE 16     // attraction: warp per vertex above this
 #define GVIZ_HUB_DEGREE 4096  // above: split across warps (attraction)
 #define GVIZ_HUB_CHUNK 2048   // adjacency entries per hub chunk
+#define GVIZ_HOST_PIECES 8    // gvizCudaForceRunHost: pieces of the positions per copy
 constexpr uint32_t kWalkDefaultThreads = 128;  // walk block size before autotuning
 // The radix sort orders the top 48 bits of the composite (graph, path) key:
 // 24 quadtree levels of one graph. Runs equal in those bits and longer than
@@ -85,6 +86,10 @@ struct gvizCudaForce {
   // and joined back to `stream` around the tree build (null: in order)
   cudaStream_t side = nullptr;
   cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  // gvizCudaForceRunHost: the uploads' stream and its events (made at its
+  // first call)
+  cudaStream_t upload = nullptr;
+  cudaEvent_t evDown[GVIZ_HOST_PIECES] = {}, evUp = nullptr;
   bool ownStream = false;
   int model = 0;
   size_t V = 0, E2 = 0, G = 1;

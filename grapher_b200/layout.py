@@ -197,6 +197,16 @@ class ForceLayout:
         self.last_stats = st
         return md
 
+    def run_host(self, xy, steps):
+        """`steps` end-to-end steps over a host position buffer (updated in
+        place after every step; copies pipelined across steps)."""
+        st = (N.StepStats * self.G)()
+        md = self.L.gvizCudaForceRunHost(self.h, N.ptr(xy, C.c_double), steps, st)
+        if md < 0:
+            N.check(int(md), "gvizCudaForceRunHost")
+        self.last_stats = st
+        return md
+
     def enqueue_steps(self, n):
         N.check(self.L.gvizCudaForceEnqueueSteps(self.h, n), "gvizCudaForceEnqueueSteps")
 

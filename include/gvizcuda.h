@@ -172,6 +172,21 @@ double gvizCudaForceStep(gvizCudaForce *h, gvizCudaStepStats *stats);
 double gvizCudaForceStepHost(gvizCudaForce *h, double *xy,
                              gvizCudaStepStats *stats);
 
+/* `steps` steps end to end over host memory, like as many gvizCudaForceStepHost
+ * calls: before every step the positions go from xy to the device, after it
+ * the new positions come back into xy (2V doubles, compact order), as the
+ * reference's Run keeps its embedding in host memory every step
+ * (src/embedders/gvizForceEmbedder.c:497-510 around :445-495). The copies of
+ * consecutive steps are pipelined in pieces: a piece's upload for the next
+ * step starts as soon as its download is back, so the two directions share
+ * the link's time. For that overlap xy must be page-locked (cudaHostAlloc or
+ * cudaHostRegister); pageable memory gives the same results without it.
+ * Waits for the last step; returns graph 0's maxDisp of the last step
+ * (negative status on failure, checked after the last step) and fills
+ * stats[graphCount] for it. The results are those of `steps` StepHost calls. */
+double gvizCudaForceRunHost(gvizCudaForce *h, double *xy, uint32_t steps,
+                            gvizCudaStepStats *stats);
+
 /* Enqueues n steps without waiting (replayed from a captured CUDA graph). */
 int gvizCudaForceEnqueueSteps(gvizCudaForce *h, uint32_t n);
 int gvizCudaForceSynchronize(gvizCudaForce *h);
